@@ -1,0 +1,405 @@
+"""Benchmark of the plain relaxation path on B200.
+
+Default workload: the mid-size specimen (periodic 2 mm cube, 20,000 wavy
+fibers of 7 and 19 um split 50:50 by volume, segment length 2 d, curvature
+limit 1/(5 d); about 2.0 M nodes), generated from a seed (synthetic: no
+dataset involved). One step = one `run_batch` of `--iterations` relaxation
+iterations (force_full_iterations, so every step does the same number of
+iterations and neighbor-list rebuilds happen as the displacement check
+requests them).
+
+Printed JSON line (rank 0):
+* value -- node-iterations/s over the K timed steps, whole job, inputs
+  resident in HBM, CUDA events on the library's stream, max over ranks;
+* e2e -- the same metric through the public API with host buffers: every
+  step uploads positions from pinned host memory, runs the batch and
+  downloads the positions;
+* roofline -- the contact pass (the dominant kernel): algorithmic bytes
+  sum_s (60 + 4 K_s) per launch over its CUDA-event duration inside the timed
+  region, against the measured HBM copy bandwidth;
+* cpu_baseline -- the CPU oracle on the same specimen, all host threads,
+  a bounded sample of iterations;
+* time_to_admissible -- seconds for plain PBD from the initial specimen to
+  max overlap < 1e-3 d with curvature <= limit.
+
+`--impl reference` times the reference algorithm's CPU restatement (the
+oracle; the reference is Rust and cannot be built here) on the same
+workload, rank 0 only.
+Multi-GPU: one independent replica specimen per rank (replicas only; the
+relaxation of one specimen runs on one GPU).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s to overlap<1e-3·d & node-iter/s: learned warm-start vs plain PBD, 1 B200"
+UNIT = "node-iter/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
+    ap.add_argument("--workload", choices=["mid_size", "cpu_runnable"], default="mid_size")
+    ap.add_argument("--iterations", type=int, default=128, help="relaxation iterations per step")
+    ap.add_argument("--scale", type=float, default=1.0, help="shrink the mid-size cell (tests only)")
+    ap.add_argument("--capacity", type=int, default=256, help="neighbor slots per segment")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tta", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-iterations", type=int, default=2)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(args, rank):
+    from tangle_b200.generate import cpu_runnable_specimen, mid_size_specimen
+    from tangle_b200.settings import RelaxationSettings
+
+    if args.workload == "cpu_runnable":
+        assembly = cpu_runnable_specimen(seed=1 + rank)
+        name = "cpu_runnable: periodic 300 um cube, 40 straight 10 um fibers x 30 segments (1,240 nodes)"
+    else:
+        assembly = mid_size_specimen(scale=args.scale, seed=1 + rank)
+        name = ("mid_size: periodic 2x2x2 mm, 20,000 wavy fibers 1.5 mm, d 7/19 um 50:50 by volume, "
+                "segment 2d, Schladitz beta 1/0.3 about z (xy-biased), curvature limit 1/(5d)")
+        if args.scale != 1.0:
+            name += f", scaled {args.scale}"
+    d_min = assembly.smallest_diameter()
+    settings = RelaxationSettings(penetration_tolerance=1.0e-3 * d_min, neighbor_capacity=args.capacity,
+                                  max_list_bytes=8 << 30, iterations_per_batch=args.iterations,
+                                  max_iterations=100000)
+    config = settings.to_config(d_min)
+    return assembly, config, name, d_min
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        self.file.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.file.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1", "yes"):
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def contact_bytes(world) -> float:
+    """Algorithmic bytes of one contact pass: sum_s (60 + 4 K_s)."""
+    counts, _ = world.debug_neighbor_lists()
+    return 60.0 * counts.size + 4.0 * float(counts.astype("float64").sum())
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the contact pass from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "contact_traffic.json")
+    try:
+        with open(path) as fh:
+            data = json.load(fh)
+        return float(data["dram_bytes_per_launch_full_size"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def cpu_baseline(packed, config, nodes, iterations):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    cores = os.cpu_count() or 1
+    orc.set_threads(cores)
+    world = orc.OracleWorld(packed, config.cell_list, config.max_step)
+    fixed = type(config)(**{**config.__dict__, "force_full_iterations": True})
+    world.run_batch(fixed, 1)  # builds the lists
+    t0 = time.perf_counter()
+    status = world.run_batch(fixed, iterations)
+    elapsed = time.perf_counter() - t0
+    done = max(status.batch_iterations, 1)
+    world.close()
+    return {"value": nodes * done / elapsed, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{done} plain iterations of the same specimen after one list-building iteration, "
+                      f"{elapsed:.1f} s, OpenMP over {cores} threads"}
+
+
+def run_reference(args):
+    rank, world_size, _ = dist_env()
+    if rank != 0:
+        return 0
+    from tangle_b200.assembly import PackedAssembly
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    assembly, config, name, d_min = workload(args, 0)
+    packed = PackedAssembly.from_assembly(assembly)
+    nodes = packed.vertex_count
+    cores = os.cpu_count() or 1
+    orc.set_threads(cores)
+    world = orc.OracleWorld(packed, config.cell_list, config.max_step)
+    fixed = type(config)(**{**config.__dict__, "force_full_iterations": True})
+    per_step = 1
+    for _ in range(max(args.warmup, 1)):
+        world.run_batch(fixed, per_step)
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(args.steps):
+        st = world.run_batch(fixed, per_step)
+        done += st.batch_iterations
+    elapsed = time.perf_counter() - t0
+    value = nodes * done / elapsed
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": name, "nodes": nodes, "segments": packed.segment_count,
+                   "iterations_per_step": per_step, "neighbor_capacity": config.cell_list.neighbor_capacity},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} steps of {per_step} iteration of the same specimen"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_cuda(args):
+    import numpy as np
+    import torch
+
+    rank, world_size, local = dist_env()
+    if world_size > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    from tangle_b200.assembly import PackedAssembly
+    from tangle_b200.build import build
+    from tangle_b200.device import DeviceWorld
+
+    build()
+    assembly, config, name, d_min = workload(args, rank)
+    packed = PackedAssembly.from_assembly(assembly)
+    nodes = packed.vertex_count
+    fixed = type(config)(**{**config.__dict__, "force_full_iterations": True})
+    world = DeviceWorld(packed, config.cell_list, config.max_step)
+    world.set_kernel_timing(True)
+    stream = torch.cuda.ExternalStream(world.stream_handle)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world_size > 1:
+            torch.distributed.barrier()
+            torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        world.run_batch(fixed, args.iterations)
+    bytes_start = contact_bytes(world)
+    launches0 = world.kernel_launches
+    contact_ms = 0.0
+    contact_passes = 0
+    update_ms = 0.0
+    rebuild_ms = 0.0
+    iterations_done = 0
+    rebuilds0 = world.neighbor_list_rebuilds()
+    launches0 = world.kernel_launches
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            start.record(stream)
+        for _ in range(args.steps):
+            st = world.run_batch(fixed, args.iterations)
+            iterations_done += st.batch_iterations
+            kt = world.last_kernel_times()
+            contact_ms += kt["contact_ms"]
+            contact_passes += kt["contact_passes"]
+            update_ms += kt["update_ms"]
+            rebuild_ms += kt["rebuild_ms"]
+        with torch.cuda.stream(stream):
+            end.record(stream)
+        end.synchronize()
+    launches = world.kernel_launches - launches0
+    rebuilds = world.neighbor_list_rebuilds() - rebuilds0
+    bytes_end = contact_bytes(world)
+    elapsed_ms = start.elapsed_time(end)
+    barrier()
+    local_t = torch.tensor([elapsed_ms, float(nodes * iterations_done)], dtype=torch.float64, device="cuda")
+    if world_size > 1:
+        t_max = local_t[:1].clone()
+        torch.distributed.all_reduce(t_max, op=torch.distributed.ReduceOp.MAX)
+        work = local_t[1:].clone()
+        torch.distributed.all_reduce(work, op=torch.distributed.ReduceOp.SUM)
+        elapsed_ms = float(t_max.item())
+        total_work = float(work.item())
+    else:
+        total_work = float(local_t[1].item())
+    value = total_work / (elapsed_ms / 1000.0)
+    clock_summary = clocks.summary()
+
+    # Roofline of the contact pass.
+    avg_contact_s = (contact_ms / max(contact_passes, 1)) / 1000.0
+    algorithmic = 0.5 * (bytes_start + bytes_end)
+    peak, peak_kind = measured_peak()
+    achieved = algorithmic / avg_contact_s / 1.0e9 if avg_contact_s > 0 else 0.0
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": ncu_traffic(), "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel": "contact_kernel (find_segment_corrections)",
+                "algorithmic_bytes_per_launch": algorithmic, "avg_launch_ms": avg_contact_s * 1000.0}
+
+    # End to end through the public API with pinned host buffers.
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(3 * nodes, dtype=torch.float32, pin_memory=True)
+        host_np = host.numpy()
+        world.download_positions(host_np)
+        for _ in range(max(1, args.warmup // 2)):
+            world.upload_positions(host_np)
+            world.run_batch(fixed, args.iterations)
+            world.download_positions(host_np)
+        barrier()
+        t0 = time.perf_counter()
+        done = 0
+        for _ in range(args.steps):
+            world.upload_positions(host_np)
+            st = world.run_batch(fixed, args.iterations)
+            world.download_positions(host_np)
+            done += st.batch_iterations
+        e2e_s = time.perf_counter() - t0
+        e2e_t = torch.tensor([e2e_s, float(nodes * done)], dtype=torch.float64, device="cuda")
+        if world_size > 1:
+            tm = e2e_t[:1].clone()
+            torch.distributed.all_reduce(tm, op=torch.distributed.ReduceOp.MAX)
+            wk = e2e_t[1:].clone()
+            torch.distributed.all_reduce(wk, op=torch.distributed.ReduceOp.SUM)
+            e2e_s, e2e_work = float(tm.item()), float(wk.item())
+        else:
+            e2e_work = float(e2e_t[1].item())
+        e2e = {"value": e2e_work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 12 * nodes,
+               "d2h_bytes_per_step": 12 * nodes + 64}
+    world.close()
+
+    # Time to admissible from the initial specimen (plain PBD, device-resident).
+    tta = None
+    if not args.no_tta:
+        fresh = DeviceWorld(packed, config.cell_list, config.max_step)
+        t0 = time.perf_counter()
+        status = None
+        while True:
+            status = fresh.run_batch(config, config.iterations_per_batch)
+            if status.converged or status.total_iterations >= 20000:
+                break
+        tta = {"seconds": time.perf_counter() - t0, "iterations": status.total_iterations,
+               "converged": status.converged, "max_penetration_over_d": status.max_penetration / d_min,
+               "max_curvature_ratio": status.max_curvature_ratio, "method": "plain PBD"}
+        fresh.close()
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu:
+        cpu = cpu_baseline(packed, config, nodes, args.cpu_iterations)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": name, "nodes": nodes, "segments": packed.segment_count,
+                       "fibers": packed.fiber_count, "iterations_per_step": args.iterations,
+                       "neighbor_capacity": config.cell_list.neighbor_capacity,
+                       "l2": "inputs larger than L2 (positions, geometry and lists exceed 126 MB)",
+                       "parallelism": f"replicas x{world_size}"},
+            "gpu_launches": int(launches),
+            "neighbor_list_rebuilds": int(rebuilds),
+            "kernel_ms": {"contact": contact_ms, "update": update_ms, "rebuild_and_gated": rebuild_ms},
+            "roofline": roofline,
+            "clocks": clock_summary,
+            "e2e": e2e,
+            "time_to_admissible": tta,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world_size > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_cuda(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,196 @@
+/*
+ * tangle_cuda.h -- C ABI of the B200 (sm_100a) relaxation backend.
+ *
+ * This library is the "cuda" implementation of TANGLE's relaxation seam: the
+ * `RelaxationBackend` / `DeviceWorld` enum of the reference
+ * (crates/tangle_relax/src/device/plugin.rs:15-28, :309-893), whose every
+ * method forwards to `DeviceFiberWorld<R>`
+ * (crates/tangle_relax/src/device/world.rs). Each entry point below names the
+ * reference method it replaces. A Rust host binds these with `extern "C"`
+ * declarations; Python binds them with ctypes (tangle_b200/device.py).
+ *
+ * Conventions (all entry points):
+ *   - return 0 on success, a nonzero TGL_ERR_* code on failure, never throw;
+ *     tgl_last_error() gives the calling thread's last message;
+ *   - host arrays are borrowed for the duration of the call and copied;
+ *   - a world handle is driven from one thread at a time (one handle per
+ *     thread is fine); kernels of one call are asynchronous and the call
+ *     returns after its single status readback, like the reference's
+ *     run_batch + read_status.
+ * Scope: round sections, non-adaptive layouts, flexible motion -- the plain
+ * relaxation path. Positions are f32 in metres, interleaved xyz.
+ */
+#ifndef TANGLE_CUDA_H
+#define TANGLE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TGL_OK 0
+#define TGL_ERR_INVALID 1     /* bad argument or assembly */
+#define TGL_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define TGL_ERR_NO_DEVICE 3   /* no usable sm_100 device */
+#define TGL_ERR_MEMORY 4      /* device allocation failed */
+#define TGL_ERR_UNSUPPORTED 5 /* a setting outside the plain path */
+
+/* Non-adaptive PackedAssembly subset
+ * (crates/tangle_relax/src/device/packed.rs:49-112, packing :150-320).
+ * Fibers must be packed as the reference packs them: a fiber's vertices are
+ * consecutive, its segments are consecutive, and its k-th segment joins its
+ * k-th and (k+1)-th vertices. */
+typedef struct {
+    uint32_t vertex_count;
+    uint32_t segment_count;
+    uint32_t fiber_count;
+    uint32_t reserved;
+    const float *positions;              /* 3V placed xyz */
+    const float *intrinsic_positions;    /* 3V rest-shape xyz */
+    const uint32_t *segment_vertices;    /* 2S */
+    const uint32_t *segment_fibers;      /* S */
+    const float *segment_radii;          /* S */
+    const float *segment_rest_lengths;   /* S */
+    const uint32_t *fiber_vertex_spans;  /* 2F: first vertex, count */
+    const uint32_t *fiber_segment_spans; /* 2F: first segment, count */
+    const uint32_t *vertex_segments;     /* 2V: previous, next (UINT32_MAX) */
+    const float *vertex_max_curvature;   /* V: 0 = unrestricted */
+    const uint32_t *vertex_pinned;       /* V: nonzero = pinned; NULL = none */
+    float cell_lower[3];
+    float cell_upper[3];
+    uint32_t cell_periodic[3];
+    uint32_t reserved2;
+} tgl_packed;
+
+/* CellListConfig (crates/tangle_contact/src/lib.rs:15-40) plus the cap on the
+ * neighbor-list buffer: 0 keeps the reference's 120 MiB
+ * (crates/tangle_relax/src/device/world.rs:35-36). The cap only chooses
+ * which segments use the exact cell-scan fallback, never which contacts
+ * are found. */
+typedef struct {
+    float cell_size_scale;     /* >= 1, default 1 */
+    float neighbor_skin_scale; /* >= 0, default 2 (x largest radius) */
+    uint32_t neighbor_capacity;/* > 0, default 48 slots per segment */
+    uint32_t reserved;
+    uint64_t max_list_bytes;   /* 0 = 120 MiB */
+} tgl_cell_list_config;
+
+/* RelaxationConfig fields the plain path reads
+ * (crates/tangle_relax/src/device/plugin.rs:77-175, defaults :145-175). */
+typedef struct {
+    float penetration_tolerance;
+    float correction_fraction;
+    float stretch_stiffness;
+    float bend_stiffness;
+    float curvature_limit_stiffness;
+    float curvature_limit_safety_margin;
+    float curvature_ratio_tolerance;
+    float max_step;
+    uint32_t constraint_iterations;
+    uint32_t curvature_cleanup_sweeps;
+    uint32_t contact_aggregation;   /* 0 uniform average, 1 penetration weighted, 2 deepest only */
+    uint32_t force_full_iterations; /* nonzero: ignore the tolerances */
+} tgl_relax_config;
+
+/* BatchStatus (crates/tangle_relax/src/device/world.rs:91-114). */
+typedef struct {
+    uint64_t total_iterations;
+    uint64_t batch_iterations;
+    float max_penetration;
+    float max_displacement;
+    float max_curvature_ratio;
+    uint32_t converged;
+    uint32_t cell_list_overflow;
+    uint32_t reserved;
+} tgl_batch_status;
+
+typedef struct tgl_world tgl_world;
+
+/* DeviceFiberWorld::upload (world.rs:308-690; DeviceWorld::upload,
+ * plugin.rs:325-356). Copies every array to the current CUDA device, sizes
+ * the cell grid and neighbor lists exactly as the reference does, and marks
+ * the lists stale so the first contact pass builds them. */
+int tgl_world_create(const tgl_packed *packed, const tgl_cell_list_config *cell_list, float max_step,
+                     tgl_world **out);
+
+/* Drop of the world (frees every device buffer and captured graph). */
+void tgl_world_destroy(tgl_world *world);
+
+/* DeviceFiberWorld::run_batch + read_status (world.rs:1020-1505,
+ * :2337-2369; DeviceWorld::run_batch, plugin.rs:407-418): up to `iterations`
+ * corrections plus one measure-only pass, stopping on the device as soon as
+ * the tolerances are met, then one status readback. */
+int tgl_run_batch(tgl_world *world, const tgl_relax_config *config, uint32_t iterations,
+                  tgl_batch_status *status);
+
+/* DeviceFiberWorld::download_positions (world.rs:2384-2390;
+ * plugin.rs:519-530): interleaved xyz, len == 3V floats. */
+int tgl_download_positions(tgl_world *world, float *xyz, size_t len);
+
+/* Replaces the resident positions (host -> device), as the reference's
+ * host-side operations between batches do (layer targets, needling); the
+ * next batch's displacement check requests a list rebuild if needed. */
+int tgl_upload_positions(tgl_world *world, const float *xyz, size_t len);
+
+/* DeviceWorld::cell_size / cell_count (plugin.rs:597-636). */
+float tgl_cell_size(const tgl_world *world);
+uint64_t tgl_cell_count(const tgl_world *world);
+/* Cells per axis (world.rs:412-414). */
+void tgl_cell_dims(const tgl_world *world, uint32_t dims[3]);
+/* Neighbor skin = skin scale x largest radius (world.rs:356). */
+float tgl_neighbor_skin(const tgl_world *world);
+/* Slots per segment list after the byte cap (world.rs:914-916). */
+uint32_t tgl_neighbor_block(const tgl_world *world);
+/* DeviceFiberWorld::neighbor_list_rebuilds (world/neighbor_list.rs:167-176). */
+int tgl_neighbor_list_rebuilds(tgl_world *world, uint32_t *rebuilds);
+
+/* Parity taps (no reference counterpart beyond its tests' readbacks,
+ * world_tests.rs:1342-1363). Forces a neighbor-list rebuild from the current
+ * positions now. */
+int tgl_debug_rebuild(tgl_world *world);
+/* Cell list in cell order: counts and exclusive offsets [cell_count], and the
+ * segment in every slot [S] (ascending segment within each cell). */
+int tgl_debug_cell_list(tgl_world *world, uint32_t *cell_counts, uint32_t *cell_offsets,
+                        uint32_t *cell_segments);
+/* True neighbor counts [S] and lists [S * block], segment-major; lists of
+ * segments whose count exceeds the block are not meaningful. */
+int tgl_debug_neighbor_lists(tgl_world *world, uint32_t *counts, uint32_t *lists);
+/* One contact pass (find_segment_corrections, contact.rs:232-902) on the
+ * current positions and lists, moving nothing: corrections [6S] and
+ * per-segment maximum penetration [S]. */
+int tgl_debug_corrections(tgl_world *world, const tgl_relax_config *config, float *corrections,
+                          float *segment_max_penetration);
+
+/* Number of kernels this world has launched since creation (graph-replayed
+ * launches included); used to report the bench's launch count. */
+uint64_t tgl_kernel_launches(const tgl_world *world);
+
+/* Per-kernel device time of the last batch, from CUDA events recorded
+ * around every step's kernels when timing is enabled (measurement support;
+ * no reference counterpart). Steps whose kernels returned at once (after
+ * convergence) are excluded. */
+typedef struct {
+    double contact_ms;      /* summed over contact passes that ran */
+    double update_ms;       /* summed over fiber updates that ran */
+    double rebuild_ms;      /* summed over neighbor-list rebuilds that ran */
+    uint32_t contact_passes;
+    uint32_t updates;
+    uint32_t rebuilds;
+    uint32_t reserved;
+} tgl_kernel_times;
+
+int tgl_set_kernel_timing(tgl_world *world, int enable);
+/* The cudaStream_t every kernel of this world runs on (as void*), so a
+ * caller can order its own work or record CUDA events against it. */
+void *tgl_world_stream(const tgl_world *world);
+int tgl_last_kernel_times(tgl_world *world, tgl_kernel_times *times);
+
+/* Thread-local message of the last failed call on this thread. */
+const char *tgl_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

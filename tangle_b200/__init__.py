@@ -1,0 +1,21 @@
+"""tangle_b200: TANGLE's plain relaxation path on NVIDIA B200 (sm_100a).
+
+The "cuda" backend of the reference's relaxation seam: the uniform-grid cell
+list, Verlet neighbor lists, capsule contact projection, stretch /
+rest-shape bend / admissible-curvature projections and the overlap and
+curvature reductions, as hand-written CUDA kernels behind the C ABI of
+include/tangle_cuda.h, with the reference's Python surface
+(`RelaxationSettings`, `Recipe.run`, `RunResult`) on top.
+"""
+
+from .assembly import Cell, FiberAssembly, Material, PackedAssembly
+from .device import DeviceWorld, load_library
+from .generate import FiberPopulation, SplitMix64, generate_fiber_population
+from .recipe import Recipe, RecipeError, RunResult
+from .settings import BatchStatus, CellListConfig, RelaxationConfig, RelaxationSettings
+
+__all__ = [
+    "BatchStatus", "Cell", "CellListConfig", "DeviceWorld", "FiberAssembly", "FiberPopulation", "Material",
+    "PackedAssembly", "Recipe", "RecipeError", "RelaxationConfig", "RelaxationSettings", "RunResult",
+    "SplitMix64", "generate_fiber_population", "load_library",
+]

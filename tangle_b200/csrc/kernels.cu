@@ -1,0 +1,1110 @@
+// kernels.cu -- sm_100a kernels of the plain relaxation path.
+//
+// One relaxation step is three launches, fused from the reference's ~13:
+//   [rebuild, gated on neighbor_state[0]]  cell list + Verlet lists
+//   contact_kernel    find_segment_corrections (contact.rs:232-902); the
+//                     last block to finish reduces the gate metrics and runs
+//                     assess_reduced_metrics (kernels.rs:129-162)
+//   fiber_kernel      everything after the gate, which only ever touches one
+//                     fiber: internal stretch/bend x constraint_iterations
+//                     (kernels.rs:1027-1163, :1417-1453), apply contact
+//                     (:1455-1537), curvature Gauss-Seidel (:1165-1415), the
+//                     displacement check (neighbor.rs:446-465) and the next
+//                     gate's curvature and step measurements (:925-980,
+//                     :95-127). One warp owns one fiber, staged in shared
+//                     memory.
+// Float reductions that feed positions are done in the reference's order
+// (contacts summed in ascending list order); only maxima, which are exact in
+// any order, use atomics (on u32 bits of non-negative floats).
+#include "kernels.cuh"
+
+#include <algorithm>
+
+namespace tgl {
+
+namespace {
+
+constexpr uint32_t FULL = 0xFFFFFFFFu;
+constexpr int CELL_SORT_CAP = 512;  // slots sorted in shared memory per cell
+
+__device__ inline uint32_t warp_max_u32(uint32_t v) { return __reduce_max_sync(FULL, v); }
+
+// ---------------------------------------------------------------- batch control
+
+// kernels.rs:3-12 begin_relaxation_batch; also clears the gate accumulators.
+__global__ void begin_batch_kernel(Control *ctl) {
+    ctl->control[2] = 0;
+    if (ctl->control[3] == 0) ctl->control[0] = 1;
+    ctl->acc[0] = 0;
+    ctl->acc[1] = 0;
+    ctl->acc[2] = 0;
+    ctl->done_blocks = 0;
+}
+
+// neighbor.rs:446-465, over every vertex (all are active in the plain path).
+__global__ void flag_displacement_kernel(WorldDev w) {
+    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    bool far = false;
+    if (v < w.V) {
+        float md = 0.5f * w.skin;
+        float4 p = w.pos[v], r = w.ref_pos[v];
+        float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
+        far = dx * dx + dy * dy + dz * dz > md * md;
+    }
+    if (__any_sync(FULL, far) && (threadIdx.x & 31) == 0) w.ctl->neighbor_state[0] = 1;
+}
+
+// neighbor.rs:436-441.
+__global__ void request_rebuild_kernel(Control *ctl) { ctl->neighbor_state[0] = 1; }
+
+// kernels.rs:925-980 at one interior vertex of a fiber whose positions are
+// p(local index).
+template <typename Fetch>
+__device__ inline float curvature_ratio_at(Fetch p, int i, float maximum) {
+    float4 a0 = p(i - 1), c = p(i), b1 = p(i + 1);
+    float ax = c.x - a0.x, ay = c.y - a0.y, az = c.z - a0.z;
+    float bx = b1.x - c.x, by = b1.y - c.y, bz = b1.z - c.z;
+    float first_length = sqrtf(ax * ax + ay * ay + az * az);
+    float second_length = sqrtf(bx * bx + by * by + bz * bz);
+    float ratio = 0.0f;
+    if (first_length > 1.0e-7f && second_length > 1.0e-7f) {
+        float cosine = (ax * bx + ay * by + az * bz) / (first_length * second_length);
+        cosine = clampf(cosine, -1.0f, 1.0f);
+        float dual_length = 0.5f * (first_length + second_length);
+        float curvature = 2.0f * sqrtf(0.5f * (1.0f - cosine)) / dual_length;
+        ratio = curvature / maximum;
+    }
+    return ratio;
+}
+
+// Gate inputs for the first step of a batch: curvature ratio of the current
+// positions and the last applied step (kernels.rs:112-127).
+__global__ void measure_start_kernel(WorldDev w) {
+    if (w.ctl->control[0] == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5;
+    uint32_t cmax = 0, smax = 0;
+    for (uint32_t f = blockIdx.x * warps + (threadIdx.x >> 5); f < w.F; f += gridDim.x * warps) {
+        uint2 span = w.fiber_vspan[f];
+        const float4 *P = w.pos + span.x;
+        for (uint32_t i = lane; i < span.y; i += 32) {
+            float step = w.vertex_step[span.x + i];
+            smax = max(smax, __float_as_uint(fmaxf(step, 0.0f)));
+            if (i > 0 && i + 1 < span.y) {
+                float maximum = w.vtx_static[span.x + i].x;
+                if (maximum > 0.0f) {
+                    float r = curvature_ratio_at([&](int k) { return P[k]; }, (int)i, maximum);
+                    cmax = max(cmax, __float_as_uint(fmaxf(r, 0.0f)));
+                }
+            }
+        }
+    }
+    cmax = warp_max_u32(cmax);
+    smax = warp_max_u32(smax);
+    if (lane == 0) {
+        if (smax) atomicMax(&w.ctl->acc[1], smax);
+        if (cmax) atomicMax(&w.ctl->acc[2], cmax);
+    }
+}
+
+// ---------------------------------------------------------------- cell list
+// cell_list.rs:63-434 / world/cell_list.rs:94-209, gated on the rebuild flag.
+
+__global__ void rb_clear_kernel(WorldDev w) {
+    if (w.ctl->neighbor_state[0] == 0) return;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < w.C; c += gridDim.x * blockDim.x)
+        w.cell_counts[c] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) w.ctl->cell_overflow = 0;
+}
+
+// count_cell_segments: each segment's midpoint cell, and its arrival ticket.
+__global__ void rb_count_kernel(WorldDev w) {
+    if (w.ctl->neighbor_state[0] == 0) return;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < w.S; s += gridDim.x * blockDim.x) {
+        float4 a = w.geom[2 * (size_t)s], b = w.geom[2 * (size_t)s + 1];
+        uint32_t cell = proxy_cell(a.x, a.y, a.z, b.x, b.y, b.z, w.grid);
+        w.cell_of[s] = cell;
+        w.ticket[s] = atomicAdd(&w.cell_counts[cell], 1u);
+    }
+}
+
+// Exclusive scan of the cell counts in one block (4096 cells per round).
+__global__ void __launch_bounds__(1024) rb_scan_kernel(WorldDev w) {
+    if (w.ctl->neighbor_state[0] == 0) return;
+    __shared__ uint32_t warp_sums[32];
+    __shared__ uint32_t carry_s;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry_s = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < w.C; base += 4096) {
+        uint32_t idx = base + threadIdx.x * 4;
+        uint32_t v[4];
+        uint32_t local = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            v[k] = (idx + k < w.C) ? w.cell_counts[idx + k] : 0u;
+            local += v[k];
+        }
+        uint32_t incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) warp_sums[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t ws = warp_sums[lane];
+            uint32_t wi = ws;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_up_sync(FULL, wi, o);
+                if (lane >= o) wi += t;
+            }
+            warp_sums[lane] = wi - ws;  // exclusive warp offsets
+        }
+        __syncthreads();
+        uint32_t run = carry_s + warp_sums[warp] + incl - local;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (idx + k < w.C) w.cell_offsets[idx + k] = run;
+            run += v[k];
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry_s = run;
+        __syncthreads();
+    }
+}
+
+// scatter_cell_segments.
+__global__ void rb_scatter_kernel(WorldDev w) {
+    if (w.ctl->neighbor_state[0] == 0) return;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < w.S; s += gridDim.x * blockDim.x)
+        w.cell_segments[w.cell_offsets[w.cell_of[s]] + w.ticket[s]] = s;
+}
+
+// rank_cell_segments (cell_list.rs:392-434): ascending segment order inside
+// every cell. One warp per cell; a rank sort in shared memory, or over the
+// global range (into the free ticket array) for very crowded cells.
+__global__ void rb_sort_cells_kernel(WorldDev w) {
+    if (w.ctl->neighbor_state[0] == 0) return;
+    extern __shared__ uint32_t sort_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    uint32_t *buf = sort_smem + warp * CELL_SORT_CAP;
+    for (uint32_t c = blockIdx.x * warps + warp; c < w.C; c += gridDim.x * warps) {
+        uint32_t n = w.cell_counts[c];
+        if (n < 2) continue;
+        uint32_t off = w.cell_offsets[c];
+        uint32_t *seg = w.cell_segments + off;
+        if (n <= CELL_SORT_CAP) {
+            for (uint32_t i = lane; i < n; i += 32) buf[i] = seg[i];
+            __syncwarp();
+            for (uint32_t i = lane; i < n; i += 32) {
+                uint32_t key = buf[i], rank = 0;
+                for (uint32_t j = 0; j < n; ++j) rank += buf[j] < key ? 1u : 0u;
+                seg[rank] = key;
+            }
+            __syncwarp();
+        } else {
+            uint32_t *tmp = w.ticket + off;
+            for (uint32_t i = lane; i < n; i += 32) {
+                uint32_t key = seg[i], rank = 0;
+                for (uint32_t j = 0; j < n; ++j) rank += seg[j] < key ? 1u : 0u;
+                tmp[rank] = key;
+            }
+            __syncwarp();
+            for (uint32_t i = lane; i < n; i += 32) seg[i] = tmp[i];
+            __syncwarp();
+        }
+    }
+}
+
+// gather_cell_slot_geometry (neighbor.rs:107-153): geometry in slot order.
+__global__ void rb_gather_kernel(WorldDev w) {
+    if (w.ctl->neighbor_state[0] == 0) return;
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.S; slot += gridDim.x * blockDim.x) {
+        uint32_t s = w.cell_segments[slot];
+        float4 a = w.geom[2 * (size_t)s], b = w.geom[2 * (size_t)s + 1];
+        b.w = __uint_as_float(s);
+        w.slot_geom[2 * (size_t)slot] = a;
+        w.slot_geom[2 * (size_t)slot + 1] = b;
+    }
+}
+
+// build_segment_neighbor_lists (neighbor.rs:155-364). One block per home cell:
+// the 27 stencil cells' slots are staged in shared memory chunk by chunk and
+// each warp tests them, 32 at a time, against one home segment, appending
+// hits in scan order (sorted afterwards).
+__global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch) {
+    if (w.ctl->neighbor_state[0] == 0) return;
+    extern __shared__ float4 build_smem[];
+    __shared__ uint32_t st_count[27], st_off[27], st_prefix[28];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    const float skin = w.skin;
+    const uint32_t block = w.block;
+    for (uint32_t h = blockIdx.x; h < w.C; h += gridDim.x) {
+        uint32_t nh = w.cell_counts[h];
+        if (nh == 0) continue;
+        uint32_t hoff = w.cell_offsets[h];
+        if (threadIdx.x < 27) {
+            uint32_t cell = stencil_cell(h, threadIdx.x, w.grid);
+            st_count[threadIdx.x] = cell == TGL_NONE ? 0u : w.cell_counts[cell];
+            st_off[threadIdx.x] = cell == TGL_NONE ? 0u : w.cell_offsets[cell];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t run = 0;
+            for (int k = 0; k < 27; ++k) {
+                st_prefix[k] = run;
+                run += st_count[k];
+            }
+            st_prefix[27] = run;
+        }
+        __syncthreads();
+        const uint32_t total = st_prefix[27];
+        for (uint32_t base = 0; base < total || base == 0; base += (uint32_t)ch) {
+            uint32_t len = total > base ? min((uint32_t)ch, total - base) : 0u;
+            for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+                uint32_t flat = base + i;
+                int k = 0;
+                while (k < 26 && st_prefix[k + 1] <= flat) ++k;
+                uint32_t slot = st_off[k] + (flat - st_prefix[k]);
+                build_smem[2 * i] = w.slot_geom[2 * (size_t)slot];
+                build_smem[2 * i + 1] = w.slot_geom[2 * (size_t)slot + 1];
+            }
+            __syncthreads();
+            for (uint32_t hi = warp; hi < nh; hi += warps) {
+                float4 a = w.slot_geom[2 * (size_t)(hoff + hi)], b = w.slot_geom[2 * (size_t)(hoff + hi) + 1];
+                const uint32_t segment = __float_as_uint(b.w);
+                const float p1x = a.x, p1y = a.y, p1z = a.z, radius = a.w;
+                const float q1x = b.x, q1y = b.y, q1z = b.z;
+                const float d1x = q1x - p1x, d1y = q1y - p1y, d1z = q1z - p1z;
+                const float half_length = 0.5f * sqrtf(d1x * d1x + d1y * d1y + d1z * d1z);
+                const float4 own = w.seg_static[segment];
+                const uint32_t owner = __float_as_uint(own.w);
+                uint32_t count = base == 0 ? 0u : w.nbr_count[segment];
+                uint32_t *list = w.nbr_list + (size_t)segment * block;
+                for (uint32_t c0 = 0; c0 < len; c0 += 32) {
+                    uint32_t c = c0 + lane;
+                    bool hit = false;
+                    uint32_t other = 0;
+                    if (c < len) {
+                        float4 oa = build_smem[2 * c], ob = build_smem[2 * c + 1];
+                        other = __float_as_uint(ob.w);
+                        float p2x = oa.x, p2y = oa.y, p2z = oa.z, q2x = ob.x, q2y = ob.y, q2z = ob.z;
+                        float other_radius = oa.w;
+                        minimum_image(p1x, p1y, p1z, q1x, q1y, q1z, p2x, p2y, p2z, q2x, q2y, q2z, w.grid);
+                        float d2x = q2x - p2x, d2y = q2y - p2y, d2z = q2z - p2z;
+                        float interaction = (radius + other_radius + skin) * (1.0f + 1.0e-4f);
+                        float mdx = 0.5f * (p2x + q2x - p1x - q1x);
+                        float mdy = 0.5f * (p2y + q2y - p1y - q1y);
+                        float mdz = 0.5f * (p2z + q2z - p1z - q1z);
+                        float reach = half_length + 0.5f * sqrtf(d2x * d2x + d2y * d2y + d2z * d2z) + interaction;
+                        if (mdx * mdx + mdy * mdy + mdz * mdz <= reach * reach &&
+                            axis_distance(p1x, p1y, p1z, d1x, d1y, d1z, p2x, p2y, p2z, d2x, d2y, d2z) <= interaction) {
+                            // The pair-independent exclusions (neighbor.rs:282-294).
+                            float4 os = w.seg_static[other];
+                            float gap = fmaxf(os.y - own.z, own.y - os.z);  // along_fiber_gap
+                            bool near_along_fiber = __float_as_uint(os.w) == owner && gap < radius + os.x;
+                            hit = other != segment && !near_along_fiber;
+                        }
+                    }
+                    uint32_t ballot = __ballot_sync(FULL, hit);
+                    uint32_t rank = __popc(ballot & ((1u << lane) - 1u));
+                    if (hit && count + rank < block) list[count + rank] = other;
+                    count += __popc(ballot);
+                }
+                if (lane == 0) w.nbr_count[segment] = count;
+            }
+            __syncthreads();
+            if (total == 0) break;
+        }
+    }
+}
+
+// sort_neighbor_lists (neighbor.rs:366-408): ascending segment order for
+// every list that fits its block; overflowed lists are never read.
+__global__ void rb_sort_lists_kernel(WorldDev w) {
+    if (w.ctl->neighbor_state[0] == 0) return;
+    extern __shared__ uint32_t list_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    uint32_t *buf = list_smem + (size_t)warp * w.block;
+    for (uint32_t s = blockIdx.x * warps + warp; s < w.S; s += gridDim.x * warps) {
+        uint32_t n = w.nbr_count[s];
+        if (n < 2 || n > w.block) continue;
+        uint32_t *list = w.nbr_list + (size_t)s * w.block;
+        for (uint32_t i = lane; i < n; i += 32) buf[i] = list[i];
+        __syncwarp();
+        for (uint32_t i = lane; i < n; i += 32) {
+            uint32_t key = buf[i], rank = 0;
+            for (uint32_t j = 0; j < n; ++j) rank += buf[j] < key ? 1u : 0u;
+            list[rank] = key;
+        }
+        __syncwarp();
+    }
+}
+
+// snapshot_neighbor_reference_positions (neighbor.rs:410-422).
+__global__ void rb_snapshot_kernel(WorldDev w) {
+    if (w.ctl->neighbor_state[0] == 0) return;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x)
+        w.ref_pos[v] = w.pos[v];
+}
+
+// finish_neighbor_list_rebuild (neighbor.rs:424-432).
+__global__ void rb_finish_kernel(Control *ctl) {
+    if (ctl->neighbor_state[0] == 0) return;
+    ctl->neighbor_state[0] = 0;
+    ctl->neighbor_state[1] += 1;
+}
+
+// ---------------------------------------------------------------- contact pass
+
+struct PairTerms {
+    float pen, t0x, t0y, t0z, t1x, t1y, t1z, aggw;
+};
+
+// One candidate pair of find_segment_corrections (contact.rs:450-870) for a
+// round lane at zero offset: returns true with the pair's terms when the
+// capsules overlap.
+__device__ inline bool contact_pair(float p1x, float p1y, float p1z, float q1x, float q1y, float q1z, float d1x,
+                                    float d1y, float d1z, float radius, float half_length, uint32_t segment,
+                                    uint32_t other, float4 oa, float4 ob, const Grid &g, float correction_fraction,
+                                    uint32_t aggregation, PairTerms &out) {
+    const float length_epsilon = 1.0e-20f;
+    const float parallel_relative_epsilon = 1.0e-6f;
+    float p2x = oa.x, p2y = oa.y, p2z = oa.z, q2x = ob.x, q2y = ob.y, q2z = ob.z;
+    const float other_radius = oa.w;
+    minimum_image(p1x, p1y, p1z, q1x, q1y, q1z, p2x, p2y, p2z, q2x, q2y, q2z, g);
+    float d2x = q2x - p2x, d2y = q2y - p2y, d2z = q2z - p2z;
+    float mdx = 0.5f * (p2x + q2x - p1x - q1x);
+    float mdy = 0.5f * (p2y + q2y - p1y - q1y);
+    float mdz = 0.5f * (p2z + q2z - p1z - q1z);
+    float reach = (half_length + 0.5f * sqrtf(d2x * d2x + d2y * d2y + d2z * d2z) + radius + other_radius) *
+                  (1.0f + 1.0e-4f);
+    if (!(mdx * mdx + mdy * mdy + mdz * mdz <= reach * reach)) return false;
+    float rx = p1x - p2x, ry = p1y - p2y, rz = p1z - p2z;
+    float a = d1x * d1x + d1y * d1y + d1z * d1z;
+    float e = d2x * d2x + d2y * d2y + d2z * d2z;
+    float f = d2x * rx + d2y * ry + d2z * rz;
+    float s = 0.0f, t = 0.0f;
+    if (a <= length_epsilon && e > length_epsilon) {
+        t = clampf(f / e, 0.0f, 1.0f);
+    } else if (a > length_epsilon) {
+        float c = d1x * rx + d1y * ry + d1z * rz;
+        if (e <= length_epsilon) {
+            s = clampf(-c / a, 0.0f, 1.0f);
+        } else {
+            float b = d1x * d2x + d1y * d2y + d1z * d2z;
+            float denominator = a * e - b * b;
+            bool parallel = fabsf(denominator) <= parallel_relative_epsilon * a * e;
+            if (!parallel) s = clampf((b * f - c * e) / denominator, 0.0f, 1.0f);
+            float projected = (b * s + f) / e;
+            if (projected < 0.0f) {
+                s = clampf(-c / a, 0.0f, 1.0f);
+            } else if (projected > 1.0f) {
+                t = 1.0f;
+                s = clampf((b - c) / a, 0.0f, 1.0f);
+            } else {
+                t = projected;
+            }
+            if (parallel) {  // contact.rs:695-726
+                float end_s = 1.0f, end_t = 0.0f;
+                float end_projected = (b + f) / e;
+                if (end_projected < 0.0f) {
+                    end_s = clampf(-c / a, 0.0f, 1.0f);
+                } else if (end_projected > 1.0f) {
+                    end_t = 1.0f;
+                    end_s = clampf((b - c) / a, 0.0f, 1.0f);
+                } else {
+                    end_t = end_projected;
+                }
+                float gx = rx + d1x * s - d2x * t, gy = ry + d1y * s - d2y * t, gz = rz + d1z * s - d2z * t;
+                float ex = rx + d1x * end_s - d2x * end_t, ey = ry + d1y * end_s - d2y * end_t,
+                      ez = rz + d1z * end_s - d2z * end_t;
+                if (ex * ex + ey * ey + ez * ez < gx * gx + gy * gy + gz * gz) {
+                    s = end_s;
+                    t = end_t;
+                }
+            }
+        }
+    }
+    float point1x = p1x + d1x * s, point1y = p1y + d1y * s, point1z = p1z + d1z * s;
+    float point2x = p2x + d2x * t, point2y = p2y + d2y * t, point2z = p2z + d2z * t;
+    float delta_x = point2x - point1x, delta_y = point2y - point1y, delta_z = point2z - point1z;
+    float distance = sqrtf(delta_x * delta_x + delta_y * delta_y + delta_z * delta_z);
+    float penetration = radius + other_radius - distance;
+    if (!(penetration > 0.0f)) return false;
+    float nx, ny, nz;
+    if (distance > 1.0e-7f) {
+        float inverse_distance = 1.0f / distance;
+        nx = delta_x * inverse_distance;
+        ny = delta_y * inverse_distance;
+        nz = delta_z * inverse_distance;
+    } else {  // contact.rs:768-812
+        nx = d1y * d2z - d1z * d2y;
+        ny = d1z * d2x - d1x * d2z;
+        nz = d1x * d2y - d1y * d2x;
+        float normal_length = sqrtf(nx * nx + ny * ny + nz * nz);
+        if (normal_length <= 1.0e-7f) {
+            if (fabsf(d1x) <= fabsf(d1y) && fabsf(d1x) <= fabsf(d1z)) {
+                nx = 0.0f;
+                ny = d1z;
+                nz = -d1y;
+            } else if (fabsf(d1y) <= fabsf(d1z)) {
+                nx = -d1z;
+                ny = 0.0f;
+                nz = d1x;
+            } else {
+                nx = d1y;
+                ny = -d1x;
+                nz = 0.0f;
+            }
+            normal_length = sqrtf(nx * nx + ny * ny + nz * nz);
+        }
+        if (normal_length > 1.0e-7f) {
+            nx /= normal_length;
+            ny /= normal_length;
+            nz /= normal_length;
+        } else {
+            nx = 1.0f;
+        }
+        float dominant;
+        if (fabsf(nx) >= fabsf(ny) && fabsf(nx) >= fabsf(nz))
+            dominant = nx;
+        else if (fabsf(ny) >= fabsf(nz))
+            dominant = ny;
+        else
+            dominant = nz;
+        if (dominant < 0.0f) {
+            nx = -nx;
+            ny = -ny;
+            nz = -nz;
+        }
+        if (segment > other) {
+            nx = -nx;
+            ny = -ny;
+            nz = -nz;
+        }
+    }
+    float weight_0 = 1.0f - s;
+    float weight_1 = s;
+    float other_weight_0 = 1.0f - t;
+    float denominator = weight_0 * weight_0 + weight_1 * weight_1 + other_weight_0 * other_weight_0 + t * t;
+    float magnitude = -correction_fraction * penetration / denominator;
+    float aggregate_weight = aggregation == 1 ? penetration : 1.0f;
+    out.pen = penetration;
+    out.t0x = nx * magnitude * weight_0 * aggregate_weight;
+    out.t0y = ny * magnitude * weight_0 * aggregate_weight;
+    out.t0z = nz * magnitude * weight_0 * aggregate_weight;
+    out.t1x = nx * magnitude * weight_1 * aggregate_weight;
+    out.t1y = ny * magnitude * weight_1 * aggregate_weight;
+    out.t1z = nz * magnitude * weight_1 * aggregate_weight;
+    out.aggw = aggregate_weight;
+    return true;
+}
+
+struct ContactAcc {
+    float c0x, c0y, c0z, c1x, c1y, c1z, weight, maxpen;
+};
+
+// Adds the group's hits to the running sums in ascending lane (= list)
+// order, exactly as the reference's serial loop does (contact.rs:750-870).
+template <int G>
+__device__ inline void accumulate_in_order(bool hit, const PairTerms &pt, uint32_t gmask, int gbase,
+                                           uint32_t aggregation, ContactAcc &acc) {
+    uint32_t ballot = __ballot_sync(gmask, hit);
+    uint32_t bits = G == 32 ? ballot : ((ballot >> gbase) & ((1u << G) - 1u));
+    while (bits) {
+        int j = __ffs(bits) - 1;
+        bits &= bits - 1u;
+        float pen = __shfl_sync(gmask, pt.pen, j, G);
+        float t0x = __shfl_sync(gmask, pt.t0x, j, G);
+        float t0y = __shfl_sync(gmask, pt.t0y, j, G);
+        float t0z = __shfl_sync(gmask, pt.t0z, j, G);
+        float t1x = __shfl_sync(gmask, pt.t1x, j, G);
+        float t1y = __shfl_sync(gmask, pt.t1y, j, G);
+        float t1z = __shfl_sync(gmask, pt.t1z, j, G);
+        float aggw = __shfl_sync(gmask, pt.aggw, j, G);
+        bool deepest = pen > acc.maxpen;
+        if (deepest) acc.maxpen = pen;
+        if (aggregation == 2) {
+            if (deepest) {
+                acc.c0x = t0x;
+                acc.c0y = t0y;
+                acc.c0z = t0z;
+                acc.c1x = t1x;
+                acc.c1y = t1y;
+                acc.c1z = t1z;
+                acc.weight = 1.0f;
+            }
+        } else {
+            acc.c0x += t0x;
+            acc.c0y += t0y;
+            acc.c0z += t0z;
+            acc.c1x += t1x;
+            acc.c1y += t1y;
+            acc.c1z += t1z;
+            acc.weight += aggw;
+        }
+    }
+}
+
+// find_segment_corrections (contact.rs:232-902) with G lanes per segment,
+// then (gate != 0) assess_reduced_metrics in the last block to finish.
+template <int G>
+__global__ void __launch_bounds__(256) contact_kernel(WorldDev w, StepParams sp, int gate) {
+    __shared__ uint32_t warp_max[8];
+    __shared__ int is_last;
+    if (gate && w.ctl->control[0] == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G;
+    const int gbase = lane - gl;
+    const uint32_t gmask = G == 32 ? FULL : (((1u << G) - 1u) << gbase);
+    const uint32_t groups = gridDim.x * (blockDim.x / G);
+    const Grid &g = w.grid;
+    uint32_t thread_max = 0;
+    for (uint32_t segment = (blockIdx.x * blockDim.x + threadIdx.x) / G; segment < w.S; segment += groups) {
+        const float4 a = w.geom[2 * (size_t)segment], b = w.geom[2 * (size_t)segment + 1];
+        const float p1x = a.x, p1y = a.y, p1z = a.z, radius = a.w;
+        const float q1x = b.x, q1y = b.y, q1z = b.z;
+        const float d1x = q1x - p1x, d1y = q1y - p1y, d1z = q1z - p1z;
+        const float half_length = 0.5f * sqrtf(d1x * d1x + d1y * d1y + d1z * d1z);
+        ContactAcc acc = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        const uint32_t listed_count = w.nbr_count[segment];
+        if (listed_count <= w.block) {
+            // Listed candidates passed the self and along-fiber exclusions
+            // when the list was built; both depend only on static data.
+            const uint32_t *list = w.nbr_list + (size_t)segment * w.block;
+            for (uint32_t k0 = 0; k0 < listed_count; k0 += G) {
+                uint32_t k = k0 + gl;
+                PairTerms pt;
+                bool hit = false;
+                if (k < listed_count) {
+                    uint32_t other = __ldg(list + k);
+                    float4 oa = w.geom[2 * (size_t)other], ob = w.geom[2 * (size_t)other + 1];
+                    hit = contact_pair(p1x, p1y, p1z, q1x, q1y, q1z, d1x, d1y, d1z, radius, half_length, segment,
+                                       other, oa, ob, g, sp.correction_fraction, sp.contact_aggregation, pt);
+                }
+                accumulate_in_order<G>(hit, pt, gmask, gbase, sp.contact_aggregation, acc);
+            }
+        } else {
+            // Overflowed list: scan the 27 cells around the home cell of the
+            // positions the lists were built from (contact.rs:365-437).
+            const float4 own = w.seg_static[segment];
+            const uint32_t owner = __float_as_uint(own.w);
+            const uint32_t v0 = w.seg_v0[segment];
+            const float4 r0 = w.ref_pos[v0], r1 = w.ref_pos[v0 + 1];
+            const uint32_t home = proxy_cell(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, g);
+            for (uint32_t n = 0; n < 27; ++n) {
+                uint32_t cell = stencil_cell(home, n, g);
+                if (cell == TGL_NONE) continue;
+                const uint32_t count = w.cell_counts[cell];
+                const uint32_t start = w.cell_offsets[cell];
+                for (uint32_t k0 = 0; k0 < count; k0 += G) {
+                    uint32_t k = k0 + gl;
+                    PairTerms pt;
+                    bool hit = false;
+                    if (k < count) {
+                        uint32_t other = w.cell_segments[start + k];
+                        float4 os = w.seg_static[other];
+                        float gap = fmaxf(os.y - own.z, own.y - os.z);
+                        bool near_along_fiber = __float_as_uint(os.w) == owner && gap < radius + os.x;
+                        if (other != segment && !near_along_fiber) {
+                            float4 oa = w.geom[2 * (size_t)other], ob = w.geom[2 * (size_t)other + 1];
+                            hit = contact_pair(p1x, p1y, p1z, q1x, q1y, q1z, d1x, d1y, d1z, radius, half_length,
+                                               segment, other, oa, ob, g, sp.correction_fraction,
+                                               sp.contact_aggregation, pt);
+                        }
+                    }
+                    accumulate_in_order<G>(hit, pt, gmask, gbase, sp.contact_aggregation, acc);
+                }
+            }
+        }
+        if (sp.contact_aggregation != 2 && acc.weight > 1.0e-20f) {
+            acc.c0x /= acc.weight;
+            acc.c0y /= acc.weight;
+            acc.c0z /= acc.weight;
+            acc.c1x /= acc.weight;
+            acc.c1y /= acc.weight;
+            acc.c1z /= acc.weight;
+        }
+        if (gl == 0) {
+            w.corr[2 * (size_t)segment] = make_float4(acc.c0x, acc.c0y, acc.c0z, acc.maxpen);
+            w.corr[2 * (size_t)segment + 1] = make_float4(acc.c1x, acc.c1y, acc.c1z, 0.0f);
+        }
+        thread_max = max(thread_max, __float_as_uint(fmaxf(acc.maxpen, 0.0f)));
+    }
+    if (!gate) return;
+    thread_max = warp_max_u32(thread_max);
+    if (lane == 0) warp_max[threadIdx.x >> 5] = thread_max;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t m = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) m = max(m, warp_max[k]);
+        if (m) atomicMax(&w.ctl->acc[0], m);
+        __threadfence();
+        is_last = atomicAdd(&w.ctl->done_blocks, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+        __threadfence();
+        Control *c = w.ctl;
+        // kernels.rs:129-162 assess_reduced_metrics.
+        float maximum_penetration = __uint_as_float(atomicAdd(&c->acc[0], 0u));
+        float maximum_step = __uint_as_float(atomicAdd(&c->acc[1], 0u));
+        float maximum_curvature_ratio = __uint_as_float(atomicAdd(&c->acc[2], 0u));
+        c->metrics[0] = maximum_penetration;
+        c->metrics[1] = maximum_step;
+        c->metrics[2] = maximum_curvature_ratio;
+        uint32_t overflow = c->cell_overflow;
+        if (overflow != 0 ||
+            (sp.force_full_iterations == 0 && maximum_penetration <= sp.penetration_tolerance &&
+             maximum_curvature_ratio <= 1.0f + sp.curvature_ratio_tolerance) ||
+            c->control[2] >= sp.max_iterations) {
+            if (overflow != 0) c->control[3] = 1;
+            c->control[0] = 0;
+        } else {
+            c->control[1] += 1;
+            c->control[2] += 1;
+        }
+        c->acc[0] = 0;
+        c->acc[1] = 0;
+        c->acc[2] = 0;
+        c->done_blocks = 0;
+        __threadfence();
+    }
+}
+
+// ---------------------------------------------------------------- fiber update
+
+struct Triplet {
+    float scale, pw, cw, nw;
+    float gux, guy, guz, cgx, cgy, cgz, gvx, gvy, gvz;
+};
+
+// project_curvature_triplet_in_place (kernels.rs:1165-1322), split into the
+// test (does it move anything?) and the move, so that a warp can test many
+// triplets at once and apply only the first that acts.
+__device__ inline bool curvature_triplet_test(const float4 *P, const float4 *St, int prev, int center, int next,
+                                              float stiffness, float safety_margin, Triplet &t) {
+    float maximum_curvature = St[center].x * (1.0f - safety_margin);
+    if (!(maximum_curvature > 0.0f)) return false;
+    float4 pp = P[prev], pc = P[center], pn = P[next];
+    float ux = pc.x - pp.x, uy = pc.y - pp.y, uz = pc.z - pp.z;
+    float vx = pn.x - pc.x, vy = pn.y - pc.y, vz = pn.z - pc.z;
+    float first_length = sqrtf(ux * ux + uy * uy + uz * uz);
+    float second_length = sqrtf(vx * vx + vy * vy + vz * vz);
+    if (!(first_length > 1.0e-7f && second_length > 1.0e-7f)) return false;
+    float unx = ux / first_length, uny = uy / first_length, unz = uz / first_length;
+    float vnx = vx / second_length, vny = vy / second_length, vnz = vz / second_length;
+    float cosine = clampf(unx * vnx + uny * vny + unz * vnz, -1.0f, 1.0f);
+    float sine_half = 0.25f * maximum_curvature * (first_length + second_length);
+    if (!(sine_half < 1.0f)) return false;
+    float minimum_cosine = 1.0f - 2.0f * sine_half * sine_half;
+    float violation = minimum_cosine - cosine;
+    float sine = sqrtf(fmaxf(1.0f - cosine * cosine, 0.0f));
+    if (violation > 0.0f && sine > 1.0e-3f) violation = (acos_f32(cosine) - acos_f32(minimum_cosine)) * sine;
+    if (!(violation > 0.0f)) return false;
+    t.gux = (vnx - cosine * unx) / first_length;
+    t.guy = (vny - cosine * uny) / first_length;
+    t.guz = (vnz - cosine * unz) / first_length;
+    t.gvx = (unx - cosine * vnx) / second_length;
+    t.gvy = (uny - cosine * vny) / second_length;
+    t.gvz = (unz - cosine * vnz) / second_length;
+    t.cgx = t.gux - t.gvx;
+    t.cgy = t.guy - t.gvy;
+    t.cgz = t.guz - t.gvz;
+    t.pw = pp.w != 0.0f ? 0.0f : 1.0f;  // w carries the pinned flag in shared memory
+    t.cw = pc.w != 0.0f ? 0.0f : 1.0f;
+    t.nw = pn.w != 0.0f ? 0.0f : 1.0f;
+    float denominator = t.pw * (t.gux * t.gux + t.guy * t.guy + t.guz * t.guz) +
+                        t.cw * (t.cgx * t.cgx + t.cgy * t.cgy + t.cgz * t.cgz) +
+                        t.nw * (t.gvx * t.gvx + t.gvy * t.gvy + t.gvz * t.gvz);
+    if (!(denominator > 1.0e-12f)) return false;
+    t.scale = stiffness * violation / denominator;
+    return t.pw > 0.0f || t.cw > 0.0f || t.nw > 0.0f;
+}
+
+__device__ inline float wall_clamp(float moved, float extent, int axis, const Grid &g) {
+    return g.periodic[axis] ? moved : clampf(moved, g.lower[axis] + extent, g.upper[axis] - extent);
+}
+
+__device__ inline void curvature_triplet_apply(float4 *P, const float4 *St, int prev, int center, int next,
+                                               const Triplet &t, const Grid &g) {
+    float4 pp = P[prev], pc = P[center], pn = P[next];
+    float pe = St[prev].w, ce = St[center].w, ne = St[next].w;
+    float mp, mc, mn;
+    mp = pp.x - t.pw * t.scale * t.gux;
+    mc = pc.x + t.cw * t.scale * t.cgx;
+    mn = pn.x + t.nw * t.scale * t.gvx;
+    if (t.pw > 0.0f) pp.x = wall_clamp(mp, pe, 0, g);
+    if (t.cw > 0.0f) pc.x = wall_clamp(mc, ce, 0, g);
+    if (t.nw > 0.0f) pn.x = wall_clamp(mn, ne, 0, g);
+    mp = pp.y - t.pw * t.scale * t.guy;
+    mc = pc.y + t.cw * t.scale * t.cgy;
+    mn = pn.y + t.nw * t.scale * t.gvy;
+    if (t.pw > 0.0f) pp.y = wall_clamp(mp, pe, 1, g);
+    if (t.cw > 0.0f) pc.y = wall_clamp(mc, ce, 1, g);
+    if (t.nw > 0.0f) pn.y = wall_clamp(mn, ne, 1, g);
+    mp = pp.z - t.pw * t.scale * t.guz;
+    mc = pc.z + t.cw * t.scale * t.cgz;
+    mn = pn.z + t.nw * t.scale * t.gvz;
+    if (t.pw > 0.0f) pp.z = wall_clamp(mp, pe, 2, g);
+    if (t.cw > 0.0f) pc.z = wall_clamp(mc, ce, 2, g);
+    if (t.nw > 0.0f) pn.z = wall_clamp(mn, ne, 2, g);
+    P[prev] = pp;
+    P[center] = pc;
+    P[next] = pn;
+}
+
+// Everything after the gate, one warp per fiber.
+__global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
+    if (w.ctl->control[0] == 0) return;
+    extern __shared__ float4 fiber_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warps = blockDim.x >> 5;
+    const int maxv = (int)w.max_fiber;
+    float4 *P = fiber_smem + (size_t)warp * 3 * maxv;  // positions, w = pinned
+    float4 *T = P + maxv;                              // internal corrections
+    float4 *St = T + maxv;                             // static vertex data
+    const Grid &g = w.grid;
+    const float md = 0.5f * w.skin;
+    uint32_t smax = 0, cmax = 0;
+    bool far = false;
+    for (uint32_t f = blockIdx.x * warps + warp; f < w.F; f += gridDim.x * warps) {
+        const uint2 span = w.fiber_vspan[f];
+        const uint32_t v0 = span.x;
+        const int n = (int)span.y;
+        const uint32_t s0 = w.fiber_s0[f];
+        const float radius = w.seg_static[s0].x;
+        for (int i = lane; i < n; i += 32) {
+            float4 p = w.pos[v0 + i];
+            p.w = w.pinned[v0 + i] ? 1.0f : 0.0f;
+            P[i] = p;
+            St[i] = w.vtx_static[v0 + i];
+        }
+        __syncwarp();
+        // find/apply_internal_corrections x constraint_iterations (Jacobi).
+        for (uint32_t pass = 0; pass < sp.constraint_iterations; ++pass) {
+            for (int i = lane; i < n; i += 32) {
+                float4 x = P[i];
+                float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+                if (x.w == 0.0f) {
+                    if (i > 0) {
+                        float4 o = P[i - 1];
+                        float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                        float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                        if (length > 1.0e-7f) {
+                            float magnitude = 0.5f * sp.stretch_stiffness * (length - w.rest[s0 + i - 1]) / length;
+                            cx += dx * magnitude;
+                            cy += dy * magnitude;
+                            cz += dz * magnitude;
+                        }
+                    }
+                    if (i + 1 < n) {
+                        float4 o = P[i + 1];
+                        float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                        float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                        if (length > 1.0e-7f) {
+                            float magnitude = 0.5f * sp.stretch_stiffness * (length - w.rest[s0 + i]) / length;
+                            cx += dx * magnitude;
+                            cy += dy * magnitude;
+                            cz += dz * magnitude;
+                        }
+                    }
+                    if (i > 1) {
+                        float4 o = P[i - 2];
+                        float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                        float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                        if (length > 1.0e-7f) {
+                            float magnitude = 0.5f * sp.bend_stiffness * (length - St[i].y) / length;
+                            cx += dx * magnitude;
+                            cy += dy * magnitude;
+                            cz += dz * magnitude;
+                        }
+                    }
+                    if (i + 2 < n) {
+                        float4 o = P[i + 2];
+                        float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                        float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                        if (length > 1.0e-7f) {
+                            float magnitude = 0.5f * sp.bend_stiffness * (length - St[i].z) / length;
+                            cx += dx * magnitude;
+                            cy += dy * magnitude;
+                            cz += dz * magnitude;
+                        }
+                    }
+                }
+                T[i] = make_float4(cx, cy, cz, 0.0f);
+            }
+            __syncwarp();
+            for (int i = lane; i < n; i += 32) {
+                float4 x = P[i];
+                if (x.w != 0.0f) continue;
+                float4 c = T[i];
+                float e = St[i].w;
+                x.x = wall_clamp(x.x + c.x, e, 0, g);
+                x.y = wall_clamp(x.y + c.y, e, 1, g);
+                x.z = wall_clamp(x.z + c.z, e, 2, g);
+                P[i] = x;
+            }
+            __syncwarp();
+        }
+        // apply_contact_corrections (flexible).
+        for (int i = lane; i < n; i += 32) {
+            float4 x = P[i];
+            float step = 0.0f;
+            if (x.w == 0.0f) {
+                float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+                if (i > 0) {
+                    float4 c1 = w.corr[2 * (size_t)(s0 + i - 1) + 1];
+                    cx += c1.x;
+                    cy += c1.y;
+                    cz += c1.z;
+                }
+                if (i + 1 < n) {
+                    float4 c0 = w.corr[2 * (size_t)(s0 + i)];
+                    cx += c0.x;
+                    cy += c0.y;
+                    cz += c0.z;
+                }
+                float length = sqrtf(cx * cx + cy * cy + cz * cz);
+                if (length > sp.max_step) {
+                    float scale = sp.max_step / length;
+                    cx *= scale;
+                    cy *= scale;
+                    cz *= scale;
+                }
+                float e = St[i].w;
+                x.x = wall_clamp(x.x + cx, e, 0, g);
+                x.y = wall_clamp(x.y + cy, e, 1, g);
+                x.z = wall_clamp(x.z + cz, e, 2, g);
+                P[i] = x;
+                step = sqrtf(cx * cx + cy * cy + cz * cz);
+            }
+            w.vertex_step[v0 + i] = step;
+            smax = max(smax, __float_as_uint(fmaxf(step, 0.0f)));
+        }
+        __syncwarp();
+        // project_fiber_curvature_in_place: forward then backward Gauss-Seidel
+        // sweeps. Lanes test 32 consecutive triplets on the current
+        // positions; every triplet before the first acting one is a no-op in
+        // the serial order, so applying that one and resuming right after it
+        // reproduces the serial sweep exactly.
+        if (n >= 3) {
+            const int last = n - 3;  // triplets t = 0..last: (t, t+1, t+2)
+            for (uint32_t sweep = 0; sweep < sp.curvature_cleanup_sweeps; ++sweep) {
+                int t0 = 0;
+                while (t0 <= last) {
+                    int t = t0 + lane;
+                    Triplet tr;
+                    bool act = t <= last &&
+                               curvature_triplet_test(P, St, t, t + 1, t + 2, sp.curvature_limit_stiffness,
+                                                      sp.curvature_limit_safety_margin, tr);
+                    uint32_t ballot = __ballot_sync(FULL, act);
+                    if (ballot == 0) {
+                        t0 += 32;
+                        continue;
+                    }
+                    int j = __ffs(ballot) - 1;
+                    if (lane == j) curvature_triplet_apply(P, St, t, t + 1, t + 2, tr, g);
+                    __syncwarp();
+                    t0 += j + 1;
+                }
+                t0 = last;
+                while (t0 >= 0) {
+                    int t = t0 - lane;
+                    Triplet tr;
+                    bool act = t >= 0 &&
+                               curvature_triplet_test(P, St, t, t + 1, t + 2, sp.curvature_limit_stiffness,
+                                                      sp.curvature_limit_safety_margin, tr);
+                    uint32_t ballot = __ballot_sync(FULL, act);
+                    if (ballot == 0) {
+                        t0 -= 32;
+                        continue;
+                    }
+                    int j = __ffs(ballot) - 1;
+                    if (lane == j) curvature_triplet_apply(P, St, t, t + 1, t + 2, tr, g);
+                    __syncwarp();
+                    t0 -= j + 1;
+                }
+            }
+        }
+        __syncwarp();
+        // Write back; displacement check; next gate's curvature ratios;
+        // geometry records for the next contact pass.
+        for (int i = lane; i < n; i += 32) {
+            float4 x = P[i];
+            float4 out = make_float4(x.x, x.y, x.z, 0.0f);
+            w.pos[v0 + i] = out;
+            float4 r = w.ref_pos[v0 + i];
+            float dx = x.x - r.x, dy = x.y - r.y, dz = x.z - r.z;
+            if (dx * dx + dy * dy + dz * dz > md * md) far = true;
+            if (i > 0 && i + 1 < n) {
+                float maximum = St[i].x;
+                if (maximum > 0.0f) {
+                    float ratio = curvature_ratio_at([&](int k) { return P[k]; }, i, maximum);
+                    cmax = max(cmax, __float_as_uint(fmaxf(ratio, 0.0f)));
+                }
+            }
+            if (i + 1 < n) {
+                float4 y = P[i + 1];
+                w.geom[2 * (size_t)(s0 + i)] = make_float4(x.x, x.y, x.z, radius);
+                w.geom[2 * (size_t)(s0 + i) + 1] = make_float4(y.x, y.y, y.z, __uint_as_float(v0 + i));
+            }
+        }
+        __syncwarp();
+    }
+    smax = warp_max_u32(smax);
+    cmax = warp_max_u32(cmax);
+    bool any_far = __any_sync(FULL, far);
+    if (lane == 0) {
+        if (smax) atomicMax(&w.ctl->acc[1], smax);
+        if (cmax) atomicMax(&w.ctl->acc[2], cmax);
+        if (any_far) w.ctl->neighbor_state[0] = 1;
+    }
+}
+
+// ---------------------------------------------------------------- host copies
+
+__global__ void positions_from_stage_kernel(WorldDev w) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x)
+        w.pos[v] = make_float4(w.xyz_stage[3 * (size_t)v], w.xyz_stage[3 * (size_t)v + 1],
+                               w.xyz_stage[3 * (size_t)v + 2], 0.0f);
+}
+
+__global__ void refresh_geometry_kernel(WorldDev w) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < w.S; s += gridDim.x * blockDim.x) {
+        uint32_t v0 = w.seg_v0[s];
+        float4 a = w.pos[v0], b = w.pos[v0 + 1];
+        w.geom[2 * (size_t)s] = make_float4(a.x, a.y, a.z, w.seg_static[s].x);
+        w.geom[2 * (size_t)s + 1] = make_float4(b.x, b.y, b.z, __uint_as_float(v0));
+    }
+}
+
+__global__ void positions_to_stage_kernel(WorldDev w) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x) {
+        float4 p = w.pos[v];
+        w.xyz_stage[3 * (size_t)v] = p.x;
+        w.xyz_stage[3 * (size_t)v + 1] = p.y;
+        w.xyz_stage[3 * (size_t)v + 2] = p.z;
+    }
+}
+
+__global__ void corrections_to_stage_kernel(WorldDev w, float *corr6, float *pen) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < w.S; s += gridDim.x * blockDim.x) {
+        float4 a = w.corr[2 * (size_t)s], b = w.corr[2 * (size_t)s + 1];
+        corr6[6 * (size_t)s] = a.x;
+        corr6[6 * (size_t)s + 1] = a.y;
+        corr6[6 * (size_t)s + 2] = a.z;
+        corr6[6 * (size_t)s + 3] = b.x;
+        corr6[6 * (size_t)s + 4] = b.y;
+        corr6[6 * (size_t)s + 5] = b.z;
+        pen[s] = a.w;
+    }
+}
+
+int grid_for(uint64_t n, int threads, int cap) {
+    uint64_t blocks = (n + threads - 1) / threads;
+    if (blocks < 1) blocks = 1;
+    if (blocks > (uint64_t)cap) blocks = cap;
+    return (int)blocks;
+}
+
+}  // namespace
+
+void plan_launches(const WorldDev &w, LaunchPlan &lp) {
+    int device = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&lp.num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (lp.num_sms <= 0) lp.num_sms = 148;
+    if (lp.contact_group != 8 && lp.contact_group != 16 && lp.contact_group != 32) lp.contact_group = 8;
+    lp.contact_blocks = grid_for((uint64_t)w.S * lp.contact_group, 256, lp.num_sms * 32);
+    // Update kernel: as many warps per block as fit 96 KB of staged fibers.
+    size_t per_warp = (size_t)3 * w.max_fiber * sizeof(float4);
+    int warps = 8;
+    while (warps > 1 && per_warp * warps > 96 * 1024) warps >>= 1;
+    lp.fiber_warps = warps;
+    lp.fiber_smem = per_warp * warps;
+    lp.fiber_blocks = grid_for(w.F, warps, 1 << 20);
+    lp.build_ch = 1536;
+    lp.build_smem = (size_t)lp.build_ch * 2 * sizeof(float4);
+    int sw = 8;
+    while (sw > 1 && (size_t)sw * w.block * 4 > 96 * 1024) sw >>= 1;
+    lp.sort_warps = sw;
+    lp.sort_smem = (size_t)sw * w.block * 4;
+    cudaFuncSetAttribute(fiber_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(lp.fiber_smem, 1));
+    cudaFuncSetAttribute(rb_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.build_smem);
+    cudaFuncSetAttribute(rb_sort_lists_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(lp.sort_smem, 1));
+}
+
+int launch_begin_batch(const WorldDev &w, cudaStream_t st) {
+    begin_batch_kernel<<<1, 1, 0, st>>>(w.ctl);
+    return 1;
+}
+
+int launch_flag_displacement(const WorldDev &w, cudaStream_t st) {
+    flag_displacement_kernel<<<grid_for(w.V, 256, 1 << 30), 256, 0, st>>>(w);
+    return 1;
+}
+
+int launch_measure_start(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
+    measure_start_kernel<<<grid_for(w.F, 8, lp.num_sms * 16), 256, 0, st>>>(w);
+    return 1;
+}
+
+int launch_request_rebuild(const WorldDev &w, cudaStream_t st) {
+    request_rebuild_kernel<<<1, 1, 0, st>>>(w.ctl);
+    return 1;
+}
+
+int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
+    const int cap = lp.num_sms * 16;
+    rb_clear_kernel<<<grid_for(w.C, 256, cap), 256, 0, st>>>(w);
+    rb_count_kernel<<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
+    rb_scan_kernel<<<1, 1024, 0, st>>>(w);
+    rb_scatter_kernel<<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
+    rb_sort_cells_kernel<<<grid_for(w.C, 8, cap), 256, 8 * CELL_SORT_CAP * sizeof(uint32_t), st>>>(w);
+    rb_gather_kernel<<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
+    rb_build_kernel<<<(int)std::min<uint64_t>(w.C, (uint64_t)lp.num_sms * 64), 256, lp.build_smem, st>>>(w, lp.build_ch);
+    rb_sort_lists_kernel<<<grid_for(w.S, lp.sort_warps, cap), lp.sort_warps * 32, lp.sort_smem, st>>>(w);
+    rb_snapshot_kernel<<<grid_for(w.V, 256, cap), 256, 0, st>>>(w);
+    rb_finish_kernel<<<1, 1, 0, st>>>(w.ctl);
+    return 10;
+}
+
+int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, bool gate, cudaStream_t st) {
+    switch (lp.contact_group) {
+        case 32: contact_kernel<32><<<lp.contact_blocks, 256, 0, st>>>(w, sp, gate ? 1 : 0); break;
+        case 16: contact_kernel<16><<<lp.contact_blocks, 256, 0, st>>>(w, sp, gate ? 1 : 0); break;
+        default: contact_kernel<8><<<lp.contact_blocks, 256, 0, st>>>(w, sp, gate ? 1 : 0); break;
+    }
+    return 1;
+}
+
+int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st) {
+    fiber_kernel<<<lp.fiber_blocks, lp.fiber_warps * 32, lp.fiber_smem, st>>>(w, sp);
+    return 1;
+}
+
+int launch_positions_from_stage(const WorldDev &w, cudaStream_t st) {
+    positions_from_stage_kernel<<<grid_for(w.V, 256, 1 << 16), 256, 0, st>>>(w);
+    refresh_geometry_kernel<<<grid_for(w.S, 256, 1 << 16), 256, 0, st>>>(w);
+    return 2;
+}
+
+int launch_positions_to_stage(const WorldDev &w, cudaStream_t st) {
+    positions_to_stage_kernel<<<grid_for(w.V, 256, 1 << 16), 256, 0, st>>>(w);
+    return 1;
+}
+
+int launch_corrections_to_stage(const WorldDev &w, float *corr6, float *pen, cudaStream_t st) {
+    corrections_to_stage_kernel<<<grid_for(w.S, 256, 1 << 16), 256, 0, st>>>(w, corr6, pen);
+    return 1;
+}
+
+}  // namespace tgl

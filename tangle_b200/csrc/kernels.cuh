@@ -1,0 +1,88 @@
+// kernels.cuh -- device buffers of one relaxation world and the launch
+// entry points of its kernels (kernels.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace tgl {
+
+// Every device pointer and size a kernel needs, passed by value.
+struct WorldDev {
+    uint32_t V, S, F, C;
+    uint32_t block;      // neighbor slots per segment list
+    uint32_t max_fiber;  // most vertices in one fiber
+    float skin;          // neighbor skin
+    Grid grid;
+    // Static, uploaded once.
+    const float4 *seg_static;   // [S] radius, arc(first vertex), arc(second vertex), fiber bits
+    const uint32_t *seg_v0;     // [S] first vertex (second = first + 1)
+    const uint2 *fiber_vspan;   // [F] first vertex, vertex count
+    const uint32_t *fiber_s0;   // [F] first segment
+    const float4 *vtx_static;   // [V] max curvature, rest chord to v-2, rest chord to v+2, wall extent
+    const uint32_t *pinned;     // [V]
+    const float *rest;          // [S] rest lengths
+    // Resident state.
+    float4 *pos;      // [V] xyz, w = 0
+    float4 *ref_pos;  // [V] positions the lists were built from
+    float4 *geom;     // [2S] {first xyz, radius}, {second xyz, first-vertex bits}
+    float4 *corr;     // [2S] {end-0 correction, max penetration}, {end-1 correction, 0}
+    float *vertex_step; // [V]
+    // Cell list.
+    uint32_t *cell_counts;   // [C]
+    uint32_t *cell_offsets;  // [C]
+    uint32_t *cell_segments; // [S] segment per slot, cell order
+    uint32_t *cell_of;       // [S] cell of each segment
+    uint32_t *ticket;        // [S] scatter position inside its cell; sort scratch
+    float4 *slot_geom;       // [2S] geometry in slot order, w of the second = segment bits
+    // Verlet lists.
+    uint32_t *nbr_count; // [S] true neighbor count
+    uint32_t *nbr_list;  // [S * block]
+    Control *ctl;
+    float *xyz_stage;    // [3V] interleaved staging for host copies
+};
+
+struct StepParams {
+    float penetration_tolerance;
+    float correction_fraction;
+    float stretch_stiffness;
+    float bend_stiffness;
+    float curvature_limit_stiffness;
+    float curvature_limit_safety_margin;
+    float curvature_ratio_tolerance;
+    float max_step;
+    uint32_t constraint_iterations;
+    uint32_t curvature_cleanup_sweeps;
+    uint32_t contact_aggregation;
+    uint32_t force_full_iterations;
+    uint32_t max_iterations;  // the batch size: the gate stops at this many
+};
+
+// Launch plans, fixed per world.
+struct LaunchPlan {
+    int num_sms;
+    int contact_group;      // lanes per segment in the contact pass (8, 16 or 32)
+    int contact_blocks;
+    int fiber_warps;        // fibers per block of the update kernel
+    int fiber_blocks;
+    size_t fiber_smem;
+    int build_ch;           // candidate slots staged per build chunk
+    size_t build_smem;
+    int sort_warps;
+    size_t sort_smem;
+};
+
+// Each launcher returns the number of kernels it enqueued.
+int launch_begin_batch(const WorldDev &w, cudaStream_t st);
+int launch_flag_displacement(const WorldDev &w, cudaStream_t st);
+int launch_measure_start(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
+int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
+int launch_request_rebuild(const WorldDev &w, cudaStream_t st);
+int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, bool gate, cudaStream_t st);
+int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st);
+int launch_positions_from_stage(const WorldDev &w, cudaStream_t st);
+int launch_positions_to_stage(const WorldDev &w, cudaStream_t st);
+int launch_corrections_to_stage(const WorldDev &w, float *corr6, float *pen, cudaStream_t st);
+
+void plan_launches(const WorldDev &w, LaunchPlan &lp);
+
+}  // namespace tgl

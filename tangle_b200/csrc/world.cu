@@ -1,0 +1,590 @@
+// world.cu -- the resident relaxation world behind the C ABI of
+// include/tangle_cuda.h: upload and grid sizing
+// (crates/tangle_relax/src/device/world.rs:308-690, :874-917), batches
+// (run_batch, world.rs:1020-1505) replayed from captured CUDA graphs, and
+// the single status readback (read_status, world.rs:2337-2369).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/tangle_cuda.h"
+#include "kernels.cuh"
+
+using namespace tgl;
+
+namespace {
+
+thread_local std::string g_error;
+constexpr uint64_t REFERENCE_MAX_LIST_BYTES = 120ull << 20;  // world.rs:36
+
+int set_error(int code, const std::string &message) {
+    g_error = message;
+    return code;
+}
+
+#define TGL_CUDA(call)                                                                               \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return set_error(TGL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));       \
+    } while (0)
+
+uint32_t f32_to_u32_host(float x) {
+    if (x != x || x <= 0.0f) return 0;
+    if (x >= 4294967296.0f) return 0xFFFFFFFFu;
+    return (uint32_t)x;
+}
+
+struct GraphKey {
+    uint32_t iterations;
+    StepParams sp;
+    bool operator<(const GraphKey &o) const {
+        if (iterations != o.iterations) return iterations < o.iterations;
+        return std::memcmp(&sp, &o.sp, sizeof(StepParams)) < 0;
+    }
+};
+
+struct GraphEntry {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;
+    uint32_t iterations = 0;
+    // With kernel timing on: four events per step (before the rebuild,
+    // before the contact pass, before the fiber update, after it).
+    std::vector<cudaEvent_t> events;
+};
+
+void destroy_entry(GraphEntry &e) {
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+    if (e.graph) cudaGraphDestroy(e.graph);
+    for (cudaEvent_t ev : e.events) cudaEventDestroy(ev);
+    e.exec = nullptr;
+    e.graph = nullptr;
+    e.events.clear();
+}
+
+}  // namespace
+
+struct tgl_world {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    WorldDev dev{};
+    LaunchPlan lp{};
+    float cell_size = 0.0f;
+    uint64_t neighbor_slots = 0;
+    Control *host_ctl = nullptr;  // pinned
+    std::vector<void *> allocations;
+    std::map<GraphKey, GraphEntry> graphs;
+    uint64_t launches = 0;
+    bool timing = false;
+    const GraphEntry *last = nullptr;  // graph of the last batch
+    uint64_t last_batch_iterations = 0;
+
+    ~tgl_world() {
+        for (auto &kv : graphs) destroy_entry(kv.second);
+        for (void *p : allocations) cudaFree(p);
+        if (host_ctl) cudaFreeHost(host_ctl);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <typename T>
+    int alloc(T **out, size_t count) {
+        void *p = nullptr;
+        size_t bytes = count * sizeof(T);
+        if (bytes == 0) bytes = sizeof(T);
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess)
+            return set_error(TGL_ERR_MEMORY, std::string("cudaMalloc of ") + std::to_string(bytes) +
+                                                 " bytes failed: " + cudaGetErrorString(e));
+        allocations.push_back(p);
+        *out = (T *)p;
+        return 0;
+    }
+
+    template <typename T>
+    int upload(T **out, const std::vector<T> &host) {
+        if (int rc = alloc(out, host.size())) return rc;
+        if (!host.empty()) TGL_CUDA(cudaMemcpy(*out, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return 0;
+    }
+};
+
+namespace {
+
+StepParams step_params(const tgl_relax_config &c, uint32_t iterations) {
+    StepParams sp{};
+    sp.penetration_tolerance = c.penetration_tolerance;
+    sp.correction_fraction = c.correction_fraction;
+    sp.stretch_stiffness = c.stretch_stiffness;
+    sp.bend_stiffness = c.bend_stiffness;
+    sp.curvature_limit_stiffness = c.curvature_limit_stiffness;
+    sp.curvature_limit_safety_margin = c.curvature_limit_safety_margin;
+    sp.curvature_ratio_tolerance = c.curvature_ratio_tolerance;
+    sp.max_step = c.max_step;
+    sp.constraint_iterations = c.constraint_iterations;
+    sp.curvature_cleanup_sweeps = c.curvature_cleanup_sweeps;
+    sp.contact_aggregation = c.contact_aggregation;
+    sp.force_full_iterations = c.force_full_iterations ? 1u : 0u;
+    sp.max_iterations = iterations;
+    return sp;
+}
+
+// plugin.rs:951-983 assertions on the solver configuration.
+int validate_config(const tgl_relax_config &c) {
+    if (!(c.penetration_tolerance >= 0.0f)) return set_error(TGL_ERR_INVALID, "penetration_tolerance must be non-negative");
+    if (!(c.correction_fraction > 0.0f && c.correction_fraction <= 1.0f))
+        return set_error(TGL_ERR_INVALID, "correction_fraction must be in (0, 1]");
+    if (!(c.stretch_stiffness >= 0.0f && c.stretch_stiffness <= 1.0f))
+        return set_error(TGL_ERR_INVALID, "stretch_stiffness must be in [0, 1]");
+    if (!(c.bend_stiffness >= 0.0f && c.bend_stiffness <= 1.0f))
+        return set_error(TGL_ERR_INVALID, "bend_stiffness must be in [0, 1]");
+    if (!(c.curvature_limit_stiffness >= 0.0f && c.curvature_limit_stiffness <= 1.0f))
+        return set_error(TGL_ERR_INVALID, "curvature_limit_stiffness must be in [0, 1]");
+    if (!(c.curvature_limit_safety_margin >= 0.0f && c.curvature_limit_safety_margin < 0.1f))
+        return set_error(TGL_ERR_INVALID, "curvature_limit_safety_margin must be in [0, 0.1)");
+    if (!(c.curvature_ratio_tolerance >= 0.0f)) return set_error(TGL_ERR_INVALID, "curvature_ratio_tolerance must be non-negative");
+    if (c.constraint_iterations == 0) return set_error(TGL_ERR_INVALID, "constraint_iterations must be positive");
+    if (c.curvature_cleanup_sweeps == 0) return set_error(TGL_ERR_INVALID, "curvature_cleanup_sweeps must be positive");
+    if (!(c.max_step > 0.0f)) return set_error(TGL_ERR_INVALID, "max_step must be positive");
+    if (c.contact_aggregation > 2) return set_error(TGL_ERR_INVALID, "contact_aggregation must be 0, 1 or 2");
+    return 0;
+}
+
+// run_batch's launch sequence (world.rs:1020-1505): begin, displacement
+// check, then iterations + 1 steps of [rebuild if flagged, contact pass with
+// the gate, fiber update]; kernels after the gate return at once once it
+// has stopped the batch.
+int enqueue_batch(tgl_world *w, const StepParams &sp, uint32_t iterations, std::vector<cudaEvent_t> *events) {
+    int kernels = 0;
+    kernels += launch_begin_batch(w->dev, w->stream);
+    kernels += launch_flag_displacement(w->dev, w->stream);
+    kernels += launch_measure_start(w->dev, w->lp, w->stream);
+    for (uint32_t step = 0; step <= iterations; ++step) {
+        if (events) cudaEventRecordWithFlags((*events)[4 * step], w->stream, cudaEventRecordExternal);
+        kernels += launch_rebuild(w->dev, w->lp, w->stream);
+        if (events) cudaEventRecordWithFlags((*events)[4 * step + 1], w->stream, cudaEventRecordExternal);
+        kernels += launch_contact(w->dev, w->lp, sp, true, w->stream);
+        if (events) cudaEventRecordWithFlags((*events)[4 * step + 2], w->stream, cudaEventRecordExternal);
+        kernels += launch_fiber_update(w->dev, w->lp, sp, w->stream);
+        if (events) cudaEventRecordWithFlags((*events)[4 * step + 3], w->stream, cudaEventRecordExternal);
+    }
+    return kernels;
+}
+
+int read_status(tgl_world *w, const tgl_relax_config &c, tgl_batch_status *status) {
+    TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    const Control &h = *w->host_ctl;
+    bool overflow = h.cell_overflow != 0 || h.control[3] != 0;
+    status->total_iterations = h.control[1];
+    status->batch_iterations = h.control[2];
+    status->max_penetration = h.metrics[0];
+    status->max_displacement = h.metrics[1];
+    status->max_curvature_ratio = h.metrics[2];
+    status->converged = (!c.force_full_iterations && h.metrics[0] <= c.penetration_tolerance &&
+                         h.metrics[2] <= 1.0f + c.curvature_ratio_tolerance && !overflow)
+                            ? 1u
+                            : 0u;
+    status->cell_list_overflow = overflow ? 1u : 0u;
+    status->reserved = 0;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *tgl_last_error(void) { return g_error.c_str(); }
+
+int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float max_step, tgl_world **out) {
+    if (!pk || !cl || !out) return set_error(TGL_ERR_INVALID, "null argument");
+    *out = nullptr;
+    const uint32_t V = pk->vertex_count, S = pk->segment_count, F = pk->fiber_count;
+    // world.rs:314-319 upload assertions.
+    if (S == 0 || F == 0) return set_error(TGL_ERR_INVALID, "assembly has no segments or fibers");
+    if (!(cl->cell_size_scale >= 1.0f)) return set_error(TGL_ERR_INVALID, "cell_size_scale must be at least 1");
+    if (!(std::isfinite(cl->neighbor_skin_scale) && cl->neighbor_skin_scale >= 0.0f))
+        return set_error(TGL_ERR_INVALID, "neighbor_skin_scale must be finite and non-negative");
+    if (cl->neighbor_capacity == 0) return set_error(TGL_ERR_INVALID, "neighbor_capacity must be positive");
+    if (!(max_step > 0.0f)) return set_error(TGL_ERR_INVALID, "max_step must be positive");
+    if (!pk->positions || !pk->intrinsic_positions || !pk->segment_vertices || !pk->segment_fibers ||
+        !pk->segment_radii || !pk->segment_rest_lengths || !pk->fiber_vertex_spans || !pk->fiber_segment_spans ||
+        !pk->vertex_segments || !pk->vertex_max_curvature)
+        return set_error(TGL_ERR_INVALID, "a required packed array is null");
+    for (int a = 0; a < 3; ++a)
+        if (!(std::isfinite(pk->cell_lower[a]) && std::isfinite(pk->cell_upper[a]) && pk->cell_upper[a] > pk->cell_lower[a]))
+            return set_error(TGL_ERR_INVALID, "cell bounds must be finite with upper > lower");
+    // The layout the reference's packing produces (packed.rs:200-248).
+    uint64_t vsum = 0, ssum = 0;
+    uint32_t max_fiber = 0;
+    for (uint32_t f = 0; f < F; ++f) {
+        uint32_t v0 = pk->fiber_vertex_spans[2 * f], n = pk->fiber_vertex_spans[2 * f + 1];
+        uint32_t s0 = pk->fiber_segment_spans[2 * f], m = pk->fiber_segment_spans[2 * f + 1];
+        if (n < 2 || m != n - 1 || (uint64_t)v0 + n > V || (uint64_t)s0 + m > S)
+            return set_error(TGL_ERR_INVALID, "fiber " + std::to_string(f) + " has an invalid vertex or segment span");
+        for (uint32_t k = 0; k < m; ++k) {
+            uint32_t s = s0 + k;
+            if (pk->segment_vertices[2 * s] != v0 + k || pk->segment_vertices[2 * s + 1] != v0 + k + 1 ||
+                pk->segment_fibers[s] != f)
+                return set_error(TGL_ERR_INVALID, "segment " + std::to_string(s) +
+                                                      " is not packed as its fiber's consecutive vertex pair");
+        }
+        for (uint32_t k = 0; k < n; ++k) {
+            uint32_t v = v0 + k;
+            uint32_t prev = k > 0 ? s0 + k - 1 : TGL_NONE, next = k + 1 < n ? s0 + k : TGL_NONE;
+            if (pk->vertex_segments[2 * v] != prev || pk->vertex_segments[2 * v + 1] != next)
+                return set_error(TGL_ERR_INVALID, "vertex_segments disagrees with the fiber packing at vertex " +
+                                                      std::to_string(v));
+        }
+        vsum += n;
+        ssum += m;
+        if (n > max_fiber) max_fiber = n;
+    }
+    if (vsum != V || ssum != S) return set_error(TGL_ERR_INVALID, "fiber spans do not cover every vertex and segment once");
+    for (uint64_t i = 0; i < 3ull * V; ++i)
+        if (!std::isfinite(pk->positions[i]) || !std::isfinite(pk->intrinsic_positions[i]))
+            return set_error(TGL_ERR_INVALID, "positions must be finite");
+    for (uint32_t s = 0; s < S; ++s)
+        if (!(pk->segment_radii[s] > 0.0f) || !std::isfinite(pk->segment_radii[s]) || !std::isfinite(pk->segment_rest_lengths[s]))
+            return set_error(TGL_ERR_INVALID, "segment radii must be positive and finite");
+    if ((size_t)max_fiber * 3 * sizeof(float4) > 200 * 1024)
+        return set_error(TGL_ERR_UNSUPPORTED, "a fiber has more vertices than one warp can stage in shared memory");
+
+    int device_count = 0;
+    if (cudaGetDeviceCount(&device_count) != cudaSuccess || device_count == 0)
+        return set_error(TGL_ERR_NO_DEVICE, "no CUDA device");
+
+    tgl_world *w = new tgl_world();
+    auto fail = [&](int rc) {
+        delete w;
+        return rc;
+    };
+    cudaGetDevice(&w->device);
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, w->device);
+    if (prop.major < 10) return fail(set_error(TGL_ERR_NO_DEVICE, "the relaxation kernels are built for sm_100a"));
+    if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(set_error(TGL_ERR_CUDA, "cudaStreamCreate failed"));
+    if (cudaMallocHost(&w->host_ctl, sizeof(Control)) != cudaSuccess)
+        return fail(set_error(TGL_ERR_MEMORY, "cudaMallocHost failed"));
+
+    // ---- world.rs:321-417: grid sizing for a uniform layout, in f32.
+    const float *P = pk->positions;
+    float maximum_rest_length = 0.0f, maximum_initial_length = 0.0f, maximum_radius = 0.0f;
+    for (uint32_t s = 0; s < S; ++s) {
+        maximum_rest_length = std::fmax(maximum_rest_length, pk->segment_rest_lengths[s]);
+        uint32_t a = pk->segment_vertices[2 * s], b = pk->segment_vertices[2 * s + 1];
+        float dx = P[3 * b] - P[3 * a], dy = P[3 * b + 1] - P[3 * a + 1], dz = P[3 * b + 2] - P[3 * a + 2];
+        maximum_initial_length = std::fmax(maximum_initial_length, std::sqrt(dx * dx + dy * dy + dz * dz));
+        maximum_radius = std::fmax(maximum_radius, pk->segment_radii[s]);
+    }
+    float maximum_length = std::fmax(maximum_rest_length, maximum_initial_length);
+    float skin = cl->neighbor_skin_scale * maximum_radius;
+    float interaction_margin = 2.0f * maximum_radius + std::fmax(2.0f * max_step, skin);
+    // Every segment is a leaf: one proxy piece and list weight 1 each.
+    float piece_length = std::fmin(maximum_length, std::fmax(maximum_length, 2.0f * interaction_margin));
+    w->cell_size = (piece_length + interaction_margin) * cl->cell_size_scale;
+    Grid grid{};
+    uint64_t C = 1;
+    for (int a = 0; a < 3; ++a) {
+        grid.lower[a] = pk->cell_lower[a];
+        grid.upper[a] = pk->cell_upper[a];
+        grid.periodic[a] = pk->cell_periodic[a] ? 1u : 0u;
+        float extent = pk->cell_upper[a] - pk->cell_lower[a];
+        grid.cells[a] = f32_to_u32_host(std::fmax(std::floor(extent / w->cell_size), 1.0f));
+        grid.length[a] = extent;
+        grid.width[a] = extent / (float)grid.cells[a];
+        C *= grid.cells[a];
+    }
+    if (C > (1ull << 31)) return fail(set_error(TGL_ERR_UNSUPPORTED, "cell grid too large: the cell size is tiny against the box"));
+    // world.rs:476-509 and :874-917: list room and the byte cap.
+    uint64_t max_bytes = cl->max_list_bytes ? cl->max_list_bytes : REFERENCE_MAX_LIST_BYTES;
+    uint64_t slots = std::min<uint64_t>((uint64_t)cl->neighbor_capacity * S, max_bytes / 4);
+    w->neighbor_slots = std::max<uint64_t>(slots, 1);
+    uint32_t block = (uint32_t)std::min<uint64_t>(cl->neighbor_capacity, std::min<uint64_t>(w->neighbor_slots / S, 0xFFFFFFFFull));
+
+    // ---- static per-segment and per-vertex data.
+    std::vector<float> arc(V, 0.0f);  // packed.rs:561-580
+    std::vector<float4> vtx_static(V);
+    std::vector<uint32_t> pinned(V, 0);
+    std::vector<uint2> fiber_vspan(F);
+    std::vector<uint32_t> fiber_s0(F);
+    const float *X = pk->intrinsic_positions;
+    for (uint32_t f = 0; f < F; ++f) {
+        uint32_t v0 = pk->fiber_vertex_spans[2 * f], n = pk->fiber_vertex_spans[2 * f + 1];
+        fiber_vspan[f] = make_uint2(v0, n);
+        fiber_s0[f] = pk->fiber_segment_spans[2 * f];
+        double total = 0.0;
+        for (uint32_t v = v0 + 1; v < v0 + n; ++v) {
+            double sum = 0.0;
+            for (int a = 0; a < 3; ++a) {
+                double delta = (double)X[3 * (size_t)v + a] - (double)X[3 * (size_t)(v - 1) + a];
+                sum += delta * delta;
+            }
+            total += std::sqrt(sum);
+            arc[v] = (float)total;
+        }
+        float radius = pk->segment_radii[fiber_s0[f]];  // packed.rs:527-546
+        for (uint32_t k = 0; k < n; ++k) {
+            uint32_t v = v0 + k;
+            // Rest chords to the second neighbors (kernels.rs:1118-1121,
+            // :1149-1152), rounded exactly as the kernel computes them.
+            float chord_prev = 0.0f, chord_next = 0.0f;
+            if (k >= 2) {
+                uint32_t o = v - 2;
+                float rx = X[3 * o] - X[3 * v], ry = X[3 * o + 1] - X[3 * v + 1], rz = X[3 * o + 2] - X[3 * v + 2];
+                chord_prev = std::sqrt(rx * rx + ry * ry + rz * rz);
+            }
+            if (k + 2 < n) {
+                uint32_t o = v + 2;
+                float rx = X[3 * o] - X[3 * v], ry = X[3 * o + 1] - X[3 * v + 1], rz = X[3 * o + 2] - X[3 * v + 2];
+                chord_next = std::sqrt(rx * rx + ry * ry + rz * rz);
+            }
+            vtx_static[v] = make_float4(pk->vertex_max_curvature[v], chord_prev, chord_next, radius);
+            pinned[v] = pk->vertex_pinned && pk->vertex_pinned[v] ? 1u : 0u;
+        }
+    }
+    std::vector<float4> seg_static(S);
+    std::vector<uint32_t> seg_v0(S);
+    std::vector<float> rest(pk->segment_rest_lengths, pk->segment_rest_lengths + S);
+    std::vector<float4> geom(2 * (size_t)S);
+    for (uint32_t s = 0; s < S; ++s) {
+        uint32_t a = pk->segment_vertices[2 * s], b = pk->segment_vertices[2 * s + 1];
+        uint32_t fiber = pk->segment_fibers[s];
+        float fb;
+        std::memcpy(&fb, &fiber, 4);
+        seg_static[s] = make_float4(pk->segment_radii[s], arc[a], arc[b], fb);
+        seg_v0[s] = a;
+        float ab;
+        std::memcpy(&ab, &a, 4);
+        geom[2 * (size_t)s] = make_float4(P[3 * a], P[3 * a + 1], P[3 * a + 2], pk->segment_radii[s]);
+        geom[2 * (size_t)s + 1] = make_float4(P[3 * b], P[3 * b + 1], P[3 * b + 2], ab);
+    }
+    std::vector<float4> pos(V);
+    for (uint32_t v = 0; v < V; ++v) pos[v] = make_float4(P[3 * v], P[3 * v + 1], P[3 * v + 2], 0.0f);
+
+    WorldDev &d = w->dev;
+    d.V = V;
+    d.S = S;
+    d.F = F;
+    d.C = (uint32_t)C;
+    d.block = block;
+    d.max_fiber = max_fiber;
+    d.skin = skin;
+    d.grid = grid;
+    int rc = 0;
+    float4 *seg_static_d, *vtx_static_d;
+    uint32_t *seg_v0_d, *fiber_s0_d, *pinned_d;
+    uint2 *fiber_vspan_d;
+    float *rest_d;
+    if ((rc = w->upload(&seg_static_d, seg_static)) || (rc = w->upload(&seg_v0_d, seg_v0)) ||
+        (rc = w->upload(&fiber_vspan_d, fiber_vspan)) || (rc = w->upload(&fiber_s0_d, fiber_s0)) ||
+        (rc = w->upload(&vtx_static_d, vtx_static)) || (rc = w->upload(&pinned_d, pinned)) ||
+        (rc = w->upload(&rest_d, rest)) || (rc = w->upload(&d.pos, pos)) || (rc = w->upload(&d.ref_pos, pos)) ||
+        (rc = w->upload(&d.geom, geom)) || (rc = w->alloc(&d.corr, 2 * (size_t)S)) ||
+        (rc = w->alloc(&d.vertex_step, V)) || (rc = w->alloc(&d.cell_counts, C)) ||
+        (rc = w->alloc(&d.cell_offsets, C)) || (rc = w->alloc(&d.cell_segments, S)) ||
+        (rc = w->alloc(&d.cell_of, S)) || (rc = w->alloc(&d.ticket, S)) ||
+        (rc = w->alloc(&d.slot_geom, 2 * (size_t)S)) || (rc = w->alloc(&d.nbr_count, S)) ||
+        (rc = w->alloc(&d.nbr_list, std::max<uint64_t>((uint64_t)S * block, 1))) || (rc = w->alloc(&d.ctl, 1)) ||
+        (rc = w->alloc(&d.xyz_stage, 3 * (size_t)V)))
+        return fail(rc);
+    d.seg_static = seg_static_d;
+    d.seg_v0 = seg_v0_d;
+    d.fiber_vspan = fiber_vspan_d;
+    d.fiber_s0 = fiber_s0_d;
+    d.vtx_static = vtx_static_d;
+    d.pinned = pinned_d;
+    d.rest = rest_d;
+    Control ctl{};
+    ctl.metrics[0] = INFINITY;  // world.rs:470
+    ctl.metrics[1] = 0.0f;
+    ctl.metrics[2] = INFINITY;
+    ctl.neighbor_state[0] = 1;  // lists start stale (world.rs:516-517)
+    if (cudaMemcpy(d.ctl, &ctl, sizeof(Control), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(d.corr, 0, 2 * (size_t)S * sizeof(float4)) != cudaSuccess ||
+        cudaMemset(d.vertex_step, 0, V * sizeof(float)) != cudaSuccess ||
+        cudaMemset(d.cell_counts, 0, C * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMemset(d.cell_offsets, 0, C * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMemset(d.nbr_count, 0, S * sizeof(uint32_t)) != cudaSuccess)
+        return fail(set_error(TGL_ERR_CUDA, "device initialisation failed"));
+    plan_launches(d, w->lp);
+    *out = w;
+    return 0;
+}
+
+void tgl_world_destroy(tgl_world *w) { delete w; }
+
+int tgl_run_batch(tgl_world *w, const tgl_relax_config *config, uint32_t iterations, tgl_batch_status *status) {
+    if (!w || !config || !status) return set_error(TGL_ERR_INVALID, "null argument");
+    if (iterations == 0) return set_error(TGL_ERR_INVALID, "iterations must be positive");  // world.rs:1021
+    if (int rc = validate_config(*config)) return rc;
+    StepParams sp = step_params(*config, iterations);
+    GraphKey key{iterations, sp};
+    auto it = w->graphs.find(key);
+    if (it == w->graphs.end()) {
+        GraphEntry entry;
+        entry.iterations = iterations;
+        if (w->timing) {
+            entry.events.resize(4 * ((size_t)iterations + 1));
+            for (cudaEvent_t &ev : entry.events)
+                if (cudaEventCreate(&ev) != cudaSuccess) {
+                    destroy_entry(entry);
+                    return set_error(TGL_ERR_CUDA, "cudaEventCreate failed");
+                }
+        }
+        TGL_CUDA(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
+        entry.kernels = enqueue_batch(w, sp, iterations, w->timing ? &entry.events : nullptr);
+        cudaError_t e = cudaStreamEndCapture(w->stream, &entry.graph);
+        if (e != cudaSuccess) return set_error(TGL_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&entry.exec, entry.graph, 0);
+        if (e != cudaSuccess) {
+            destroy_entry(entry);
+            return set_error(TGL_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(e));
+        }
+        if (w->graphs.size() >= 16) {  // keep the cache small
+            auto old = w->graphs.begin();
+            if (&old->second == w->last) w->last = nullptr;
+            destroy_entry(old->second);
+            w->graphs.erase(old);
+        }
+        it = w->graphs.emplace(key, entry).first;
+    }
+    TGL_CUDA(cudaGraphLaunch(it->second.exec, w->stream));
+    w->launches += (uint64_t)it->second.kernels;
+    if (int rc = read_status(w, *config, status)) return rc;
+    TGL_CUDA(cudaGetLastError());
+    w->last = &it->second;
+    w->last_batch_iterations = status->batch_iterations;
+    return 0;
+}
+
+void *tgl_world_stream(const tgl_world *w) { return w ? (void *)w->stream : nullptr; }
+
+int tgl_set_kernel_timing(tgl_world *w, int enable) {
+    if (!w) return set_error(TGL_ERR_INVALID, "null argument");
+    if ((enable != 0) != w->timing) {
+        for (auto &kv : w->graphs) destroy_entry(kv.second);
+        w->graphs.clear();
+        w->last = nullptr;
+        w->timing = enable != 0;
+    }
+    return 0;
+}
+
+int tgl_last_kernel_times(tgl_world *w, tgl_kernel_times *times) {
+    if (!w || !times) return set_error(TGL_ERR_INVALID, "null argument");
+    std::memset(times, 0, sizeof(*times));
+    if (!w->last || w->last->events.empty()) return set_error(TGL_ERR_INVALID, "no timed batch: enable timing first");
+    const GraphEntry &e = *w->last;
+    uint32_t steps = e.iterations + 1;
+    uint32_t contact_passes = (uint32_t)std::min<uint64_t>(w->last_batch_iterations + 1, steps);
+    uint32_t updates = (uint32_t)std::min<uint64_t>(w->last_batch_iterations, steps);
+    for (uint32_t k = 0; k < steps; ++k) {
+        float rebuild = 0.0f, contact = 0.0f, update = 0.0f;
+        TGL_CUDA(cudaEventElapsedTime(&rebuild, e.events[4 * k], e.events[4 * k + 1]));
+        TGL_CUDA(cudaEventElapsedTime(&contact, e.events[4 * k + 1], e.events[4 * k + 2]));
+        TGL_CUDA(cudaEventElapsedTime(&update, e.events[4 * k + 2], e.events[4 * k + 3]));
+        times->rebuild_ms += rebuild;
+        if (k < contact_passes) times->contact_ms += contact;
+        if (k < updates) times->update_ms += update;
+    }
+    times->contact_passes = contact_passes;
+    times->updates = updates;
+    times->rebuilds = steps;
+    return 0;
+}
+
+int tgl_download_positions(tgl_world *w, float *xyz, size_t len) {
+    if (!w || !xyz) return set_error(TGL_ERR_INVALID, "null argument");
+    if (len != 3 * (size_t)w->dev.V) return set_error(TGL_ERR_INVALID, "position buffer has the wrong length");
+    w->launches += launch_positions_to_stage(w->dev, w->stream);
+    TGL_CUDA(cudaMemcpyAsync(xyz, w->dev.xyz_stage, len * sizeof(float), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    return 0;
+}
+
+int tgl_upload_positions(tgl_world *w, const float *xyz, size_t len) {
+    if (!w || !xyz) return set_error(TGL_ERR_INVALID, "null argument");
+    if (len != 3 * (size_t)w->dev.V) return set_error(TGL_ERR_INVALID, "position buffer has the wrong length");
+    for (size_t i = 0; i < len; ++i)
+        if (!std::isfinite(xyz[i])) return set_error(TGL_ERR_INVALID, "positions must be finite");
+    TGL_CUDA(cudaMemcpyAsync(w->dev.xyz_stage, xyz, len * sizeof(float), cudaMemcpyHostToDevice, w->stream));
+    w->launches += launch_positions_from_stage(w->dev, w->stream);
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    return 0;
+}
+
+float tgl_cell_size(const tgl_world *w) { return w ? w->cell_size : 0.0f; }
+uint64_t tgl_cell_count(const tgl_world *w) { return w ? w->dev.C : 0; }
+void tgl_cell_dims(const tgl_world *w, uint32_t dims[3]) {
+    for (int a = 0; a < 3; ++a) dims[a] = w ? w->dev.grid.cells[a] : 0;
+}
+float tgl_neighbor_skin(const tgl_world *w) { return w ? w->dev.skin : 0.0f; }
+uint32_t tgl_neighbor_block(const tgl_world *w) { return w ? w->dev.block : 0; }
+uint64_t tgl_kernel_launches(const tgl_world *w) { return w ? w->launches : 0; }
+
+int tgl_neighbor_list_rebuilds(tgl_world *w, uint32_t *rebuilds) {
+    if (!w || !rebuilds) return set_error(TGL_ERR_INVALID, "null argument");
+    TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    *rebuilds = w->host_ctl->neighbor_state[1];
+    return 0;
+}
+
+int tgl_debug_rebuild(tgl_world *w) {
+    if (!w) return set_error(TGL_ERR_INVALID, "null argument");
+    w->launches += launch_request_rebuild(w->dev, w->stream);
+    w->launches += launch_rebuild(w->dev, w->lp, w->stream);
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    TGL_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int tgl_debug_cell_list(tgl_world *w, uint32_t *cell_counts, uint32_t *cell_offsets, uint32_t *cell_segments) {
+    if (!w || !cell_counts || !cell_offsets || !cell_segments) return set_error(TGL_ERR_INVALID, "null argument");
+    TGL_CUDA(cudaMemcpyAsync(cell_counts, w->dev.cell_counts, w->dev.C * 4ull, cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaMemcpyAsync(cell_offsets, w->dev.cell_offsets, w->dev.C * 4ull, cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaMemcpyAsync(cell_segments, w->dev.cell_segments, w->dev.S * 4ull, cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    return 0;
+}
+
+int tgl_debug_neighbor_lists(tgl_world *w, uint32_t *counts, uint32_t *lists) {
+    if (!w || !counts || !lists) return set_error(TGL_ERR_INVALID, "null argument");
+    TGL_CUDA(cudaMemcpyAsync(counts, w->dev.nbr_count, w->dev.S * 4ull, cudaMemcpyDeviceToHost, w->stream));
+    size_t n = (size_t)w->dev.S * w->dev.block;
+    if (n) TGL_CUDA(cudaMemcpyAsync(lists, w->dev.nbr_list, n * 4, cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    return 0;
+}
+
+int tgl_debug_corrections(tgl_world *w, const tgl_relax_config *config, float *corrections, float *segment_max) {
+    if (!w || !config || !corrections || !segment_max) return set_error(TGL_ERR_INVALID, "null argument");
+    if (int rc = validate_config(*config)) return rc;
+    StepParams sp = step_params(*config, 1);
+    float *corr6 = nullptr, *pen = nullptr;
+    TGL_CUDA(cudaMalloc(&corr6, 6ull * w->dev.S * sizeof(float)));
+    if (cudaMalloc(&pen, (size_t)w->dev.S * sizeof(float)) != cudaSuccess) {
+        cudaFree(corr6);
+        return set_error(TGL_ERR_MEMORY, "cudaMalloc failed");
+    }
+    w->launches += launch_rebuild(w->dev, w->lp, w->stream);
+    w->launches += launch_contact(w->dev, w->lp, sp, false, w->stream);
+    w->launches += launch_corrections_to_stage(w->dev, corr6, pen, w->stream);
+    cudaMemcpyAsync(corrections, corr6, 6ull * w->dev.S * sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    cudaMemcpyAsync(segment_max, pen, (size_t)w->dev.S * sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    cudaError_t e = cudaStreamSynchronize(w->stream);
+    cudaFree(corr6);
+    cudaFree(pen);
+    if (e != cudaSuccess) return set_error(TGL_ERR_CUDA, cudaGetErrorString(e));
+    TGL_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,371 @@
+"""ctypes binding of libtangle_cuda.so: the resident relaxation world.
+
+`DeviceWorld` is the Python face of the reference's `DeviceWorld` seam
+(crates/tangle_relax/src/device/plugin.rs:309-893) for the "cuda" backend:
+`upload` (world.rs:308-690), `run_batch` (world.rs:1020-1505, returning
+`BatchStatus`), `download_positions` (world.rs:2384-2390), `cell_size` /
+`cell_count` (plugin.rs:597-636) and `neighbor_list_rebuilds`
+(world/neighbor_list.rs:167-176). Errors from the C ABI raise
+`ValueError` (invalid input) or `RuntimeError` (CUDA failure); there is no
+CPU fallback: a missing library or device raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+from .settings import BatchStatus, CellListConfig, RelaxationConfig
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtangle_cuda.so")
+_lib = None
+
+TGL_ERR_INVALID = 1
+TGL_ERR_UNSUPPORTED = 5
+
+#: Every symbol include/tangle_cuda.h declares.
+EXPORTS = (
+    "tgl_world_create", "tgl_world_destroy", "tgl_run_batch", "tgl_download_positions", "tgl_upload_positions",
+    "tgl_cell_size", "tgl_cell_count", "tgl_cell_dims", "tgl_neighbor_skin", "tgl_neighbor_block",
+    "tgl_neighbor_list_rebuilds", "tgl_debug_rebuild", "tgl_debug_cell_list", "tgl_debug_neighbor_lists",
+    "tgl_debug_corrections", "tgl_kernel_launches", "tgl_set_kernel_timing", "tgl_last_kernel_times",
+    "tgl_world_stream", "tgl_last_error",
+)
+
+
+class Packed(ctypes.Structure):
+    """tgl_packed."""
+
+    _fields_ = [
+        ("vertex_count", ctypes.c_uint32),
+        ("segment_count", ctypes.c_uint32),
+        ("fiber_count", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("positions", ctypes.c_void_p),
+        ("intrinsic_positions", ctypes.c_void_p),
+        ("segment_vertices", ctypes.c_void_p),
+        ("segment_fibers", ctypes.c_void_p),
+        ("segment_radii", ctypes.c_void_p),
+        ("segment_rest_lengths", ctypes.c_void_p),
+        ("fiber_vertex_spans", ctypes.c_void_p),
+        ("fiber_segment_spans", ctypes.c_void_p),
+        ("vertex_segments", ctypes.c_void_p),
+        ("vertex_max_curvature", ctypes.c_void_p),
+        ("vertex_pinned", ctypes.c_void_p),
+        ("cell_lower", ctypes.c_float * 3),
+        ("cell_upper", ctypes.c_float * 3),
+        ("cell_periodic", ctypes.c_uint32 * 3),
+        ("reserved2", ctypes.c_uint32),
+    ]
+
+
+class CellList(ctypes.Structure):
+    """tgl_cell_list_config."""
+
+    _fields_ = [
+        ("cell_size_scale", ctypes.c_float),
+        ("neighbor_skin_scale", ctypes.c_float),
+        ("neighbor_capacity", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("max_list_bytes", ctypes.c_uint64),
+    ]
+
+
+class Config(ctypes.Structure):
+    """tgl_relax_config."""
+
+    _fields_ = [
+        ("penetration_tolerance", ctypes.c_float),
+        ("correction_fraction", ctypes.c_float),
+        ("stretch_stiffness", ctypes.c_float),
+        ("bend_stiffness", ctypes.c_float),
+        ("curvature_limit_stiffness", ctypes.c_float),
+        ("curvature_limit_safety_margin", ctypes.c_float),
+        ("curvature_ratio_tolerance", ctypes.c_float),
+        ("max_step", ctypes.c_float),
+        ("constraint_iterations", ctypes.c_uint32),
+        ("curvature_cleanup_sweeps", ctypes.c_uint32),
+        ("contact_aggregation", ctypes.c_uint32),
+        ("force_full_iterations", ctypes.c_uint32),
+    ]
+
+
+class KernelTimes(ctypes.Structure):
+    """tgl_kernel_times."""
+
+    _fields_ = [
+        ("contact_ms", ctypes.c_double),
+        ("update_ms", ctypes.c_double),
+        ("rebuild_ms", ctypes.c_double),
+        ("contact_passes", ctypes.c_uint32),
+        ("updates", ctypes.c_uint32),
+        ("rebuilds", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+class Status(ctypes.Structure):
+    """tgl_batch_status."""
+
+    _fields_ = [
+        ("total_iterations", ctypes.c_uint64),
+        ("batch_iterations", ctypes.c_uint64),
+        ("max_penetration", ctypes.c_float),
+        ("max_displacement", ctypes.c_float),
+        ("max_curvature_ratio", ctypes.c_float),
+        ("converged", ctypes.c_uint32),
+        ("cell_list_overflow", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+def load_library():
+    """Loads the in-tree library (no fallback: raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m tangle_b200.build` (the CUDA path has no fallback)"
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    lib.tgl_world_create.argtypes = [ctypes.POINTER(Packed), ctypes.POINTER(CellList), ctypes.c_float,
+                                     ctypes.POINTER(P)]
+    lib.tgl_world_create.restype = ctypes.c_int
+    lib.tgl_world_destroy.argtypes = [P]
+    lib.tgl_world_destroy.restype = None
+    lib.tgl_run_batch.argtypes = [P, ctypes.POINTER(Config), ctypes.c_uint32, ctypes.POINTER(Status)]
+    lib.tgl_run_batch.restype = ctypes.c_int
+    lib.tgl_download_positions.argtypes = [P, P, ctypes.c_size_t]
+    lib.tgl_download_positions.restype = ctypes.c_int
+    lib.tgl_upload_positions.argtypes = [P, P, ctypes.c_size_t]
+    lib.tgl_upload_positions.restype = ctypes.c_int
+    lib.tgl_cell_size.argtypes = [P]
+    lib.tgl_cell_size.restype = ctypes.c_float
+    lib.tgl_cell_count.argtypes = [P]
+    lib.tgl_cell_count.restype = ctypes.c_uint64
+    lib.tgl_cell_dims.argtypes = [P, P]
+    lib.tgl_cell_dims.restype = None
+    lib.tgl_neighbor_skin.argtypes = [P]
+    lib.tgl_neighbor_skin.restype = ctypes.c_float
+    lib.tgl_neighbor_block.argtypes = [P]
+    lib.tgl_neighbor_block.restype = ctypes.c_uint32
+    lib.tgl_neighbor_list_rebuilds.argtypes = [P, ctypes.POINTER(ctypes.c_uint32)]
+    lib.tgl_neighbor_list_rebuilds.restype = ctypes.c_int
+    lib.tgl_debug_rebuild.argtypes = [P]
+    lib.tgl_debug_rebuild.restype = ctypes.c_int
+    lib.tgl_debug_cell_list.argtypes = [P, P, P, P]
+    lib.tgl_debug_cell_list.restype = ctypes.c_int
+    lib.tgl_debug_neighbor_lists.argtypes = [P, P, P]
+    lib.tgl_debug_neighbor_lists.restype = ctypes.c_int
+    lib.tgl_debug_corrections.argtypes = [P, ctypes.POINTER(Config), P, P]
+    lib.tgl_debug_corrections.restype = ctypes.c_int
+    lib.tgl_kernel_launches.argtypes = [P]
+    lib.tgl_kernel_launches.restype = ctypes.c_uint64
+    lib.tgl_set_kernel_timing.argtypes = [P, ctypes.c_int]
+    lib.tgl_set_kernel_timing.restype = ctypes.c_int
+    lib.tgl_last_kernel_times.argtypes = [P, ctypes.POINTER(KernelTimes)]
+    lib.tgl_last_kernel_times.restype = ctypes.c_int
+    lib.tgl_world_stream.argtypes = [P]
+    lib.tgl_world_stream.restype = ctypes.c_void_p
+    lib.tgl_last_error.argtypes = []
+    lib.tgl_last_error.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def _raise(lib, rc: int):
+    message = lib.tgl_last_error().decode()
+    if rc in (TGL_ERR_INVALID, TGL_ERR_UNSUPPORTED):
+        raise ValueError(message)
+    raise RuntimeError(f"tangle CUDA error {rc}: {message}")
+
+
+def _ptr(array: Optional[np.ndarray]):
+    return None if array is None else array.ctypes.data_as(ctypes.c_void_p)
+
+
+def packed_struct(packed, keep: list) -> Packed:
+    arrays = [
+        np.ascontiguousarray(packed.positions, dtype=np.float32),
+        np.ascontiguousarray(packed.intrinsic_positions, dtype=np.float32),
+        np.ascontiguousarray(packed.segment_vertices, dtype=np.uint32),
+        np.ascontiguousarray(packed.segment_fibers, dtype=np.uint32),
+        np.ascontiguousarray(packed.segment_radii, dtype=np.float32),
+        np.ascontiguousarray(packed.segment_rest_lengths, dtype=np.float32),
+        np.ascontiguousarray(packed.fiber_vertex_spans, dtype=np.uint32),
+        np.ascontiguousarray(packed.fiber_segment_spans, dtype=np.uint32),
+        np.ascontiguousarray(packed.vertex_segments, dtype=np.uint32),
+        np.ascontiguousarray(packed.vertex_max_curvature, dtype=np.float32),
+        np.ascontiguousarray(packed.vertex_pinned, dtype=np.uint32),
+    ]
+    keep.extend(arrays)
+    pk = Packed()
+    pk.vertex_count = packed.vertex_count
+    pk.segment_count = packed.segment_count
+    pk.fiber_count = packed.fiber_count
+    (pk.positions, pk.intrinsic_positions, pk.segment_vertices, pk.segment_fibers, pk.segment_radii,
+     pk.segment_rest_lengths, pk.fiber_vertex_spans, pk.fiber_segment_spans, pk.vertex_segments,
+     pk.vertex_max_curvature, pk.vertex_pinned) = [a.ctypes.data for a in arrays]
+    for a in range(3):
+        pk.cell_lower[a] = float(packed.cell_lower[a])
+        pk.cell_upper[a] = float(packed.cell_upper[a])
+        pk.cell_periodic[a] = int(packed.cell_periodic[a])
+    return pk
+
+
+def config_struct(config: RelaxationConfig) -> Config:
+    return Config(
+        float(config.penetration_tolerance), float(config.correction_fraction), float(config.stretch_stiffness),
+        float(config.bend_stiffness), float(config.curvature_limit_stiffness),
+        float(config.curvature_limit_safety_margin), float(config.curvature_ratio_tolerance),
+        float(config.max_step), int(config.constraint_iterations), int(config.curvature_cleanup_sweeps),
+        int(config.contact_aggregation), int(bool(config.force_full_iterations)),
+    )
+
+
+def cell_list_struct(cell_list: CellListConfig) -> CellList:
+    return CellList(float(cell_list.cell_size_scale), float(cell_list.neighbor_skin_scale),
+                    int(cell_list.neighbor_capacity), 0, int(cell_list.max_list_bytes))
+
+
+class DeviceWorld:
+    """Resident relaxation world on the current CUDA device."""
+
+    def __init__(self, packed, cell_list: Optional[CellListConfig] = None, max_step: float = 0.006):
+        lib = load_library()
+        cell_list = cell_list or CellListConfig()
+        keep: list = []
+        pk = packed_struct(packed, keep)
+        cl = cell_list_struct(cell_list)
+        handle = ctypes.c_void_p()
+        rc = lib.tgl_world_create(ctypes.byref(pk), ctypes.byref(cl), ctypes.c_float(max_step), ctypes.byref(handle))
+        if rc:
+            _raise(lib, rc)
+        self._lib = lib
+        self._handle = handle
+        self.vertex_count = packed.vertex_count
+        self.segment_count = packed.segment_count
+
+    @classmethod
+    def upload(cls, config: RelaxationConfig, packed) -> "DeviceWorld":
+        """DeviceWorld::upload(config, packed) (plugin.rs:422-424)."""
+        return cls(packed, config.cell_list, config.max_step)
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            self._lib.tgl_world_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            _raise(self._lib, rc)
+
+    def run_batch(self, config: RelaxationConfig, iterations: int) -> BatchStatus:
+        st = Status()
+        self._check(self._lib.tgl_run_batch(self._handle, ctypes.byref(config_struct(config)), int(iterations),
+                                            ctypes.byref(st)))
+        return BatchStatus(
+            total_iterations=int(st.total_iterations),
+            batch_iterations=int(st.batch_iterations),
+            max_penetration=float(st.max_penetration),
+            max_displacement=float(st.max_displacement),
+            max_curvature_ratio=float(st.max_curvature_ratio),
+            converged=bool(st.converged),
+            cell_list_overflow=bool(st.cell_list_overflow),
+        )
+
+    def download_positions(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(3 * self.vertex_count, dtype=np.float32)
+        self._check(self._lib.tgl_download_positions(self._handle, _ptr(out), out.size))
+        return out
+
+    def upload_positions(self, positions) -> None:
+        arr = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
+        self._check(self._lib.tgl_upload_positions(self._handle, _ptr(arr), arr.size))
+
+    @property
+    def cell_size(self) -> float:
+        return float(self._lib.tgl_cell_size(self._handle))
+
+    @property
+    def cell_count(self) -> int:
+        return int(self._lib.tgl_cell_count(self._handle))
+
+    @property
+    def cell_dims(self):
+        dims = np.zeros(3, dtype=np.uint32)
+        self._lib.tgl_cell_dims(self._handle, _ptr(dims))
+        return tuple(int(v) for v in dims)
+
+    @property
+    def neighbor_skin(self) -> float:
+        return float(self._lib.tgl_neighbor_skin(self._handle))
+
+    @property
+    def neighbor_block(self) -> int:
+        return int(self._lib.tgl_neighbor_block(self._handle))
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self._lib.tgl_kernel_launches(self._handle))
+
+    @property
+    def stream_handle(self) -> int:
+        """The cudaStream_t (as an int) this world's kernels run on."""
+        return int(self._lib.tgl_world_stream(self._handle) or 0)
+
+    def set_kernel_timing(self, enable: bool) -> None:
+        self._check(self._lib.tgl_set_kernel_timing(self._handle, 1 if enable else 0))
+
+    def last_kernel_times(self) -> dict:
+        t = KernelTimes()
+        self._check(self._lib.tgl_last_kernel_times(self._handle, ctypes.byref(t)))
+        return {"contact_ms": t.contact_ms, "update_ms": t.update_ms, "rebuild_ms": t.rebuild_ms,
+                "contact_passes": t.contact_passes, "updates": t.updates, "steps": t.rebuilds}
+
+    def neighbor_list_rebuilds(self) -> int:
+        out = ctypes.c_uint32()
+        self._check(self._lib.tgl_neighbor_list_rebuilds(self._handle, ctypes.byref(out)))
+        return int(out.value)
+
+    def debug_rebuild(self) -> None:
+        self._check(self._lib.tgl_debug_rebuild(self._handle))
+
+    def debug_cell_list(self):
+        C = self.cell_count
+        counts = np.empty(C, dtype=np.uint32)
+        offsets = np.empty(C, dtype=np.uint32)
+        segments = np.empty(self.segment_count, dtype=np.uint32)
+        self._check(self._lib.tgl_debug_cell_list(self._handle, _ptr(counts), _ptr(offsets), _ptr(segments)))
+        return counts, offsets, segments
+
+    def debug_neighbor_lists(self):
+        block = self.neighbor_block
+        counts = np.empty(self.segment_count, dtype=np.uint32)
+        lists = np.empty(max(block * self.segment_count, 1), dtype=np.uint32)
+        self._check(self._lib.tgl_debug_neighbor_lists(self._handle, _ptr(counts), _ptr(lists)))
+        out = []
+        for s in range(self.segment_count):
+            n = int(counts[s])
+            out.append(lists[block * s: block * s + n].copy() if n <= block else None)
+        return counts, out
+
+    def debug_corrections(self, config: RelaxationConfig):
+        corr = np.empty(6 * self.segment_count, dtype=np.float32)
+        pen = np.empty(self.segment_count, dtype=np.float32)
+        self._check(self._lib.tgl_debug_corrections(self._handle, ctypes.byref(config_struct(config)), _ptr(corr),
+                                                    _ptr(pen)))
+        return corr, pen

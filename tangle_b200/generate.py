@@ -1,0 +1,315 @@
+"""Seeded synthetic fiber inputs.
+
+* `SplitMix64` -- the reference's generator, bit for bit
+  (crates/tangle_generate/src/population.rs:795-812): 53-bit unit doubles.
+* `FiberPopulation` / `generate_fiber_population` -- the reference's biased
+  box generator (population.rs:246-357) for isotropic orientation and uniform
+  position: per fiber it draws length, radius, waviness amplitude and
+  handedness, builds the local centerline (population.rs:554-565), draws a
+  direction (population.rs:567-578) and a contained centre
+  (population.rs:657-693), in that order. Python defaults follow
+  crates/tangle_python/src/generators.rs:395-450 (length 16-24 diameters,
+  curvature amplitude 0-0.8 diameters, 8 segments, seed 1).
+* `mid_size_specimen`, `cpu_runnable_specimen`, `batched_specimens` -- the
+  benchmark workloads: synthetic stand-ins with the shapes, sizes and value
+  distributions of the configurations they are named after (no dataset is
+  involved; every input is generated here from a seed).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, replace
+from typing import List, Optional, Sequence, Tuple, Union
+
+import numpy as np
+
+from .assembly import Cell, FiberAssembly, Material
+
+MASK64 = (1 << 64) - 1
+
+
+class SplitMix64:
+    """population.rs:795-812."""
+
+    def __init__(self, seed: int):
+        self.state = int(seed) & MASK64
+
+    def unit(self) -> float:
+        self.state = (self.state + 0x9E3779B97F4A7C15) & MASK64
+        value = self.state
+        value = ((value ^ (value >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+        value = ((value ^ (value >> 27)) * 0x94D049BB133111EB) & MASK64
+        value ^= value >> 31
+        return float(value >> 11) * (1.0 / float(1 << 53))
+
+
+def _normalize(v):
+    n = math.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+    return [v[0] / n, v[1] / n, v[2] / n]
+
+
+def _cross(a, b):
+    return [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+
+
+def perpendicular(direction):
+    """population.rs:758-768."""
+    ax, ay, az = abs(direction[0]), abs(direction[1]), abs(direction[2])
+    if ax <= ay and ax <= az:
+        axis = [1.0, 0.0, 0.0]
+    elif ay <= az:
+        axis = [0.0, 1.0, 0.0]
+    else:
+        axis = [0.0, 0.0, 1.0]
+    return _normalize(_cross(direction, axis))
+
+
+def isotropic_direction(random: SplitMix64):
+    """population.rs:573-578."""
+    z = 2.0 * random.unit() - 1.0
+    azimuth = 2.0 * math.pi * random.unit()
+    radial = math.sqrt(1.0 - z * z)
+    return [radial * math.cos(azimuth), radial * math.sin(azimuth), z]
+
+
+def schladitz_axis_cosine_quantile(beta: float, p: float) -> float:
+    """|cos theta| quantile of the Schladitz orientation density about an
+    axis (crates/tangle_characterize/src/shape.rs:550-556)."""
+    beta2 = beta * beta
+    p = min(max(p, 0.0), 1.0)
+    return min(p / math.sqrt(beta2 - (beta2 - 1.0) * p * p), 1.0)
+
+
+def local_centerline(segments: int, length: float, amplitude: float, handedness: float) -> np.ndarray:
+    """population.rs:554-565."""
+    points = []
+    for index in range(segments + 1):
+        centered = index / segments - 0.5
+        points.append([
+            centered * length,
+            amplitude * math.sin(2.0 * math.pi * centered),
+            0.5 * amplitude * handedness * math.sin(4.0 * math.pi * centered),
+        ])
+    return np.array(points, dtype=np.float64)
+
+
+Range = Union[float, Tuple[float, float], None]
+
+
+def _range(value: Range) -> Optional[Tuple[float, float]]:
+    if value is None:
+        return None
+    if isinstance(value, (int, float)):
+        return (float(value), float(value))
+    low, high = value
+    return (float(low), float(high))
+
+
+@dataclass
+class FiberPopulation:
+    """Random fibers for `generate_fiber_population` (_tangle.pyi:459-500)."""
+
+    material: Material = None
+    count: int = 32
+    segments_per_fiber: int = 8
+    seed: int = 1
+    length: Range = None
+    diameter: Range = None
+    curvature_amplitude: Range = None
+    max_attempts_per_fiber: int = 1000
+
+    def __post_init__(self):
+        if self.material is None:
+            self.material = Material("fiber", 0.025, 0.08)
+        if self.count < 0:
+            raise ValueError("count must be non-negative")
+        if self.segments_per_fiber < 2:
+            raise ValueError("segments_per_fiber must be at least 2")
+
+    def copy(self) -> "FiberPopulation":
+        return replace(self)
+
+    def replace(self, **changes) -> "FiberPopulation":
+        return replace(self, **changes)
+
+
+def generate_fiber_population(cell: Cell, population: FiberPopulation) -> FiberAssembly:
+    """population.rs:246-357, isotropic directions and uniform centres."""
+    assembly = FiberAssembly(cell)
+    d = population.material.diameter
+    length = _range(population.length) or (16.0 * d, 24.0 * d)
+    diameter = _range(population.diameter) or (d, d)
+    amplitude = _range(population.curvature_amplitude) or (0.0, 0.8 * d)
+    min_bend = population.material.min_bend_radius
+    random = SplitMix64(population.seed)
+    low = np.array(cell.origin)
+    high = low + np.array(cell.lengths)
+    periodic = cell.periodic
+    for fiber_index in range(population.count):
+        placed_fiber = None
+        for _ in range(population.max_attempts_per_fiber):
+            fiber_length = length[0] + (length[1] - length[0]) * random.unit()
+            radius = 0.5 * (diameter[0] + (diameter[1] - diameter[0]) * random.unit())
+            wave = amplitude[0] + (amplitude[1] - amplitude[0]) * random.unit()
+            handedness = -1.0 if random.unit() < 0.5 else 1.0
+            intrinsic = local_centerline(population.segments_per_fiber, fiber_length, wave, handedness)
+            if min_bend is not None and maximum_polyline_curvature(intrinsic) > (1.0 / min_bend) * (1.0 + 1.0e-10):
+                continue
+            direction = isotropic_direction(random)
+            ta = perpendicular(direction)
+            tb = _normalize(_cross(direction, ta))
+            offsets = (np.outer(intrinsic[:, 0], direction) + np.outer(intrinsic[:, 1], ta)
+                       + np.outer(intrinsic[:, 2], tb))
+            lower = np.empty(3)
+            upper = np.empty(3)
+            ok = True
+            for axis in range(3):
+                if periodic[axis]:
+                    lower[axis], upper[axis] = low[axis], high[axis]
+                    continue
+                lower[axis] = low[axis] + radius - offsets[:, axis].min()
+                upper[axis] = high[axis] - radius - offsets[:, axis].max()
+                if lower[axis] > upper[axis]:
+                    ok = False
+                    break
+            if not ok:
+                continue
+            center = np.array([lower[a] + (upper[a] - lower[a]) * random.unit() for a in range(3)])
+            placed_fiber = (intrinsic, center + offsets, radius)
+            break
+        if placed_fiber is None:
+            raise RuntimeError(f"could not place fiber {fiber_index} inside the cell")
+        intrinsic, placed, radius = placed_fiber
+        assembly.add_fiber(placed, intrinsic, radius=radius, min_bend_radius=min_bend)
+    return assembly
+
+
+def maximum_polyline_curvature(points: np.ndarray) -> float:
+    """crates/tangle_core/src/curvature.rs:21-61 (f64)."""
+    best = 0.0
+    for i in range(1, len(points) - 1):
+        a = points[i] - points[i - 1]
+        b = points[i + 1] - points[i]
+        la, lb = float(np.linalg.norm(a)), float(np.linalg.norm(b))
+        if la <= 2.220446049250313e-16 or lb <= 2.220446049250313e-16:
+            continue
+        cosine = min(max(float(a @ b) / (la * lb), -1.0), 1.0)
+        angle = math.acos(cosine)
+        curvature = 2.0 * math.sin(0.5 * angle) / (0.5 * (la + lb))
+        best = max(best, curvature)
+    return best
+
+
+def _straight_fibers(assembly: FiberAssembly, starts: np.ndarray, directions: np.ndarray, length: float,
+                     segments: int, radius: float, min_bend_radius: Optional[float]) -> None:
+    steps = np.arange(segments + 1, dtype=np.float64) * (length / segments)
+    for start, direction in zip(starts, directions):
+        points = start[None, :] + steps[:, None] * direction[None, :]
+        assembly.add_fiber(points, points, radius=radius, min_bend_radius=min_bend_radius)
+
+
+def cpu_runnable_specimen(seed: int = 1) -> FiberAssembly:
+    """Periodic 300 um cube, 40 straight 10 um fibers, 300 um long as 30
+    segments (31 nodes); first node uniform in the cell, direction uniform on
+    the sphere; curvature limit 1/(5 d). 1,240 nodes."""
+    d = 10.0e-6
+    side = 300.0e-6
+    cell = Cell([side] * 3, "xyz")
+    assembly = FiberAssembly(cell)
+    random = SplitMix64(seed)
+    starts, directions = [], []
+    for _ in range(40):
+        starts.append([side * random.unit() for _ in range(3)])
+        directions.append(isotropic_direction(random))
+    _straight_fibers(assembly, np.array(starts), np.array(directions), 300.0e-6, 30, 0.5 * d, 5.0 * d)
+    return assembly
+
+
+def _wavy_fibers(assembly, centers, directions, normals, phases, lengths, segments, diameter, min_bend_radius):
+    """Planar sinusoidal waviness: offset 0.5 d sin(2 pi s / (20 d) + phase)
+    along a normal perpendicular to the axis; rest shape = initial shape."""
+    amplitude = 0.5 * diameter
+    wavelength = 20.0 * diameter
+    for center, direction, normal, phase, length in zip(centers, directions, normals, phases, lengths):
+        s = (np.arange(segments + 1, dtype=np.float64) / segments - 0.5) * length
+        wave = amplitude * np.sin(2.0 * math.pi * s / wavelength + phase)
+        points = center[None, :] + s[:, None] * direction[None, :] + wave[:, None] * normal[None, :]
+        assembly.add_fiber(points, points, radius=0.5 * diameter, min_bend_radius=min_bend_radius)
+
+
+def mid_size_specimen(scale: float = 1.0, seed: int = 1, beta: float = 1.0 / 0.3,
+                      fibers: int = 20000) -> FiberAssembly:
+    """Periodic 2x2x2 mm cell, 20,000 fibers 1.5 mm long, diameters 7 and
+    19 um split 50:50 by fiber volume (17,610 and 2,390 fibers), segment
+    length 2 d (round(1.5 mm / 2 d) segments: 107 and 39), Schladitz
+    orientation about z, sinusoidal waviness of amplitude 0.5 d, wavelength
+    20 d and uniform phase, curvature limit 1/(5 d). About 2.0 M nodes.
+
+    `beta` uses the Schladitz convention of
+    crates/tangle_characterize/src/shape.rs:26-30 (beta = 1 isotropic, beta > 1
+    lays fibers in the plane normal to the axis). The default 1/0.3 is the
+    xy-biased reading of "beta = 0.3 (xy-biased)". `scale` < 1 shrinks the
+    cell side by scale and the fiber count by scale**3, keeping the volume
+    fraction (used for the learned-warm-start training specimens and for small
+    parity cases).
+    """
+    side = 2.0e-3 * scale
+    count = max(int(round(fibers * scale ** 3)), 2)
+    ratio = (19.0 / 7.0) ** 2
+    n19 = int(round(count / (1.0 + ratio)))
+    n7 = count - n19
+    cell = Cell([side] * 3, "xyz")
+    assembly = FiberAssembly(cell)
+    random = SplitMix64(seed)
+    for diameter, n in ((19.0e-6, n19), (7.0e-6, n7)):
+        segments = int(round(1.5e-3 / (2.0 * diameter)))
+        centers, directions, normals, phases = [], [], [], []
+        for _ in range(n):
+            center = [side * random.unit() for _ in range(3)]
+            cz = schladitz_axis_cosine_quantile(beta, random.unit())
+            if random.unit() < 0.5:
+                cz = -cz
+            azimuth = 2.0 * math.pi * random.unit()
+            sz = math.sqrt(max(1.0 - cz * cz, 0.0))
+            direction = [sz * math.cos(azimuth), sz * math.sin(azimuth), cz]
+            ta = perpendicular(direction)
+            tb = _normalize(_cross(direction, ta))
+            turn = 2.0 * math.pi * random.unit()
+            normal = [math.cos(turn) * ta[i] + math.sin(turn) * tb[i] for i in range(3)]
+            phase = 2.0 * math.pi * random.unit()
+            centers.append(center)
+            directions.append(direction)
+            normals.append(normal)
+            phases.append(phase)
+        _wavy_fibers(assembly, np.array(centers), np.array(directions), np.array(normals), phases,
+                     [1.5e-3] * n, segments, diameter, 5.0 * diameter)
+    return assembly
+
+
+def batched_specimens(count: int = 512, seed: int = 1, max_fibers: int = 5000) -> List[FiberAssembly]:
+    """Independent specimens: fiber count log-uniform in [40, max_fibers],
+    10 um fibers, length uniform in [0.3, 1] mm with segment length 2 d,
+    isotropic straight fibers, periodic cube whose side gives a fiber volume
+    fraction uniform in [5 %, 25 %], curvature limit 1/(5 d)."""
+    d = 10.0e-6
+    out = []
+    for index in range(count):
+        random = SplitMix64(seed * 1_000_003 + index)
+        fibers = int(round(math.exp(math.log(40.0) + (math.log(max_fibers) - math.log(40.0)) * random.unit())))
+        fraction = 0.05 + 0.20 * random.unit()
+        lengths = [0.3e-3 + 0.7e-3 * random.unit() for _ in range(fibers)]
+        volume = sum(math.pi * (0.5 * d) ** 2 * length for length in lengths)
+        side = (volume / fraction) ** (1.0 / 3.0)
+        side = max(side, 1.05 * max(lengths) / 2.0)
+        cell = Cell([side] * 3, "xyz")
+        assembly = FiberAssembly(cell)
+        for length in lengths:
+            segments = max(int(round(length / (2.0 * d))), 2)
+            start = np.array([side * random.unit() for _ in range(3)])
+            direction = np.array(isotropic_direction(random))
+            steps = np.arange(segments + 1) * (length / segments)
+            points = start[None, :] + steps[:, None] * direction[None, :]
+            assembly.add_fiber(points, points, radius=0.5 * d, min_bend_radius=5.0 * d)
+        out.append(assembly)
+    return out

@@ -1,0 +1,195 @@
+"""`Recipe` / `RunResult`: the reference's Python entry point to relaxation.
+
+Mirrors crates/tangle_python/python/tangle/_tangle.pyi:915-1014 for the
+relaxation operations, and the run loop of
+crates/tangle_python/src/recipe.rs:618-723 with the batch controller of
+crates/tangle_relax/src/device/plugin.rs:1041-1181 and the operation
+controllers of crates/tangle_generate/src/recipe.rs:1311-1380:
+
+* unset length settings are sized from the smallest fiber diameter;
+* a recipe that only inserts fibers relaxes them until converged;
+* each batch runs at most `iterations_per_batch` iterations and at most the
+  run-wide `max_iterations` remaining; `relax_for` forces full batches;
+* a `relax_until_converged` step that exhausts its budget raises
+  `RecipeError`.
+"""
+
+from __future__ import annotations
+
+import copy
+from dataclasses import dataclass
+from typing import List, Optional, Union
+
+import numpy as np
+
+from .assembly import Cell, FiberAssembly, PackedAssembly
+from .device import DeviceWorld
+from .generate import FiberPopulation, generate_fiber_population
+from .settings import BatchStatus, RelaxationSettings
+
+
+class RecipeError(RuntimeError):
+    """A recorded step could not be completed (_tangle.pyi:38)."""
+
+    def __init__(self, operation: int, description: str, iteration: int, reason: str):
+        super().__init__(f"operation {operation} ({description}) failed at iteration {iteration}: {reason}")
+        self.operation = operation
+        self.description = description
+        self.iteration = iteration
+        self.reason = reason
+
+
+@dataclass
+class _Insert:
+    assembly: FiberAssembly
+
+
+@dataclass
+class _RelaxUntilConverged:
+    maximum_iterations: int
+
+
+@dataclass
+class _RelaxFor:
+    iterations: int
+
+
+class RunResult:
+    """The relaxed fibers and run statistics (_tangle.pyi:1003-1014)."""
+
+    def __init__(self, assembly: FiberAssembly, status: BatchStatus, uploaded_bytes: int, downloaded_bytes: int,
+                 cell_size: float, cell_count: int, rebuilds: int):
+        self.assembly = assembly
+        self._status = status
+        self.uploaded_bytes = uploaded_bytes
+        self.downloaded_bytes = downloaded_bytes
+        self.cell_size = cell_size
+        self.cell_count = cell_count
+        self.neighbor_list_rebuilds = rebuilds
+
+    fiber_count = property(lambda self: self.assembly.fiber_count)
+    iterations = property(lambda self: self._status.total_iterations)
+    converged = property(lambda self: self._status.converged)
+    max_penetration = property(lambda self: self._status.max_penetration)
+    max_curvature_ratio = property(lambda self: self._status.max_curvature_ratio)
+    max_displacement = property(lambda self: self._status.max_displacement)
+
+    def centerlines(self) -> List[List[List[float]]]:
+        return self.assembly.centerlines()
+
+    def __repr__(self) -> str:
+        return (f"RunResult(fibers={self.fiber_count}, iterations={self.iterations}, converged={self.converged}, "
+                f"max_penetration={self.max_penetration:.3e}, max_curvature_ratio={self.max_curvature_ratio:.6f})")
+
+
+def _upload_bytes(packed: PackedAssembly) -> int:
+    arrays = [packed.positions, packed.intrinsic_positions, packed.segment_vertices, packed.segment_fibers,
+              packed.segment_radii, packed.segment_rest_lengths, packed.fiber_vertex_spans,
+              packed.fiber_segment_spans, packed.vertex_segments, packed.vertex_max_curvature, packed.vertex_pinned]
+    return int(sum(a.nbytes for a in arrays)) + 6 * 4 + 3 * 4
+
+
+class Recipe:
+    """An ordered list of steps on one cell; nothing runs until `run`."""
+
+    def __init__(self, cell: Union[Cell, FiberAssembly]):
+        if isinstance(cell, FiberAssembly):
+            self._assembly = copy.deepcopy(cell)
+        elif isinstance(cell, Cell):
+            self._assembly = FiberAssembly(cell)
+        else:
+            raise TypeError("Recipe needs a Cell or a FiberAssembly")
+        self._operations: list = []
+        self._descriptions: List[str] = []
+
+    @property
+    def cell(self) -> Cell:
+        return self._assembly.cell
+
+    def insert(self, collection) -> None:
+        if isinstance(collection, FiberPopulation):
+            collection = generate_fiber_population(self._assembly.cell, collection)
+        if not isinstance(collection, FiberAssembly):
+            raise TypeError("insert takes a FiberAssembly (a generated collection) or a FiberPopulation")
+        for fiber in collection.fibers:
+            self._assembly.add_fiber(fiber.placed, fiber.intrinsic, radius=fiber.radius,
+                                     min_bend_radius=fiber.min_bend_radius)
+        self._operations.append(_Insert(collection))
+        self._descriptions.append(f"insert {collection.fiber_count} fibers")
+
+    def relax_until_converged(self, *, max_iterations: int = 2000) -> None:
+        if max_iterations <= 0:
+            raise ValueError("max_iterations must be positive")
+        self._operations.append(_RelaxUntilConverged(int(max_iterations)))
+        self._descriptions.append("relax until converged")
+
+    def relax_for(self, iterations: int) -> None:
+        if iterations <= 0:
+            raise ValueError("iterations must be positive")
+        self._operations.append(_RelaxFor(int(iterations)))
+        self._descriptions.append(f"relax for {iterations} iterations")
+
+    def operations(self) -> List[str]:
+        return list(self._descriptions)
+
+    def centerlines(self) -> List[List[List[float]]]:
+        return self._assembly.centerlines()
+
+    def run(self, settings: Optional[RelaxationSettings] = None) -> RunResult:
+        if not self._assembly.fibers:
+            raise ValueError("recipe contains no fibers")
+        if not self._operations:
+            raise ValueError("recipe contains no operations")
+        settings = settings or RelaxationSettings()
+        if settings.backend != "cuda":
+            raise ValueError(f"backend={settings.backend!r} belongs to the reference implementation; "
+                             "this library provides backend='cuda'")
+        config = settings.to_config(self._assembly.smallest_diameter())
+        operations = list(self._operations)
+        descriptions = list(self._descriptions)
+        if all(isinstance(op, _Insert) for op in operations):
+            operations.append(_RelaxUntilConverged(config.max_iterations))
+            descriptions.append("relax until converged")
+        assembly = copy.deepcopy(self._assembly)
+        packed = PackedAssembly.from_assembly(assembly, config.pin_fiber_ends)
+        world = DeviceWorld.upload(config, packed)
+        status = BatchStatus(max_penetration=float("inf"), max_curvature_ratio=float("inf"))
+        downloaded = 0
+        try:
+            for index, op in enumerate(operations):
+                if isinstance(op, _Insert):
+                    continue
+                started = status.total_iterations
+                force = isinstance(op, _RelaxFor)
+                budget = op.iterations if force else op.maximum_iterations
+                while True:
+                    completed = status.total_iterations - started
+                    if not force and status.converged:
+                        break
+                    if completed >= budget:
+                        if force:
+                            break
+                        raise RecipeError(index, descriptions[index], status.total_iterations,
+                                          f"failed to converge in {budget} iterations: penetration "
+                                          f"{status.max_penetration:.3e}, curvature ratio "
+                                          f"{status.max_curvature_ratio:.6f}")
+                    remaining = config.max_iterations - status.total_iterations
+                    if remaining <= 0:
+                        raise RecipeError(index, descriptions[index], status.total_iterations,
+                                          "run-wide max_iterations exhausted")
+                    batch = min(remaining, config.iterations_per_batch, budget - completed)
+                    batch_config = copy.copy(config)
+                    batch_config.force_full_iterations = config.force_full_iterations or force
+                    status = world.run_batch(batch_config, batch)
+                    downloaded += 11 * 4 + 3 * 4
+                    if status.cell_list_overflow:
+                        raise RecipeError(index, descriptions[index], status.total_iterations, "cell list overflow")
+                if force:
+                    status.converged = False
+            positions = world.download_positions()
+            downloaded += positions.nbytes
+            packed.unpack_positions(positions, assembly)
+            return RunResult(assembly, status, _upload_bytes(packed), downloaded, world.cell_size, world.cell_count,
+                             world.neighbor_list_rebuilds())
+        finally:
+            world.close()
