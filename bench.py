@@ -60,7 +60,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tta", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-iterations", type=int, default=2)
+    ap.add_argument("--cpu-iterations", type=int, default=4)
+    ap.add_argument("--save-positions", default=None, help="write the positions after the timed steps (.npy)")
+    ap.add_argument("--load-positions", default=None, help="start from saved positions (.npy)")
     return ap.parse_args()
 
 
@@ -252,6 +254,8 @@ def run_cuda(args):
     nodes = packed.vertex_count
     fixed = type(config)(**{**config.__dict__, "force_full_iterations": True})
     world = DeviceWorld(packed, config.cell_list, config.max_step)
+    if args.load_positions:
+        world.upload_positions(np.load(args.load_positions))
     world.set_kernel_timing(True)
     stream = torch.cuda.ExternalStream(world.stream_handle)
 
@@ -291,6 +295,8 @@ def run_cuda(args):
         end.synchronize()
     launches = world.kernel_launches - launches0
     rebuilds = world.neighbor_list_rebuilds() - rebuilds0
+    if args.save_positions and rank == 0:
+        np.save(args.save_positions, world.download_positions())
     bytes_end = contact_bytes(world)
     elapsed_ms = start.elapsed_time(end)
     barrier()

@@ -243,6 +243,8 @@ struct orc_world {
     std::vector<float> reference_positions;
     std::vector<float> corrections, segment_max, curvature_ratio, internal, vertex_step,
         wall_reactions;
+    /* Curvature triplets that moved a vertex (a diagnostic count). */
+    uint64_t projections = 0;
 };
 
 namespace {
@@ -902,6 +904,8 @@ void project_curvature_triplet(orc_world &w, uint32_t previous, uint32_t center,
                         center_weight * (cgx * cgx + cgy * cgy + cgz * cgz) +
                         next_weight * (gvx * gvx + gvy * gvy + gvz * gvz);
     if (!(denominator > 1.0e-12f)) return;
+    if (previous_weight > 0.0f || center_weight > 0.0f || next_weight > 0.0f)
+        __atomic_fetch_add(&w.projections, 1, __ATOMIC_RELAXED);
     float scale = stiffness * violation / denominator;
     const float pg[3] = {gux, guy, guz};
     const float cg[3] = {cgx, cgy, cgz};
@@ -1107,6 +1111,7 @@ void orc_cell_dims(const orc_world *w, uint32_t dims[3]) {
 float orc_neighbor_skin(const orc_world *w) { return w->neighbor_skin; }
 uint32_t orc_neighbor_block(const orc_world *w) { return w->neighbor_block; }
 uint32_t orc_neighbor_list_rebuilds(const orc_world *w) { return w->neighbor_state[1]; }
+uint64_t orc_curvature_projections(const orc_world *w) { return w->projections; }
 
 int orc_debug_cell_list(const orc_world *w, uint32_t *cell_counts, uint32_t *cell_offsets, uint32_t *cell_segments) {
     std::memcpy(cell_counts, w->cell_counts.data(), w->cell_counts.size() * 4);

@@ -110,6 +110,8 @@ void orc_cell_dims(const orc_world *world, uint32_t dims[3]);
 float orc_neighbor_skin(const orc_world *world);
 uint32_t orc_neighbor_block(const orc_world *world);
 uint32_t orc_neighbor_list_rebuilds(const orc_world *world);
+/* Curvature triplet projections that moved a vertex, since creation. */
+uint64_t orc_curvature_projections(const orc_world *world);
 void orc_set_threads(int threads);
 
 /* Parity taps. Each rebuilds nothing; they copy the current state out. */

@@ -23,6 +23,7 @@ struct Grid {
     float upper[3];
     float length[3];
     float width[3];
+    float inv_length[3];  // 1 / length in f32, for image_round's fast path
     uint32_t periodic[3];
     uint32_t cells[3];
 };
@@ -118,29 +119,55 @@ __device__ inline uint32_t stencil_cell(uint32_t home, uint32_t neighbor, const 
     return (nz * g.cells[1] + ny) * g.cells[0] + nx;
 }
 
+// roundf(x / length[a]) -- the image count of a periodic axis -- without the
+// IEEE division in all but a vanishing set of cases. With q = x * (1/length)
+// rounded twice in f32, |q - x/length| <= |q| 2^-22 and the correctly
+// rounded quotient is within |q| 2^-24 of x/length; for |q| < 4096 both lie
+// within 7.4e-4 of q. Rounding to the nearest integer only changes at
+// half-integers, so when q is more than 1e-3 from one, roundf(q) is exactly
+// roundf(x / length) (same integer, same sign of zero). Otherwise the
+// division is done.
+__device__ inline float image_round(float x, int a, const Grid &g) {
+    float q = x * g.inv_length[a];
+    float aq = fabsf(q);
+    if (aq < 0.499f) return copysignf(0.0f, q);  // the common case: same cell image
+    float fraction = aq - floorf(aq);
+    if (aq < 4096.0f && fabsf(fraction - 0.5f) > 1.0e-3f) return roundf(q);
+    return roundf(x / g.length[a]);
+}
+
 // Minimum-image shift of the second segment against the first, per periodic
-// axis (neighbor.rs:301-318, contact.rs:456-473).
-__device__ inline void minimum_image(float p1x, float p1y, float p1z, float q1x, float q1y, float q1z,
+// axis (neighbor.rs:301-318, contact.rs:456-473). Returns true when some axis
+// shifted by a nonzero number of box lengths.
+__device__ inline bool minimum_image(float p1x, float p1y, float p1z, float q1x, float q1y, float q1z,
                                      float &p2x, float &p2y, float &p2z, float &q2x, float &q2y, float &q2z,
                                      const Grid &g) {
     float image_dx = 0.5f * (p2x + q2x - p1x - q1x);
     float image_dy = 0.5f * (p2y + q2y - p1y - q1y);
     float image_dz = 0.5f * (p2z + q2z - p1z - q1z);
+    bool moved = false;
     if (g.periodic[0]) {
-        float shift = roundf(image_dx / g.length[0]) * g.length[0];
+        float images = image_round(image_dx, 0, g);
+        float shift = images * g.length[0];
         p2x -= shift;
         q2x -= shift;
+        moved |= images != 0.0f;
     }
     if (g.periodic[1]) {
-        float shift = roundf(image_dy / g.length[1]) * g.length[1];
+        float images = image_round(image_dy, 1, g);
+        float shift = images * g.length[1];
         p2y -= shift;
         q2y -= shift;
+        moved |= images != 0.0f;
     }
     if (g.periodic[2]) {
-        float shift = roundf(image_dz / g.length[2]) * g.length[2];
+        float images = image_round(image_dz, 2, g);
+        float shift = images * g.length[2];
         p2z -= shift;
         q2z -= shift;
+        moved |= images != 0.0f;
     }
+    return moved;
 }
 
 // neighbor.rs:27-86 with one proxy piece per segment (the canonical-pair

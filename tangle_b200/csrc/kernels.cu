@@ -19,6 +19,7 @@
 #include "kernels.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace tgl {
 
@@ -220,36 +221,76 @@ __global__ void rb_sort_cells_kernel(WorldDev w) {
     }
 }
 
-// gather_cell_slot_geometry (neighbor.rs:107-153): geometry in slot order.
+// gather_cell_slot_geometry (neighbor.rs:107-153): geometry in slot order,
+// plus each slot's bounding sphere (midpoint, half length + radius) for the
+// build's pre-test.
 __global__ void rb_gather_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.S; slot += gridDim.x * blockDim.x) {
         uint32_t s = w.cell_segments[slot];
         float4 a = w.geom[2 * (size_t)s], b = w.geom[2 * (size_t)s + 1];
-        b.w = __uint_as_float(s);
         w.slot_geom[2 * (size_t)slot] = a;
         w.slot_geom[2 * (size_t)slot + 1] = b;
+        w.slot_sphere[slot] = make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z), b.w + a.w);
     }
 }
 
-// build_segment_neighbor_lists (neighbor.rs:155-364). One block per home cell:
-// the 27 stencil cells' slots are staged in shared memory chunk by chunk and
-// each warp tests them, 32 at a time, against one home segment, appending
-// hits in scan order (sorted afterwards).
-__global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch) {
+// The exact pair test of build_segment_neighbor_lists (neighbor.rs:282-359)
+// for home segment 1 against the segment in `slot`.
+__device__ inline bool build_pair(const WorldDev &w, float p1x, float p1y, float p1z, float q1x, float q1y,
+                                  float q1z, float d1x, float d1y, float d1z, float radius, float half_length,
+                                  uint32_t segment, float4 own, uint32_t slot, uint32_t &other) {
+    const float4 oa = w.slot_geom[2 * (size_t)slot], ob = w.slot_geom[2 * (size_t)slot + 1];
+    other = w.cell_segments[slot];
+    float p2x = oa.x, p2y = oa.y, p2z = oa.z, q2x = ob.x, q2y = ob.y, q2z = ob.z;
+    const float other_radius = oa.w;
+    bool moved = minimum_image(p1x, p1y, p1z, q1x, q1y, q1z, p2x, p2y, p2z, q2x, q2y, q2z, w.grid);
+    float d2x = q2x - p2x, d2y = q2y - p2y, d2z = q2z - p2z;
+    float interaction = (radius + other_radius + w.skin) * (1.0f + 1.0e-4f);
+    float mdx = 0.5f * (p2x + q2x - p1x - q1x);
+    float mdy = 0.5f * (p2y + q2y - p1y - q1y);
+    float mdz = 0.5f * (p2z + q2z - p1z - q1z);
+    float other_half = moved ? 0.5f * sqrtf(d2x * d2x + d2y * d2y + d2z * d2z) : ob.w;
+    float reach = half_length + other_half + interaction;
+    if (!(mdx * mdx + mdy * mdy + mdz * mdz <= reach * reach)) return false;
+    if (!(axis_distance(p1x, p1y, p1z, d1x, d1y, d1z, p2x, p2y, p2z, d2x, d2y, d2z) <= interaction)) return false;
+    // The pair-independent exclusions (neighbor.rs:282-294).
+    float4 os = w.seg_static[other];
+    float gap = fmaxf(os.y - own.z, own.y - os.z);  // along_fiber_gap
+    bool near_along_fiber = __float_as_uint(os.w) == __float_as_uint(own.w) && gap < radius + os.x;
+    return other != segment && !near_along_fiber;
+}
+
+// build_segment_neighbor_lists (neighbor.rs:155-364). One block per home cell.
+// The 27 stencil cells' bounding spheres are staged in shared memory; each
+// warp takes one home segment and tests 32 candidates at a time with a
+// conservative sphere test. A pair the exact test accepts always passes it:
+// the sphere threshold exceeds the exact reach by 2e-4 relative plus an
+// absolute margin far above f32 rounding, and the sphere test's image
+// (nearest integer of the separation in box lengths, ties to even) can only
+// differ from the exact test's near a half-box separation, which with at
+// least 3 cells on every periodic axis is beyond any reach. (Coordinates are
+// unwrapped, so a segment's cell says nothing about its image.) Survivors
+// queue up and get the exact test 32 at a time; hits append in scan order
+// and are sorted later.
+__global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int prefilter, float sphere_eps) {
     if (w.ctl->neighbor_state[0] == 0) return;
     extern __shared__ float4 build_smem[];
+    uint32_t *slot_of = reinterpret_cast<uint32_t *>(build_smem + ch);
     __shared__ uint32_t st_count[27], st_off[27], st_prefix[28];
+    __shared__ uint32_t queue[8][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int warps = blockDim.x >> 5;
     const float skin = w.skin;
     const uint32_t block = w.block;
+    const Grid &g = w.grid;
+    uint32_t *q = queue[warp];
     for (uint32_t h = blockIdx.x; h < w.C; h += gridDim.x) {
         uint32_t nh = w.cell_counts[h];
         if (nh == 0) continue;
         uint32_t hoff = w.cell_offsets[h];
         if (threadIdx.x < 27) {
-            uint32_t cell = stencil_cell(h, threadIdx.x, w.grid);
+            uint32_t cell = stencil_cell(h, threadIdx.x, g);
             st_count[threadIdx.x] = cell == TGL_NONE ? 0u : w.cell_counts[cell];
             st_off[threadIdx.x] = cell == TGL_NONE ? 0u : w.cell_offsets[cell];
         }
@@ -264,62 +305,75 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch) {
         }
         __syncthreads();
         const uint32_t total = st_prefix[27];
-        for (uint32_t base = 0; base < total || base == 0; base += (uint32_t)ch) {
-            uint32_t len = total > base ? min((uint32_t)ch, total - base) : 0u;
+        for (uint32_t base = 0; base < total; base += (uint32_t)ch) {
+            uint32_t len = min((uint32_t)ch, total - base);
             for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
                 uint32_t flat = base + i;
                 int k = 0;
                 while (k < 26 && st_prefix[k + 1] <= flat) ++k;
                 uint32_t slot = st_off[k] + (flat - st_prefix[k]);
-                build_smem[2 * i] = w.slot_geom[2 * (size_t)slot];
-                build_smem[2 * i + 1] = w.slot_geom[2 * (size_t)slot + 1];
+                slot_of[i] = slot;
+                build_smem[i] = w.slot_sphere[slot];
             }
             __syncthreads();
             for (uint32_t hi = warp; hi < nh; hi += warps) {
-                float4 a = w.slot_geom[2 * (size_t)(hoff + hi)], b = w.slot_geom[2 * (size_t)(hoff + hi) + 1];
-                const uint32_t segment = __float_as_uint(b.w);
+                const uint32_t home = hoff + hi;
+                const float4 a = w.slot_geom[2 * (size_t)home], b = w.slot_geom[2 * (size_t)home + 1];
+                const float4 hs = w.slot_sphere[home];
+                const uint32_t segment = w.cell_segments[home];
                 const float p1x = a.x, p1y = a.y, p1z = a.z, radius = a.w;
                 const float q1x = b.x, q1y = b.y, q1z = b.z;
                 const float d1x = q1x - p1x, d1y = q1y - p1y, d1z = q1z - p1z;
-                const float half_length = 0.5f * sqrtf(d1x * d1x + d1y * d1y + d1z * d1z);
+                const float half_length = b.w;
                 const float4 own = w.seg_static[segment];
-                const uint32_t owner = __float_as_uint(own.w);
                 uint32_t count = base == 0 ? 0u : w.nbr_count[segment];
                 uint32_t *list = w.nbr_list + (size_t)segment * block;
-                for (uint32_t c0 = 0; c0 < len; c0 += 32) {
-                    uint32_t c = c0 + lane;
-                    bool hit = false;
-                    uint32_t other = 0;
-                    if (c < len) {
-                        float4 oa = build_smem[2 * c], ob = build_smem[2 * c + 1];
-                        other = __float_as_uint(ob.w);
-                        float p2x = oa.x, p2y = oa.y, p2z = oa.z, q2x = ob.x, q2y = ob.y, q2z = ob.z;
-                        float other_radius = oa.w;
-                        minimum_image(p1x, p1y, p1z, q1x, q1y, q1z, p2x, p2y, p2z, q2x, q2y, q2z, w.grid);
-                        float d2x = q2x - p2x, d2y = q2y - p2y, d2z = q2z - p2z;
-                        float interaction = (radius + other_radius + skin) * (1.0f + 1.0e-4f);
-                        float mdx = 0.5f * (p2x + q2x - p1x - q1x);
-                        float mdy = 0.5f * (p2y + q2y - p1y - q1y);
-                        float mdz = 0.5f * (p2z + q2z - p1z - q1z);
-                        float reach = half_length + 0.5f * sqrtf(d2x * d2x + d2y * d2y + d2z * d2z) + interaction;
-                        if (mdx * mdx + mdy * mdy + mdz * mdz <= reach * reach &&
-                            axis_distance(p1x, p1y, p1z, d1x, d1y, d1z, p2x, p2y, p2z, d2x, d2y, d2z) <= interaction) {
-                            // The pair-independent exclusions (neighbor.rs:282-294).
-                            float4 os = w.seg_static[other];
-                            float gap = fmaxf(os.y - own.z, own.y - os.z);  // along_fiber_gap
-                            bool near_along_fiber = __float_as_uint(os.w) == owner && gap < radius + os.x;
-                            hit = other != segment && !near_along_fiber;
+                uint32_t queued = 0;
+                for (uint32_t c0 = 0; c0 < len || queued; c0 += 32) {
+                    if (c0 < len) {
+                        uint32_t c = c0 + lane;
+                        bool pass = false;
+                        if (c < len) {
+                            pass = true;
+                            if (prefilter) {
+                                float4 sp = build_smem[c];
+                                float dx = sp.x - hs.x, dy = sp.y - hs.y, dz = sp.z - hs.z;
+                                if (g.periodic[0]) dx -= rintf(dx * g.inv_length[0]) * g.length[0];
+                                if (g.periodic[1]) dy -= rintf(dy * g.inv_length[1]) * g.length[1];
+                                if (g.periodic[2]) dz -= rintf(dz * g.inv_length[2]) * g.length[2];
+                                float limit = (hs.w + sp.w + skin) * 1.0002f + sphere_eps;
+                                pass = dx * dx + dy * dy + dz * dz <= limit * limit;
+                            }
                         }
+                        uint32_t ballot = __ballot_sync(FULL, pass);
+                        if (pass) q[queued + __popc(ballot & ((1u << lane) - 1u))] = c;
+                        queued += __popc(ballot);
+                        __syncwarp();
                     }
-                    uint32_t ballot = __ballot_sync(FULL, hit);
-                    uint32_t rank = __popc(ballot & ((1u << lane) - 1u));
-                    if (hit && count + rank < block) list[count + rank] = other;
-                    count += __popc(ballot);
+                    // Exact tests, 32 at a time, or the remainder at the end.
+                    if (queued >= 32 || (c0 + 32 >= len && queued)) {
+                        uint32_t n = min(queued, 32u);
+                        bool hit = false;
+                        uint32_t other = 0;
+                        if ((uint32_t)lane < n)
+                            hit = build_pair(w, p1x, p1y, p1z, q1x, q1y, q1z, d1x, d1y, d1z, radius, half_length,
+                                             segment, own, slot_of[q[lane]], other);
+                        uint32_t ballot = __ballot_sync(FULL, hit);
+                        uint32_t rank = __popc(ballot & ((1u << lane) - 1u));
+                        if (hit && count + rank < block) list[count + rank] = other;
+                        count += __popc(ballot);
+                        __syncwarp();
+                        uint32_t rest = queued - n;
+                        uint32_t moved_entry = (uint32_t)lane < rest ? q[n + lane] : 0u;
+                        __syncwarp();
+                        if ((uint32_t)lane < rest) q[lane] = moved_entry;
+                        __syncwarp();
+                        queued = rest;
+                    }
                 }
                 if (lane == 0) w.nbr_count[segment] = count;
             }
             __syncthreads();
-            if (total == 0) break;
         }
     }
 }
@@ -367,25 +421,58 @@ struct PairTerms {
     float pen, t0x, t0y, t0z, t1x, t1y, t1z, aggw;
 };
 
-// One candidate pair of find_segment_corrections (contact.rs:450-870) for a
-// round lane at zero offset: returns true with the pair's terms when the
-// capsules overlap.
-__device__ inline bool contact_pair(float p1x, float p1y, float p1z, float q1x, float q1y, float q1z, float d1x,
-                                    float d1y, float d1z, float radius, float half_length, uint32_t segment,
-                                    uint32_t other, float4 oa, float4 ob, const Grid &g, float correction_fraction,
-                                    uint32_t aggregation, PairTerms &out) {
+// Home segment of a candidate pair, as the contact pass reads it.
+struct Home {
+    float p1x, p1y, p1z, q1x, q1y, q1z, d1x, d1y, d1z, radius, half_length;
+    uint32_t segment;
+};
+
+__device__ inline Home make_home(float4 a, float4 b, uint32_t segment) {
+    Home h;
+    h.p1x = a.x;
+    h.p1y = a.y;
+    h.p1z = a.z;
+    h.radius = a.w;
+    h.q1x = b.x;
+    h.q1y = b.y;
+    h.q1z = b.z;
+    h.half_length = b.w;  // 0.5 |q1 - p1|
+    h.d1x = h.q1x - h.p1x;
+    h.d1y = h.q1y - h.p1y;
+    h.d1z = h.q1z - h.p1z;
+    h.segment = segment;
+    return h;
+}
+
+// The midpoint reject of find_segment_corrections (contact.rs:456-493):
+// shifts the candidate to its minimum image and returns whether the
+// capsules can touch.
+__device__ inline bool contact_reach(const Home &h, float4 oa, float4 ob, const Grid &g, float &p2x, float &p2y,
+                                     float &p2z, float &q2x, float &q2y, float &q2z) {
+    p2x = oa.x, p2y = oa.y, p2z = oa.z, q2x = ob.x, q2y = ob.y, q2z = ob.z;
+    bool moved = minimum_image(h.p1x, h.p1y, h.p1z, h.q1x, h.q1y, h.q1z, p2x, p2y, p2z, q2x, q2y, q2z, g);
+    float d2x = q2x - p2x, d2y = q2y - p2y, d2z = q2z - p2z;
+    float mdx = 0.5f * (p2x + q2x - h.p1x - h.q1x);
+    float mdy = 0.5f * (p2y + q2y - h.p1y - h.q1y);
+    float mdz = 0.5f * (p2z + q2z - h.p1z - h.q1z);
+    // Without a periodic shift d2 equals the unshifted q2 - p2, whose half
+    // length the geometry record carries; after a shift it is recomputed.
+    float other_half = moved ? 0.5f * sqrtf(d2x * d2x + d2y * d2y + d2z * d2z) : ob.w;
+    float reach = (h.half_length + other_half + h.radius + oa.w) * (1.0f + 1.0e-4f);
+    return mdx * mdx + mdy * mdy + mdz * mdz <= reach * reach;
+}
+
+// One candidate of find_segment_corrections past the midpoint reject
+// (contact.rs:663-870) for a round lane at zero offset: returns true with
+// the pair's terms when the capsules overlap.
+__device__ inline bool contact_solve(const Home &h, uint32_t other, float other_radius, float p2x, float p2y,
+                                     float p2z, float q2x, float q2y, float q2z, float correction_fraction,
+                                     uint32_t aggregation, PairTerms &out) {
     const float length_epsilon = 1.0e-20f;
     const float parallel_relative_epsilon = 1.0e-6f;
-    float p2x = oa.x, p2y = oa.y, p2z = oa.z, q2x = ob.x, q2y = ob.y, q2z = ob.z;
-    const float other_radius = oa.w;
-    minimum_image(p1x, p1y, p1z, q1x, q1y, q1z, p2x, p2y, p2z, q2x, q2y, q2z, g);
+    const float p1x = h.p1x, p1y = h.p1y, p1z = h.p1z, d1x = h.d1x, d1y = h.d1y, d1z = h.d1z;
+    const float radius = h.radius;
     float d2x = q2x - p2x, d2y = q2y - p2y, d2z = q2z - p2z;
-    float mdx = 0.5f * (p2x + q2x - p1x - q1x);
-    float mdy = 0.5f * (p2y + q2y - p1y - q1y);
-    float mdz = 0.5f * (p2z + q2z - p1z - q1z);
-    float reach = (half_length + 0.5f * sqrtf(d2x * d2x + d2y * d2y + d2z * d2z) + radius + other_radius) *
-                  (1.0f + 1.0e-4f);
-    if (!(mdx * mdx + mdy * mdy + mdz * mdz <= reach * reach)) return false;
     float rx = p1x - p2x, ry = p1y - p2y, rz = p1z - p2z;
     float a = d1x * d1x + d1y * d1y + d1z * d1z;
     float e = d2x * d2x + d2y * d2y + d2z * d2z;
@@ -484,7 +571,7 @@ __device__ inline bool contact_pair(float p1x, float p1y, float p1z, float q1x, 
             ny = -ny;
             nz = -nz;
         }
-        if (segment > other) {
+        if (h.segment > other) {
             nx = -nx;
             ny = -ny;
             nz = -nz;
@@ -511,140 +598,227 @@ struct ContactAcc {
     float c0x, c0y, c0z, c1x, c1y, c1z, weight, maxpen;
 };
 
-// Adds the group's hits to the running sums in ascending lane (= list)
-// order, exactly as the reference's serial loop does (contact.rs:750-870).
-template <int G>
-__device__ inline void accumulate_in_order(bool hit, const PairTerms &pt, uint32_t gmask, int gbase,
-                                           uint32_t aggregation, ContactAcc &acc) {
-    uint32_t ballot = __ballot_sync(gmask, hit);
-    uint32_t bits = G == 32 ? ballot : ((ballot >> gbase) & ((1u << G) - 1u));
-    while (bits) {
-        int j = __ffs(bits) - 1;
-        bits &= bits - 1u;
-        float pen = __shfl_sync(gmask, pt.pen, j, G);
-        float t0x = __shfl_sync(gmask, pt.t0x, j, G);
-        float t0y = __shfl_sync(gmask, pt.t0y, j, G);
-        float t0z = __shfl_sync(gmask, pt.t0z, j, G);
-        float t1x = __shfl_sync(gmask, pt.t1x, j, G);
-        float t1y = __shfl_sync(gmask, pt.t1y, j, G);
-        float t1z = __shfl_sync(gmask, pt.t1z, j, G);
-        float aggw = __shfl_sync(gmask, pt.aggw, j, G);
-        bool deepest = pen > acc.maxpen;
-        if (deepest) acc.maxpen = pen;
-        if (aggregation == 2) {
-            if (deepest) {
-                acc.c0x = t0x;
-                acc.c0y = t0y;
-                acc.c0z = t0z;
-                acc.c1x = t1x;
-                acc.c1y = t1y;
-                acc.c1z = t1z;
-                acc.weight = 1.0f;
-            }
-        } else {
-            acc.c0x += t0x;
-            acc.c0y += t0y;
-            acc.c0z += t0z;
-            acc.c1x += t1x;
-            acc.c1y += t1y;
-            acc.c1z += t1z;
-            acc.weight += aggw;
+// contact.rs:750-870 for one hit: the running sums in the reference's order.
+__device__ inline void add_hit(ContactAcc &acc, uint32_t aggregation, float pen, float t0x, float t0y, float t0z,
+                               float t1x, float t1y, float t1z, float aggw) {
+    bool deepest = pen > acc.maxpen;
+    if (deepest) acc.maxpen = pen;
+    if (aggregation == 2) {
+        if (deepest) {
+            acc.c0x = t0x;
+            acc.c0y = t0y;
+            acc.c0z = t0z;
+            acc.c1x = t1x;
+            acc.c1y = t1y;
+            acc.c1z = t1z;
+            acc.weight = 1.0f;
         }
+    } else {
+        acc.c0x += t0x;
+        acc.c0y += t0y;
+        acc.c0z += t0z;
+        acc.c1x += t1x;
+        acc.c1y += t1y;
+        acc.c1z += t1z;
+        acc.weight += aggw;
     }
 }
 
-// find_segment_corrections (contact.rs:232-902) with G lanes per segment,
-// then (gate != 0) assess_reduced_metrics in the last block to finish.
-template <int G>
-__global__ void __launch_bounds__(256) contact_kernel(WorldDev w, StepParams sp, int gate) {
-    __shared__ uint32_t warp_max[8];
+// contact.rs:879-901: average (unless deepest-only) and store.
+__device__ inline void finish_segment(const WorldDev &w, uint32_t segment, ContactAcc acc, uint32_t aggregation) {
+    if (aggregation != 2 && acc.weight > 1.0e-20f) {
+        acc.c0x /= acc.weight;
+        acc.c0y /= acc.weight;
+        acc.c0z /= acc.weight;
+        acc.c1x /= acc.weight;
+        acc.c1y /= acc.weight;
+        acc.c1z /= acc.weight;
+    }
+    w.corr[2 * (size_t)segment] = make_float4(acc.c0x, acc.c0y, acc.c0z, acc.maxpen);
+    w.corr[2 * (size_t)segment + 1] = make_float4(acc.c1x, acc.c1y, acc.c1z, 0.0f);
+}
+
+// A segment whose list overflowed: the whole warp scans the 27 cells around
+// the home cell of the positions the lists were built from
+// (contact.rs:365-437), 32 candidates at a time, summing hits in scan order.
+__device__ ContactAcc overflow_segment(const WorldDev &w, const StepParams &sp, uint32_t segment, int lane) {
+    const Grid &g = w.grid;
+    const Home h = make_home(w.geom[2 * (size_t)segment], w.geom[2 * (size_t)segment + 1], segment);
+    const float4 own = w.seg_static[segment];
+    const uint32_t owner = __float_as_uint(own.w);
+    const uint32_t v0 = w.seg_v0[segment];
+    const float4 r0 = w.ref_pos[v0], r1 = w.ref_pos[v0 + 1];
+    const uint32_t home = proxy_cell(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, g);
+    ContactAcc acc = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (uint32_t n = 0; n < 27; ++n) {
+        uint32_t cell = stencil_cell(home, n, g);
+        if (cell == TGL_NONE) continue;
+        const uint32_t count = w.cell_counts[cell];
+        const uint32_t start = w.cell_offsets[cell];
+        for (uint32_t k0 = 0; k0 < count; k0 += 32) {
+            uint32_t k = k0 + lane;
+            PairTerms pt;
+            bool hit = false;
+            if (k < count) {
+                uint32_t other = w.cell_segments[start + k];
+                float4 os = w.seg_static[other];
+                float gap = fmaxf(os.y - own.z, own.y - os.z);
+                bool near_along_fiber = __float_as_uint(os.w) == owner && gap < h.radius + os.x;
+                if (other != segment && !near_along_fiber) {
+                    float4 oa = w.geom[2 * (size_t)other], ob = w.geom[2 * (size_t)other + 1];
+                    float p2x, p2y, p2z, q2x, q2y, q2z;
+                    if (contact_reach(h, oa, ob, g, p2x, p2y, p2z, q2x, q2y, q2z))
+                        hit = contact_solve(h, other, oa.w, p2x, p2y, p2z, q2x, q2y, q2z, sp.correction_fraction,
+                                            sp.contact_aggregation, pt);
+                }
+            }
+            uint32_t bits = __ballot_sync(FULL, hit);
+            while (bits) {
+                int j = __ffs(bits) - 1;
+                bits &= bits - 1u;
+                add_hit(acc, sp.contact_aggregation, __shfl_sync(FULL, pt.pen, j), __shfl_sync(FULL, pt.t0x, j),
+                        __shfl_sync(FULL, pt.t0y, j), __shfl_sync(FULL, pt.t0z, j), __shfl_sync(FULL, pt.t1x, j),
+                        __shfl_sync(FULL, pt.t1y, j), __shfl_sync(FULL, pt.t1z, j), __shfl_sync(FULL, pt.aggw, j));
+            }
+        }
+    }
+    return acc;
+}
+
+constexpr int CONTACT_WARPS = 8;
+
+// find_segment_corrections (contact.rs:232-902) over warp-owned batches of 32
+// segments taken in cell-list order: lane i owns the i-th segment's sums. The batch's listed
+// candidates are walked as one flat sequence, 32 at a time, through the
+// exact midpoint reject; the survivors queue up in that order and get the
+// closed-form closest-point solve 32 at a time, and every hit is added to
+// its segment's sums in list order, as the reference's serial loop adds it.
+// Overflowed segments then take the exact cell scan. With `gate`, the last
+// block to finish runs assess_reduced_metrics (kernels.rs:129-162).
+__global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams sp, int gate) {
+    __shared__ float4 home_geom[CONTACT_WARPS][64];
+    __shared__ uint32_t prefix[CONTACT_WARPS][33];
+    __shared__ uint32_t queue[CONTACT_WARPS][64];
+    __shared__ uint32_t segments[CONTACT_WARPS][32];
+    __shared__ uint32_t warp_max[CONTACT_WARPS];
     __shared__ int is_last;
     if (gate && w.ctl->control[0] == 0) return;
-    const int lane = threadIdx.x & 31;
-    const int gl = lane % G;
-    const int gbase = lane - gl;
-    const uint32_t gmask = G == 32 ? FULL : (((1u << G) - 1u) << gbase);
-    const uint32_t groups = gridDim.x * (blockDim.x / G);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const Grid &g = w.grid;
+    const uint32_t block = w.block;
+    float4 *hg = home_geom[warp];
+    uint32_t *pre = prefix[warp];
+    uint32_t *q = queue[warp];
+    uint32_t *seg_of = segments[warp];
     uint32_t thread_max = 0;
-    for (uint32_t segment = (blockIdx.x * blockDim.x + threadIdx.x) / G; segment < w.S; segment += groups) {
-        const float4 a = w.geom[2 * (size_t)segment], b = w.geom[2 * (size_t)segment + 1];
-        const float p1x = a.x, p1y = a.y, p1z = a.z, radius = a.w;
-        const float q1x = b.x, q1y = b.y, q1z = b.z;
-        const float d1x = q1x - p1x, d1y = q1y - p1y, d1z = q1z - p1z;
-        const float half_length = 0.5f * sqrtf(d1x * d1x + d1y * d1y + d1z * d1z);
+    const uint32_t warps_total = gridDim.x * CONTACT_WARPS;
+    for (uint32_t base = (blockIdx.x * CONTACT_WARPS + warp) * 32u; base < w.S; base += warps_total * 32u) {
+        // Batches follow the cell list's slot order, so the 32 segments of a
+        // batch are spatial neighbors and share most of their candidates.
+        const bool valid = base + lane < w.S;
+        const uint32_t segment = valid ? w.cell_segments[base + lane] : 0u;
+        uint32_t count = valid ? w.nbr_count[segment] : 0u;
+        const bool listed = valid && count <= block;
+        uint32_t k = listed ? count : 0u;
+        uint32_t incl = k;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += t;
+        }
+        pre[lane + 1] = incl;
+        if (lane == 0) pre[0] = 0;
+        if (valid) {
+            hg[2 * lane] = w.geom[2 * (size_t)segment];
+            hg[2 * lane + 1] = w.geom[2 * (size_t)segment + 1];
+        }
+        seg_of[lane] = segment;
+        __syncwarp();
+        const uint32_t total = pre[32];
         ContactAcc acc = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-        const uint32_t listed_count = w.nbr_count[segment];
-        if (listed_count <= w.block) {
-            // Listed candidates passed the self and along-fiber exclusions
-            // when the list was built; both depend only on static data.
-            const uint32_t *list = w.nbr_list + (size_t)segment * w.block;
-            for (uint32_t k0 = 0; k0 < listed_count; k0 += G) {
-                uint32_t k = k0 + gl;
+        uint32_t queued = 0;
+        for (uint32_t f0 = 0; f0 < total || queued; f0 += 32) {
+            if (f0 < total) {
+                const uint32_t f = f0 + lane;
+                bool pass = false;
+                if (f < total) {
+                    // Owner of flat index f: the last h with pre[h] <= f.
+                    int h = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1)
+                        if (pre[h + step] <= f) h += step;
+                    const uint32_t other = __ldcs(w.nbr_list + (size_t)seg_of[h] * block + (f - pre[h]));
+                    const Home home = make_home(hg[2 * h], hg[2 * h + 1], seg_of[h]);
+                    const float4 oa = w.geom[2 * (size_t)other], ob = w.geom[2 * (size_t)other + 1];
+                    float p2x, p2y, p2z, q2x, q2y, q2z;
+                    pass = contact_reach(home, oa, ob, g, p2x, p2y, p2z, q2x, q2y, q2z);
+                }
+                const uint32_t ballot = __ballot_sync(FULL, pass);
+                if (pass) q[queued + __popc(ballot & ((1u << lane) - 1u))] = f;
+                queued += __popc(ballot);
+                __syncwarp();
+            }
+            if (queued >= 32 || (f0 + 32 >= total && queued)) {
+                const uint32_t n = min(queued, 32u);
                 PairTerms pt;
                 bool hit = false;
-                if (k < listed_count) {
-                    uint32_t other = __ldg(list + k);
-                    float4 oa = w.geom[2 * (size_t)other], ob = w.geom[2 * (size_t)other + 1];
-                    hit = contact_pair(p1x, p1y, p1z, q1x, q1y, q1z, d1x, d1y, d1z, radius, half_length, segment,
-                                       other, oa, ob, g, sp.correction_fraction, sp.contact_aggregation, pt);
+                int h = 0;
+                if ((uint32_t)lane < n) {
+                    const uint32_t f = q[lane];
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1)
+                        if (pre[h + step] <= f) h += step;
+                    const uint32_t other = w.nbr_list[(size_t)seg_of[h] * block + (f - pre[h])];
+                    const Home home = make_home(hg[2 * h], hg[2 * h + 1], seg_of[h]);
+                    const float4 oa = w.geom[2 * (size_t)other], ob = w.geom[2 * (size_t)other + 1];
+                    float p2x, p2y, p2z, q2x, q2y, q2z;
+                    contact_reach(home, oa, ob, g, p2x, p2y, p2z, q2x, q2y, q2z);
+                    hit = contact_solve(home, other, oa.w, p2x, p2y, p2z, q2x, q2y, q2z, sp.correction_fraction,
+                                        sp.contact_aggregation, pt);
                 }
-                accumulate_in_order<G>(hit, pt, gmask, gbase, sp.contact_aggregation, acc);
-            }
-        } else {
-            // Overflowed list: scan the 27 cells around the home cell of the
-            // positions the lists were built from (contact.rs:365-437).
-            const float4 own = w.seg_static[segment];
-            const uint32_t owner = __float_as_uint(own.w);
-            const uint32_t v0 = w.seg_v0[segment];
-            const float4 r0 = w.ref_pos[v0], r1 = w.ref_pos[v0 + 1];
-            const uint32_t home = proxy_cell(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, g);
-            for (uint32_t n = 0; n < 27; ++n) {
-                uint32_t cell = stencil_cell(home, n, g);
-                if (cell == TGL_NONE) continue;
-                const uint32_t count = w.cell_counts[cell];
-                const uint32_t start = w.cell_offsets[cell];
-                for (uint32_t k0 = 0; k0 < count; k0 += G) {
-                    uint32_t k = k0 + gl;
-                    PairTerms pt;
-                    bool hit = false;
-                    if (k < count) {
-                        uint32_t other = w.cell_segments[start + k];
-                        float4 os = w.seg_static[other];
-                        float gap = fmaxf(os.y - own.z, own.y - os.z);
-                        bool near_along_fiber = __float_as_uint(os.w) == owner && gap < radius + os.x;
-                        if (other != segment && !near_along_fiber) {
-                            float4 oa = w.geom[2 * (size_t)other], ob = w.geom[2 * (size_t)other + 1];
-                            hit = contact_pair(p1x, p1y, p1z, q1x, q1y, q1z, d1x, d1y, d1z, radius, half_length,
-                                               segment, other, oa, ob, g, sp.correction_fraction,
-                                               sp.contact_aggregation, pt);
-                        }
-                    }
-                    accumulate_in_order<G>(hit, pt, gmask, gbase, sp.contact_aggregation, acc);
+                uint32_t bits = __ballot_sync(FULL, hit);
+                while (bits) {
+                    const int j = __ffs(bits) - 1;
+                    bits &= bits - 1u;
+                    const int owner = __shfl_sync(FULL, h, j);
+                    const float pen = __shfl_sync(FULL, pt.pen, j);
+                    const float t0x = __shfl_sync(FULL, pt.t0x, j), t0y = __shfl_sync(FULL, pt.t0y, j),
+                                t0z = __shfl_sync(FULL, pt.t0z, j);
+                    const float t1x = __shfl_sync(FULL, pt.t1x, j), t1y = __shfl_sync(FULL, pt.t1y, j),
+                                t1z = __shfl_sync(FULL, pt.t1z, j);
+                    const float aggw = __shfl_sync(FULL, pt.aggw, j);
+                    if (lane == owner) add_hit(acc, sp.contact_aggregation, pen, t0x, t0y, t0z, t1x, t1y, t1z, aggw);
                 }
+                const uint32_t rest = queued - n;
+                const uint32_t moved_entry = (uint32_t)lane < rest ? q[n + lane] : 0u;
+                __syncwarp();
+                if ((uint32_t)lane < rest) q[lane] = moved_entry;
+                __syncwarp();
+                queued = rest;
             }
         }
-        if (sp.contact_aggregation != 2 && acc.weight > 1.0e-20f) {
-            acc.c0x /= acc.weight;
-            acc.c0y /= acc.weight;
-            acc.c0z /= acc.weight;
-            acc.c1x /= acc.weight;
-            acc.c1y /= acc.weight;
-            acc.c1z /= acc.weight;
+        if (listed) {
+            finish_segment(w, segment, acc, sp.contact_aggregation);
+            thread_max = max(thread_max, __float_as_uint(fmaxf(acc.maxpen, 0.0f)));
         }
-        if (gl == 0) {
-            w.corr[2 * (size_t)segment] = make_float4(acc.c0x, acc.c0y, acc.c0z, acc.maxpen);
-            w.corr[2 * (size_t)segment + 1] = make_float4(acc.c1x, acc.c1y, acc.c1z, 0.0f);
+        uint32_t spill = __ballot_sync(FULL, valid && !listed);
+        while (spill) {
+            const int j = __ffs(spill) - 1;
+            spill &= spill - 1u;
+            const uint32_t spilled = __shfl_sync(FULL, segment, j);
+            ContactAcc o = overflow_segment(w, sp, spilled, lane);
+            if (lane == 0) finish_segment(w, spilled, o, sp.contact_aggregation);
+            thread_max = max(thread_max, __float_as_uint(fmaxf(o.maxpen, 0.0f)));
         }
-        thread_max = max(thread_max, __float_as_uint(fmaxf(acc.maxpen, 0.0f)));
+        __syncwarp();
     }
     if (!gate) return;
     thread_max = warp_max_u32(thread_max);
-    if (lane == 0) warp_max[threadIdx.x >> 5] = thread_max;
+    if (lane == 0) warp_max[warp] = thread_max;
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t m = 0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) m = max(m, warp_max[k]);
+        for (int k = 0; k < CONTACT_WARPS; ++k) m = max(m, warp_max[k]);
         if (m) atomicMax(&w.ctl->acc[0], m);
         __threadfence();
         is_last = atomicAdd(&w.ctl->done_blocks, 1u) == gridDim.x - 1;
@@ -953,8 +1127,9 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
             }
             if (i + 1 < n) {
                 float4 y = P[i + 1];
+                float dx = y.x - x.x, dy = y.y - x.y, dz = y.z - x.z;
                 w.geom[2 * (size_t)(s0 + i)] = make_float4(x.x, x.y, x.z, radius);
-                w.geom[2 * (size_t)(s0 + i) + 1] = make_float4(y.x, y.y, y.z, __uint_as_float(v0 + i));
+                w.geom[2 * (size_t)(s0 + i) + 1] = make_float4(y.x, y.y, y.z, 0.5f * sqrtf(dx * dx + dy * dy + dz * dz));
             }
         }
         __syncwarp();
@@ -962,6 +1137,336 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
     smax = warp_max_u32(smax);
     cmax = warp_max_u32(cmax);
     bool any_far = __any_sync(FULL, far);
+    if (lane == 0) {
+        if (smax) atomicMax(&w.ctl->acc[1], smax);
+        if (cmax) atomicMax(&w.ctl->acc[2], cmax);
+        if (any_far) w.ctl->neighbor_state[0] = 1;
+    }
+}
+
+// ------------------------------------------------------ fiber update, lane per fiber
+
+constexpr int LANES_KMAX = 8;  // vertices per lane in the cooperative passes: fibers <= 256
+
+// Shared-memory vertex record of the lane-per-fiber update: xyz, and w =
+// the vertex's curvature limit with the sign bit set when it is pinned
+// (0 and -0 keep the flag for an unrestricted vertex).
+__device__ inline bool lanes_pinned(float4 p) { return signbit(p.w); }
+__device__ inline float lanes_limit(float4 p) { return fabsf(p.w); }
+
+// project_curvature_triplet_in_place (kernels.rs:1165-1322) for triplet
+// (t, t+1, t+2) of a staged fiber, split into the test (does the projection
+// move anything?) and the move, so that a lane group can test several
+// triplets at once and apply only the first that acts. A cheap test first
+// rules out triplets that certainly satisfy their limit: the limit's cosine
+// uses the same IEEE square roots as the exact path (so it is identical),
+// and the rsqrt-based cosine is within 1e-6 of the exact f32 cosine, so a
+// 1e-5 margin never skips a triplet the exact computation would project.
+__device__ inline bool lanes_test(const float4 *P, int t, float stiffness, float safety_margin, Triplet &tr) {
+    const float4 pp = P[t], pc = P[t + 1], pn = P[t + 2];
+    const float maximum_curvature = lanes_limit(pc) * (1.0f - safety_margin);
+    if (!(maximum_curvature > 0.0f)) return false;
+    const float ux = pc.x - pp.x, uy = pc.y - pp.y, uz = pc.z - pp.z;
+    const float vx = pn.x - pc.x, vy = pn.y - pc.y, vz = pn.z - pc.z;
+    const float uu = ux * ux + uy * uy + uz * uz;
+    const float vv = vx * vx + vy * vy + vz * vz;
+    const float first_length = sqrtf(uu);
+    const float second_length = sqrtf(vv);
+    if (!(first_length > 1.0e-7f && second_length > 1.0e-7f)) return false;
+    const float sine_half = 0.25f * maximum_curvature * (first_length + second_length);
+    if (!(sine_half < 1.0f)) return false;
+    const float minimum_cosine = 1.0f - 2.0f * sine_half * sine_half;
+    if (uu > 1.0e-12f && vv > 1.0e-12f &&
+        (ux * vx + uy * vy + uz * vz) * rsqrtf(uu * vv) > minimum_cosine + 1.0e-5f)
+        return false;
+    const float unx = ux / first_length, uny = uy / first_length, unz = uz / first_length;
+    const float vnx = vx / second_length, vny = vy / second_length, vnz = vz / second_length;
+    const float cosine = clampf(unx * vnx + uny * vny + unz * vnz, -1.0f, 1.0f);
+    float violation = minimum_cosine - cosine;
+    const float sine = sqrtf(fmaxf(1.0f - cosine * cosine, 0.0f));
+    if (violation > 0.0f && sine > 1.0e-3f) violation = (acos_f32(cosine) - acos_f32(minimum_cosine)) * sine;
+    if (!(violation > 0.0f)) return false;
+    tr.gux = (vnx - cosine * unx) / first_length;
+    tr.guy = (vny - cosine * uny) / first_length;
+    tr.guz = (vnz - cosine * unz) / first_length;
+    tr.gvx = (unx - cosine * vnx) / second_length;
+    tr.gvy = (uny - cosine * vny) / second_length;
+    tr.gvz = (unz - cosine * vnz) / second_length;
+    tr.cgx = tr.gux - tr.gvx;
+    tr.cgy = tr.guy - tr.gvy;
+    tr.cgz = tr.guz - tr.gvz;
+    tr.pw = lanes_pinned(pp) ? 0.0f : 1.0f;
+    tr.cw = lanes_pinned(pc) ? 0.0f : 1.0f;
+    tr.nw = lanes_pinned(pn) ? 0.0f : 1.0f;
+    const float denominator = tr.pw * (tr.gux * tr.gux + tr.guy * tr.guy + tr.guz * tr.guz) +
+                              tr.cw * (tr.cgx * tr.cgx + tr.cgy * tr.cgy + tr.cgz * tr.cgz) +
+                              tr.nw * (tr.gvx * tr.gvx + tr.gvy * tr.gvy + tr.gvz * tr.gvz);
+    if (!(denominator > 1.0e-12f)) return false;
+    tr.scale = stiffness * violation / denominator;
+    return tr.pw > 0.0f || tr.cw > 0.0f || tr.nw > 0.0f;
+}
+
+__device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float extent, const Grid &g) {
+    const float4 pp = P[t], pc = P[t + 1], pn = P[t + 2];
+    float4 a = pp, b = pc, c = pn;
+    if (tr.pw > 0.0f) {
+        a.x = wall_clamp(pp.x - tr.pw * tr.scale * tr.gux, extent, 0, g);
+        a.y = wall_clamp(pp.y - tr.pw * tr.scale * tr.guy, extent, 1, g);
+        a.z = wall_clamp(pp.z - tr.pw * tr.scale * tr.guz, extent, 2, g);
+    }
+    if (tr.cw > 0.0f) {
+        b.x = wall_clamp(pc.x + tr.cw * tr.scale * tr.cgx, extent, 0, g);
+        b.y = wall_clamp(pc.y + tr.cw * tr.scale * tr.cgy, extent, 1, g);
+        b.z = wall_clamp(pc.z + tr.cw * tr.scale * tr.cgz, extent, 2, g);
+    }
+    if (tr.nw > 0.0f) {
+        c.x = wall_clamp(pn.x + tr.nw * tr.scale * tr.gvx, extent, 0, g);
+        c.y = wall_clamp(pn.y + tr.nw * tr.scale * tr.gvy, extent, 1, g);
+        c.z = wall_clamp(pn.z + tr.nw * tr.scale * tr.gvz, extent, 2, g);
+    }
+    P[t] = a;
+    P[t + 1] = b;
+    P[t + 2] = c;
+}
+
+// Everything after the gate for 32/LPF fibers per warp (fibers of at most
+// 256 vertices), LPF lanes per fiber in the curvature sweeps. The warp stages
+// the fibers in shared memory and runs the internal stretch/bend passes
+// (kernels.rs:1027-1163, :1417-1453) and the contact step (:1455-1537)
+// cooperatively, one fiber at a time. Then each group of LPF lanes runs
+// project_fiber_curvature_in_place (:1324-1415) on its fiber: the group tests
+// LPF consecutive triplets on the current positions; every triplet before
+// the first acting one is a no-op in the serial order, so applying that one
+// and resuming right after it reproduces the serial sweep exactly. Last the
+// warp writes the fibers back with the displacement check
+// (neighbor.rs:446-465) and the next gate's curvature and step maxima
+// (:925-980, :95-127).
+template <int LPF>
+__global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepParams sp, int stride) {
+    constexpr int FPW = 32 / LPF;  // fibers per warp
+    if (w.ctl->control[0] == 0) return;
+    extern __shared__ float4 lanes_smem[];
+    const int lane = threadIdx.x;
+    const int group = lane / LPF, gl = lane % LPF;
+    const uint32_t gmask = LPF == 32 ? FULL : (((1u << LPF) - 1u) << (group * LPF));
+    const Grid &g = w.grid;
+    const float md = 0.5f * w.skin;
+    uint32_t smax = 0, cmax = 0;
+    bool far = false;
+    for (uint32_t batch = blockIdx.x; batch * FPW < w.F; batch += gridDim.x) {
+        const uint32_t slot = batch * FPW + group;
+        const uint32_t mine = slot < w.F ? w.fiber_order[slot] : TGL_NONE;
+        for (int j = 0; j < FPW; ++j) {
+            const uint32_t f = __shfl_sync(FULL, mine, j * LPF);
+            if (f == TGL_NONE) continue;
+            const uint2 span = w.fiber_vspan[f];
+            const uint32_t v0 = span.x;
+            const int n = (int)span.y;
+            const uint32_t s0 = w.fiber_s0[f];
+            const float extent = w.seg_static[s0].x;
+            float4 *P = lanes_smem + (size_t)j * stride;
+            for (int i = lane; i < n; i += 32) {
+                float4 p = w.pos[v0 + i];
+                const float limit = w.vtx_static[v0 + i].x;
+                p.w = w.pinned[v0 + i] ? -limit : limit;
+                if (w.pinned[v0 + i] && limit == 0.0f) p.w = -0.0f;
+                P[i] = p;
+            }
+            __syncwarp();
+            // find/apply_internal_corrections x constraint_iterations (Jacobi).
+            for (uint32_t pass = 0; pass < sp.constraint_iterations; ++pass) {
+                float cxs[LANES_KMAX], cys[LANES_KMAX], czs[LANES_KMAX];
+#pragma unroll
+                for (int k = 0; k < LANES_KMAX; ++k) {
+                    const int i = lane + 32 * k;
+                    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+                    if (i < n) {
+                        const float4 x = P[i];
+                        if (!lanes_pinned(x)) {
+                            if (i > 0) {
+                                float4 o = P[i - 1];
+                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                                if (length > 1.0e-7f) {
+                                    float magnitude = 0.5f * sp.stretch_stiffness * (length - w.rest[s0 + i - 1]) / length;
+                                    cx += dx * magnitude;
+                                    cy += dy * magnitude;
+                                    cz += dz * magnitude;
+                                }
+                            }
+                            if (i + 1 < n) {
+                                float4 o = P[i + 1];
+                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                                if (length > 1.0e-7f) {
+                                    float magnitude = 0.5f * sp.stretch_stiffness * (length - w.rest[s0 + i]) / length;
+                                    cx += dx * magnitude;
+                                    cy += dy * magnitude;
+                                    cz += dz * magnitude;
+                                }
+                            }
+                            if (i > 1) {
+                                float4 o = P[i - 2];
+                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                                if (length > 1.0e-7f) {
+                                    float magnitude = 0.5f * sp.bend_stiffness * (length - w.vtx_static[v0 + i].y) / length;
+                                    cx += dx * magnitude;
+                                    cy += dy * magnitude;
+                                    cz += dz * magnitude;
+                                }
+                            }
+                            if (i + 2 < n) {
+                                float4 o = P[i + 2];
+                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                                if (length > 1.0e-7f) {
+                                    float magnitude = 0.5f * sp.bend_stiffness * (length - w.vtx_static[v0 + i].z) / length;
+                                    cx += dx * magnitude;
+                                    cy += dy * magnitude;
+                                    cz += dz * magnitude;
+                                }
+                            }
+                        }
+                    }
+                    cxs[k] = cx;
+                    cys[k] = cy;
+                    czs[k] = cz;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int k = 0; k < LANES_KMAX; ++k) {
+                    const int i = lane + 32 * k;
+                    if (i < n) {
+                        float4 x = P[i];
+                        if (!lanes_pinned(x)) {
+                            x.x = wall_clamp(x.x + cxs[k], extent, 0, g);
+                            x.y = wall_clamp(x.y + cys[k], extent, 1, g);
+                            x.z = wall_clamp(x.z + czs[k], extent, 2, g);
+                            P[i] = x;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            // apply_contact_corrections (flexible).
+            for (int i = lane; i < n; i += 32) {
+                float4 x = P[i];
+                float step = 0.0f;
+                if (!lanes_pinned(x)) {
+                    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+                    if (i > 0) {
+                        float4 c1 = w.corr[2 * (size_t)(s0 + i - 1) + 1];
+                        cx += c1.x;
+                        cy += c1.y;
+                        cz += c1.z;
+                    }
+                    if (i + 1 < n) {
+                        float4 c0 = w.corr[2 * (size_t)(s0 + i)];
+                        cx += c0.x;
+                        cy += c0.y;
+                        cz += c0.z;
+                    }
+                    float length = sqrtf(cx * cx + cy * cy + cz * cz);
+                    if (length > sp.max_step) {
+                        float scale = sp.max_step / length;
+                        cx *= scale;
+                        cy *= scale;
+                        cz *= scale;
+                    }
+                    x.x = wall_clamp(x.x + cx, extent, 0, g);
+                    x.y = wall_clamp(x.y + cy, extent, 1, g);
+                    x.z = wall_clamp(x.z + cz, extent, 2, g);
+                    P[i] = x;
+                    step = sqrtf(cx * cx + cy * cy + cz * cz);
+                }
+                w.vertex_step[v0 + i] = step;
+                smax = max(smax, __float_as_uint(fmaxf(step, 0.0f)));
+            }
+            __syncwarp();
+        }
+        // Curvature Gauss-Seidel, LPF lanes per fiber, forward then backward.
+        if (mine != TGL_NONE) {
+            const uint2 span = w.fiber_vspan[mine];
+            const int last = (int)span.y - 3;
+            const float extent = w.seg_static[w.fiber_s0[mine]].x;
+            float4 *P = lanes_smem + (size_t)group * stride;
+            for (uint32_t sweep = 0; sweep < sp.curvature_cleanup_sweeps; ++sweep) {
+                int t0 = 0;
+                while (t0 <= last) {
+                    const int t = t0 + gl;
+                    Triplet tr;
+                    const bool act = t <= last && lanes_test(P, t, sp.curvature_limit_stiffness,
+                                                             sp.curvature_limit_safety_margin, tr);
+                    const uint32_t bits = LPF == 32 ? __ballot_sync(gmask, act)
+                                                    : (__ballot_sync(gmask, act) >> (group * LPF)) & ((1u << LPF) - 1u);
+                    if (bits == 0) {
+                        t0 += LPF;
+                        continue;
+                    }
+                    const int first = __ffs(bits) - 1;
+                    if (gl == first) lanes_apply(P, t, tr, extent, g);
+                    __syncwarp(gmask);
+                    t0 += first + 1;
+                }
+                t0 = last;
+                while (t0 >= 0) {
+                    const int t = t0 - gl;
+                    Triplet tr;
+                    const bool act = t >= 0 && lanes_test(P, t, sp.curvature_limit_stiffness,
+                                                          sp.curvature_limit_safety_margin, tr);
+                    const uint32_t bits = LPF == 32 ? __ballot_sync(gmask, act)
+                                                    : (__ballot_sync(gmask, act) >> (group * LPF)) & ((1u << LPF) - 1u);
+                    if (bits == 0) {
+                        t0 -= LPF;
+                        continue;
+                    }
+                    const int first = __ffs(bits) - 1;
+                    if (gl == first) lanes_apply(P, t, tr, extent, g);
+                    __syncwarp(gmask);
+                    t0 -= first + 1;
+                }
+            }
+        }
+        __syncwarp();
+        // Write back; displacement check; next gate's curvature ratios;
+        // geometry records for the next contact pass.
+        for (int j = 0; j < FPW; ++j) {
+            const uint32_t f = __shfl_sync(FULL, mine, j * LPF);
+            if (f == TGL_NONE) continue;
+            const uint2 span = w.fiber_vspan[f];
+            const uint32_t v0 = span.x;
+            const int n = (int)span.y;
+            const uint32_t s0 = w.fiber_s0[f];
+            const float radius = w.seg_static[s0].x;
+            const float4 *P = lanes_smem + (size_t)j * stride;
+            for (int i = lane; i < n; i += 32) {
+                const float4 x = P[i];
+                w.pos[v0 + i] = make_float4(x.x, x.y, x.z, 0.0f);
+                const float4 r = w.ref_pos[v0 + i];
+                const float dx = x.x - r.x, dy = x.y - r.y, dz = x.z - r.z;
+                if (dx * dx + dy * dy + dz * dz > md * md) far = true;
+                if (i > 0 && i + 1 < n) {
+                    const float maximum = lanes_limit(x);
+                    if (maximum > 0.0f) {
+                        const float ratio = curvature_ratio_at([&](int k) { return P[k]; }, i, maximum);
+                        cmax = max(cmax, __float_as_uint(fmaxf(ratio, 0.0f)));
+                    }
+                }
+                if (i + 1 < n) {
+                    const float4 y = P[i + 1];
+                    const float ex = y.x - x.x, ey = y.y - x.y, ez = y.z - x.z;
+                    w.geom[2 * (size_t)(s0 + i)] = make_float4(x.x, x.y, x.z, radius);
+                    w.geom[2 * (size_t)(s0 + i) + 1] =
+                        make_float4(y.x, y.y, y.z, 0.5f * sqrtf(ex * ex + ey * ey + ez * ez));
+                }
+            }
+        }
+        __syncwarp();
+    }
+    smax = warp_max_u32(smax);
+    cmax = warp_max_u32(cmax);
+    const bool any_far = __any_sync(FULL, far);
     if (lane == 0) {
         if (smax) atomicMax(&w.ctl->acc[1], smax);
         if (cmax) atomicMax(&w.ctl->acc[2], cmax);
@@ -981,8 +1486,9 @@ __global__ void refresh_geometry_kernel(WorldDev w) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < w.S; s += gridDim.x * blockDim.x) {
         uint32_t v0 = w.seg_v0[s];
         float4 a = w.pos[v0], b = w.pos[v0 + 1];
+        float dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
         w.geom[2 * (size_t)s] = make_float4(a.x, a.y, a.z, w.seg_static[s].x);
-        w.geom[2 * (size_t)s + 1] = make_float4(b.x, b.y, b.z, __uint_as_float(v0));
+        w.geom[2 * (size_t)s + 1] = make_float4(b.x, b.y, b.z, 0.5f * sqrtf(dx * dx + dy * dy + dz * dz));
     }
 }
 
@@ -1022,8 +1528,8 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&lp.num_sms, cudaDevAttrMultiProcessorCount, device);
     if (lp.num_sms <= 0) lp.num_sms = 148;
-    if (lp.contact_group != 8 && lp.contact_group != 16 && lp.contact_group != 32) lp.contact_group = 8;
-    lp.contact_blocks = grid_for((uint64_t)w.S * lp.contact_group, 256, lp.num_sms * 32);
+    lp.contact_group = 32;
+    lp.contact_blocks = grid_for((w.S + 31) / 32, CONTACT_WARPS, lp.num_sms * 3);
     // Update kernel: as many warps per block as fit 96 KB of staged fibers.
     size_t per_warp = (size_t)3 * w.max_fiber * sizeof(float4);
     int warps = 8;
@@ -1031,13 +1537,39 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     lp.fiber_warps = warps;
     lp.fiber_smem = per_warp * warps;
     lp.fiber_blocks = grid_for(w.F, warps, 1 << 20);
-    lp.build_ch = 1536;
-    lp.build_smem = (size_t)lp.build_ch * 2 * sizeof(float4);
+    // Lane-per-fiber update for fibers of at most 32 * LANES_KMAX vertices:
+    // 32 fibers per warp, an odd float4 stride per fiber so that the lanes'
+    // same-index accesses spread over the banks.
+    if (const char *env = std::getenv("TGL_LANES_PER_FIBER")) lp.lanes_per_fiber = std::atoi(env);
+    if (lp.lanes_per_fiber != 2 && lp.lanes_per_fiber != 4 && lp.lanes_per_fiber != 8 && lp.lanes_per_fiber != 32)
+        lp.lanes_per_fiber = 8;
+    const int fpw = 32 / lp.lanes_per_fiber;
+    lp.lanes_stride = (int)(w.max_fiber | 1u);
+    lp.lanes_smem = (size_t)fpw * lp.lanes_stride * sizeof(float4);
+    lp.fiber_lanes = w.max_fiber <= 32u * LANES_KMAX && lp.lanes_smem <= 200 * 1024;
+    lp.lanes_blocks = (int)((w.F + fpw - 1) / fpw);
+    lp.build_ch = 3072;
+    lp.build_smem = (size_t)lp.build_ch * (sizeof(float4) + sizeof(uint32_t));
+    // The sphere pre-test needs >= 3 cells on every periodic axis (see
+    // rb_build_kernel); its absolute margin is 1e-6 of the largest box edge.
+    lp.build_prefilter = 1;
+    float edge = 0.0f;
+    for (int a = 0; a < 3; ++a) {
+        if (w.grid.periodic[a] && w.grid.cells[a] < 3) lp.build_prefilter = 0;
+        edge = std::max(edge, w.grid.length[a]);
+    }
+    lp.build_sphere_eps = 1.0e-6f * edge;
     int sw = 8;
     while (sw > 1 && (size_t)sw * w.block * 4 > 96 * 1024) sw >>= 1;
     lp.sort_warps = sw;
     lp.sort_smem = (size_t)sw * w.block * 4;
     cudaFuncSetAttribute(fiber_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(lp.fiber_smem, 1));
+    if (lp.fiber_lanes) {
+        cudaFuncSetAttribute(fiber_lanes_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.lanes_smem);
+        cudaFuncSetAttribute(fiber_lanes_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.lanes_smem);
+        cudaFuncSetAttribute(fiber_lanes_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.lanes_smem);
+        cudaFuncSetAttribute(fiber_lanes_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.lanes_smem);
+    }
     cudaFuncSetAttribute(rb_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.build_smem);
     cudaFuncSetAttribute(rb_sort_lists_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(lp.sort_smem, 1));
 }
@@ -1070,7 +1602,8 @@ int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
     rb_scatter_kernel<<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
     rb_sort_cells_kernel<<<grid_for(w.C, 8, cap), 256, 8 * CELL_SORT_CAP * sizeof(uint32_t), st>>>(w);
     rb_gather_kernel<<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
-    rb_build_kernel<<<(int)std::min<uint64_t>(w.C, (uint64_t)lp.num_sms * 64), 256, lp.build_smem, st>>>(w, lp.build_ch);
+    rb_build_kernel<<<(int)std::min<uint64_t>(w.C, (uint64_t)lp.num_sms * 64), 256, lp.build_smem, st>>>(
+        w, lp.build_ch, lp.build_prefilter, lp.build_sphere_eps);
     rb_sort_lists_kernel<<<grid_for(w.S, lp.sort_warps, cap), lp.sort_warps * 32, lp.sort_smem, st>>>(w);
     rb_snapshot_kernel<<<grid_for(w.V, 256, cap), 256, 0, st>>>(w);
     rb_finish_kernel<<<1, 1, 0, st>>>(w.ctl);
@@ -1078,16 +1611,20 @@ int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
 }
 
 int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, bool gate, cudaStream_t st) {
-    switch (lp.contact_group) {
-        case 32: contact_kernel<32><<<lp.contact_blocks, 256, 0, st>>>(w, sp, gate ? 1 : 0); break;
-        case 16: contact_kernel<16><<<lp.contact_blocks, 256, 0, st>>>(w, sp, gate ? 1 : 0); break;
-        default: contact_kernel<8><<<lp.contact_blocks, 256, 0, st>>>(w, sp, gate ? 1 : 0); break;
-    }
+    contact_kernel<<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, gate ? 1 : 0);
     return 1;
 }
 
 int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st) {
-    fiber_kernel<<<lp.fiber_blocks, lp.fiber_warps * 32, lp.fiber_smem, st>>>(w, sp);
+    if (lp.fiber_lanes) {
+        switch (lp.lanes_per_fiber) {
+            case 2: fiber_lanes_kernel<2><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+            case 8: fiber_lanes_kernel<8><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+            case 32: fiber_lanes_kernel<32><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+            default: fiber_lanes_kernel<4><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+        }
+    } else
+        fiber_kernel<<<lp.fiber_blocks, lp.fiber_warps * 32, lp.fiber_smem, st>>>(w, sp);
     return 1;
 }
 

@@ -18,13 +18,14 @@ struct WorldDev {
     const uint32_t *seg_v0;     // [S] first vertex (second = first + 1)
     const uint2 *fiber_vspan;   // [F] first vertex, vertex count
     const uint32_t *fiber_s0;   // [F] first segment
+    const uint32_t *fiber_order; // [F] fibers by descending vertex count
     const float4 *vtx_static;   // [V] max curvature, rest chord to v-2, rest chord to v+2, wall extent
     const uint32_t *pinned;     // [V]
     const float *rest;          // [S] rest lengths
     // Resident state.
     float4 *pos;      // [V] xyz, w = 0
     float4 *ref_pos;  // [V] positions the lists were built from
-    float4 *geom;     // [2S] {first xyz, radius}, {second xyz, first-vertex bits}
+    float4 *geom;     // [2S] {first xyz, radius}, {second xyz, half length}
     float4 *corr;     // [2S] {end-0 correction, max penetration}, {end-1 correction, 0}
     float *vertex_step; // [V]
     // Cell list.
@@ -33,7 +34,8 @@ struct WorldDev {
     uint32_t *cell_segments; // [S] segment per slot, cell order
     uint32_t *cell_of;       // [S] cell of each segment
     uint32_t *ticket;        // [S] scatter position inside its cell; sort scratch
-    float4 *slot_geom;       // [2S] geometry in slot order, w of the second = segment bits
+    float4 *slot_geom;       // [2S] geometry records in slot order
+    float4 *slot_sphere;     // [S] midpoint and half length + radius, slot order
     // Verlet lists.
     uint32_t *nbr_count; // [S] true neighbor count
     uint32_t *nbr_list;  // [S * block]
@@ -65,8 +67,15 @@ struct LaunchPlan {
     int fiber_warps;        // fibers per block of the update kernel
     int fiber_blocks;
     size_t fiber_smem;
+    bool fiber_lanes;       // grouped-lane update (fibers of at most 256 vertices)
+    int lanes_per_fiber;    // lanes per fiber in its curvature sweeps (2, 4, 8 or 32)
+    int lanes_stride;
+    size_t lanes_smem;
+    int lanes_blocks;
     int build_ch;           // candidate slots staged per build chunk
     size_t build_smem;
+    int build_prefilter;    // sphere pre-test on (needs >= 3 cells per periodic axis)
+    float build_sphere_eps; // its absolute margin
     int sort_warps;
     size_t sort_smem;
 };

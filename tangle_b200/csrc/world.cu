@@ -299,6 +299,7 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
         grid.cells[a] = f32_to_u32_host(std::fmax(std::floor(extent / w->cell_size), 1.0f));
         grid.length[a] = extent;
         grid.width[a] = extent / (float)grid.cells[a];
+        grid.inv_length[a] = 1.0f / extent;
         C *= grid.cells[a];
     }
     if (C > (1ull << 31)) return fail(set_error(TGL_ERR_UNSUPPORTED, "cell grid too large: the cell size is tiny against the box"));
@@ -349,6 +350,11 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
             pinned[v] = pk->vertex_pinned && pk->vertex_pinned[v] ? 1u : 0u;
         }
     }
+    // Fibers by descending vertex count, so a warp's 32 fibers finish together.
+    std::vector<uint32_t> fiber_order(F);
+    for (uint32_t f = 0; f < F; ++f) fiber_order[f] = f;
+    std::stable_sort(fiber_order.begin(), fiber_order.end(),
+                     [&](uint32_t a, uint32_t b) { return fiber_vspan[a].y > fiber_vspan[b].y; });
     std::vector<float4> seg_static(S);
     std::vector<uint32_t> seg_v0(S);
     std::vector<float> rest(pk->segment_rest_lengths, pk->segment_rest_lengths + S);
@@ -360,10 +366,9 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
         std::memcpy(&fb, &fiber, 4);
         seg_static[s] = make_float4(pk->segment_radii[s], arc[a], arc[b], fb);
         seg_v0[s] = a;
-        float ab;
-        std::memcpy(&ab, &a, 4);
+        float dx = P[3 * b] - P[3 * a], dy = P[3 * b + 1] - P[3 * a + 1], dz = P[3 * b + 2] - P[3 * a + 2];
         geom[2 * (size_t)s] = make_float4(P[3 * a], P[3 * a + 1], P[3 * a + 2], pk->segment_radii[s]);
-        geom[2 * (size_t)s + 1] = make_float4(P[3 * b], P[3 * b + 1], P[3 * b + 2], ab);
+        geom[2 * (size_t)s + 1] = make_float4(P[3 * b], P[3 * b + 1], P[3 * b + 2], 0.5f * std::sqrt(dx * dx + dy * dy + dz * dz));
     }
     std::vector<float4> pos(V);
     for (uint32_t v = 0; v < V; ++v) pos[v] = make_float4(P[3 * v], P[3 * v + 1], P[3 * v + 2], 0.0f);
@@ -379,18 +384,19 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
     d.grid = grid;
     int rc = 0;
     float4 *seg_static_d, *vtx_static_d;
-    uint32_t *seg_v0_d, *fiber_s0_d, *pinned_d;
+    uint32_t *seg_v0_d, *fiber_s0_d, *pinned_d, *fiber_order_d;
     uint2 *fiber_vspan_d;
     float *rest_d;
     if ((rc = w->upload(&seg_static_d, seg_static)) || (rc = w->upload(&seg_v0_d, seg_v0)) ||
         (rc = w->upload(&fiber_vspan_d, fiber_vspan)) || (rc = w->upload(&fiber_s0_d, fiber_s0)) ||
+        (rc = w->upload(&fiber_order_d, fiber_order)) ||
         (rc = w->upload(&vtx_static_d, vtx_static)) || (rc = w->upload(&pinned_d, pinned)) ||
         (rc = w->upload(&rest_d, rest)) || (rc = w->upload(&d.pos, pos)) || (rc = w->upload(&d.ref_pos, pos)) ||
         (rc = w->upload(&d.geom, geom)) || (rc = w->alloc(&d.corr, 2 * (size_t)S)) ||
         (rc = w->alloc(&d.vertex_step, V)) || (rc = w->alloc(&d.cell_counts, C)) ||
         (rc = w->alloc(&d.cell_offsets, C)) || (rc = w->alloc(&d.cell_segments, S)) ||
         (rc = w->alloc(&d.cell_of, S)) || (rc = w->alloc(&d.ticket, S)) ||
-        (rc = w->alloc(&d.slot_geom, 2 * (size_t)S)) || (rc = w->alloc(&d.nbr_count, S)) ||
+        (rc = w->alloc(&d.slot_geom, 2 * (size_t)S)) || (rc = w->alloc(&d.slot_sphere, S)) || (rc = w->alloc(&d.nbr_count, S)) ||
         (rc = w->alloc(&d.nbr_list, std::max<uint64_t>((uint64_t)S * block, 1))) || (rc = w->alloc(&d.ctl, 1)) ||
         (rc = w->alloc(&d.xyz_stage, 3 * (size_t)V)))
         return fail(rc);
@@ -398,6 +404,7 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
     d.seg_v0 = seg_v0_d;
     d.fiber_vspan = fiber_vspan_d;
     d.fiber_s0 = fiber_s0_d;
+    d.fiber_order = fiber_order_d;
     d.vtx_static = vtx_static_d;
     d.pinned = pinned_d;
     d.rest = rest_d;
@@ -413,6 +420,12 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
         cudaMemset(d.cell_offsets, 0, C * sizeof(uint32_t)) != cudaSuccess ||
         cudaMemset(d.nbr_count, 0, S * sizeof(uint32_t)) != cudaSuccess)
         return fail(set_error(TGL_ERR_CUDA, "device initialisation failed"));
+    {  // Any permutation works before the first rebuild replaces it.
+        std::vector<uint32_t> iota(S);
+        for (uint32_t s = 0; s < S; ++s) iota[s] = s;
+        if (cudaMemcpy(d.cell_segments, iota.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(set_error(TGL_ERR_CUDA, "device initialisation failed"));
+    }
     plan_launches(d, w->lp);
     *out = w;
     return 0;
