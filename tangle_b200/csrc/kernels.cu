@@ -462,6 +462,28 @@ __device__ inline bool contact_reach(const Home &h, float4 oa, float4 ob, const 
     return mdx * mdx + mdy * mdy + mdz * mdz <= reach * reach;
 }
 
+// A lower bound test on the capsules' overlap: the segments lie on their
+// axis lines, so their distance is at least the lines' distance
+// |(p2 - p1) . (d1 x d2)| / |d1 x d2|. When that exceeds r1 + r2 by a margin
+// (1e-3 relative plus `eps`, above every f32 rounding in this bound and in
+// the closest-point solve), the solve's penetration is certainly negative.
+// Axes closer to parallel than 0.01 rad (where d1 x d2 loses relative
+// accuracy) give no bound.
+__device__ inline bool lines_may_touch(const Home &h, float p2x, float p2y, float p2z, float q2x, float q2y,
+                                       float q2z, float other_radius, float eps) {
+    const float d2x = q2x - p2x, d2y = q2y - p2y, d2z = q2z - p2z;
+    const float nx = h.d1y * d2z - h.d1z * d2y;
+    const float ny = h.d1z * d2x - h.d1x * d2z;
+    const float nz = h.d1x * d2y - h.d1y * d2x;
+    const float nn = nx * nx + ny * ny + nz * nz;
+    const float aa = h.d1x * h.d1x + h.d1y * h.d1y + h.d1z * h.d1z;
+    const float ee = d2x * d2x + d2y * d2y + d2z * d2z;
+    if (!(nn > 1.0e-4f * aa * ee)) return true;
+    const float rn = (p2x - h.p1x) * nx + (p2y - h.p1y) * ny + (p2z - h.p1z) * nz;
+    const float threshold = (h.radius + other_radius) * 1.001f + eps;
+    return rn * rn <= threshold * threshold * nn;
+}
+
 // One candidate of find_segment_corrections past the midpoint reject
 // (contact.rs:663-870) for a round lane at zero offset: returns true with
 // the pair's terms when the capsules overlap.
@@ -685,6 +707,35 @@ __device__ ContactAcc overflow_segment(const WorldDev &w, const StepParams &sp, 
     return acc;
 }
 
+// Owner segment (batch lane) of flat candidate index f: the last h with
+// pre[h] <= f (segments without candidates share their successor's start).
+__device__ inline int owner_of(const uint32_t *pre, uint32_t f) {
+    int h = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1)
+        if (pre[h + step] <= f) h += step;
+    return h;
+}
+
+// Neighbor-list entries are read once per pass: stream them past L2.
+__device__ inline uint32_t load_stream(const uint32_t *p) { return __ldcs(p); }
+
+// Geometry records are gathered many times per pass: keep them in L2 ahead
+// of the streamed lists (a per-load cache-eviction hint, no cache state kept).
+__device__ inline uint64_t make_keep_policy() {
+    uint64_t policy;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(policy));
+    return policy;
+}
+
+__device__ inline float4 load_keep(const float4 *p, uint64_t policy) {
+    float4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(policy));
+    return v;
+}
+
 constexpr int CONTACT_WARPS = 8;
 
 // find_segment_corrections (contact.rs:232-902) over warp-owned batches of 32
@@ -695,10 +746,11 @@ constexpr int CONTACT_WARPS = 8;
 // its segment's sums in list order, as the reference's serial loop adds it.
 // Overflowed segments then take the exact cell scan. With `gate`, the last
 // block to finish runs assess_reduced_metrics (kernels.rs:129-162).
-__global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams sp, int gate) {
+__global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams sp, int gate, float line_eps) {
     __shared__ float4 home_geom[CONTACT_WARPS][64];
     __shared__ uint32_t prefix[CONTACT_WARPS][33];
-    __shared__ uint32_t queue[CONTACT_WARPS][64];
+    __shared__ float4 queue_geom[CONTACT_WARPS][128];  // 64 entries: {p2, r2}, {q2, other}
+    __shared__ uint8_t queue_owner[CONTACT_WARPS][64];
     __shared__ uint32_t segments[CONTACT_WARPS][32];
     __shared__ uint32_t warp_max[CONTACT_WARPS];
     __shared__ int is_last;
@@ -708,10 +760,12 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     const uint32_t block = w.block;
     float4 *hg = home_geom[warp];
     uint32_t *pre = prefix[warp];
-    uint32_t *q = queue[warp];
+    float4 *qg = queue_geom[warp];
+    uint8_t *qo = queue_owner[warp];
     uint32_t *seg_of = segments[warp];
     uint32_t thread_max = 0;
     const uint32_t warps_total = gridDim.x * CONTACT_WARPS;
+    const uint64_t geom_policy = make_keep_policy();
     for (uint32_t base = (blockIdx.x * CONTACT_WARPS + warp) * 32u; base < w.S; base += warps_total * 32u) {
         // Batches follow the cell list's slot order, so the 32 segments of a
         // batch are spatial neighbors and share most of their candidates.
@@ -737,24 +791,60 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         const uint32_t total = pre[32];
         ContactAcc acc = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
         uint32_t queued = 0;
+        // Software pipeline over the flat candidate sequence: the list entry
+        // of round r + 2 and the geometry of round r + 1 are in flight while
+        // round r is tested.
+        int h_next = 0, h_next2 = 0;
+        uint32_t other_next = 0, other_next2 = 0;
+        float4 oa_next = make_float4(0.0f, 0.0f, 0.0f, 0.0f), ob_next = oa_next;
+        if (lane < (int)total) {
+            h_next = owner_of(pre, lane);
+            other_next = load_stream(w.nbr_list + (size_t)seg_of[h_next] * block + (lane - pre[h_next]));
+        }
+        if (32u + lane < total) {
+            h_next2 = owner_of(pre, 32u + lane);
+            other_next2 = load_stream(w.nbr_list + (size_t)seg_of[h_next2] * block + (32u + lane - pre[h_next2]));
+        }
+        if (lane < (int)total) {
+            oa_next = load_keep(w.geom + 2 * (size_t)other_next, geom_policy);
+            ob_next = load_keep(w.geom + 2 * (size_t)other_next + 1, geom_policy);
+        }
         for (uint32_t f0 = 0; f0 < total || queued; f0 += 32) {
             if (f0 < total) {
                 const uint32_t f = f0 + lane;
+                const int h = h_next;
+                const uint32_t other = other_next;
+                const float4 oa = oa_next, ob = ob_next;
+                // Advance the pipeline.
+                h_next = h_next2;
+                other_next = other_next2;
+                if (f + 32 < total) {
+                    oa_next = load_keep(w.geom + 2 * (size_t)other_next, geom_policy);
+                    ob_next = load_keep(w.geom + 2 * (size_t)other_next + 1, geom_policy);
+                }
+                if (f + 64 < total) {
+                    h_next2 = owner_of(pre, f + 64);
+                    other_next2 = load_stream(w.nbr_list + (size_t)seg_of[h_next2] * block + (f + 64 - pre[h_next2]));
+                }
                 bool pass = false;
+                float p2x = 0.0f, p2y = 0.0f, p2z = 0.0f, q2x = 0.0f, q2y = 0.0f, q2z = 0.0f, r2 = 0.0f;
+                uint32_t other_id = 0;
+                int owner = 0;
                 if (f < total) {
-                    // Owner of flat index f: the last h with pre[h] <= f.
-                    int h = 0;
-#pragma unroll
-                    for (int step = 16; step > 0; step >>= 1)
-                        if (pre[h + step] <= f) h += step;
-                    const uint32_t other = __ldcs(w.nbr_list + (size_t)seg_of[h] * block + (f - pre[h]));
                     const Home home = make_home(hg[2 * h], hg[2 * h + 1], seg_of[h]);
-                    const float4 oa = w.geom[2 * (size_t)other], ob = w.geom[2 * (size_t)other + 1];
-                    float p2x, p2y, p2z, q2x, q2y, q2z;
-                    pass = contact_reach(home, oa, ob, g, p2x, p2y, p2z, q2x, q2y, q2z);
+                    pass = contact_reach(home, oa, ob, g, p2x, p2y, p2z, q2x, q2y, q2z) &&
+                           lines_may_touch(home, p2x, p2y, p2z, q2x, q2y, q2z, oa.w, line_eps);
+                    r2 = oa.w;
+                    other_id = other;
+                    owner = h;
                 }
                 const uint32_t ballot = __ballot_sync(FULL, pass);
-                if (pass) q[queued + __popc(ballot & ((1u << lane) - 1u))] = f;
+                if (pass) {
+                    const uint32_t at = queued + __popc(ballot & ((1u << lane) - 1u));
+                    qg[2 * at] = make_float4(p2x, p2y, p2z, r2);
+                    qg[2 * at + 1] = make_float4(q2x, q2y, q2z, __uint_as_float(other_id));
+                    qo[at] = (uint8_t)owner;
+                }
                 queued += __popc(ballot);
                 __syncwarp();
             }
@@ -764,17 +854,11 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
                 bool hit = false;
                 int h = 0;
                 if ((uint32_t)lane < n) {
-                    const uint32_t f = q[lane];
-#pragma unroll
-                    for (int step = 16; step > 0; step >>= 1)
-                        if (pre[h + step] <= f) h += step;
-                    const uint32_t other = w.nbr_list[(size_t)seg_of[h] * block + (f - pre[h])];
+                    const float4 ea = qg[2 * lane], eb = qg[2 * lane + 1];
+                    h = qo[lane];
                     const Home home = make_home(hg[2 * h], hg[2 * h + 1], seg_of[h]);
-                    const float4 oa = w.geom[2 * (size_t)other], ob = w.geom[2 * (size_t)other + 1];
-                    float p2x, p2y, p2z, q2x, q2y, q2z;
-                    contact_reach(home, oa, ob, g, p2x, p2y, p2z, q2x, q2y, q2z);
-                    hit = contact_solve(home, other, oa.w, p2x, p2y, p2z, q2x, q2y, q2z, sp.correction_fraction,
-                                        sp.contact_aggregation, pt);
+                    hit = contact_solve(home, __float_as_uint(eb.w), ea.w, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z,
+                                        sp.correction_fraction, sp.contact_aggregation, pt);
                 }
                 uint32_t bits = __ballot_sync(FULL, hit);
                 while (bits) {
@@ -790,9 +874,19 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
                     if (lane == owner) add_hit(acc, sp.contact_aggregation, pen, t0x, t0y, t0z, t1x, t1y, t1z, aggw);
                 }
                 const uint32_t rest = queued - n;
-                const uint32_t moved_entry = (uint32_t)lane < rest ? q[n + lane] : 0u;
+                float4 ma = make_float4(0.0f, 0.0f, 0.0f, 0.0f), mb = ma;
+                uint8_t mo = 0;
+                if ((uint32_t)lane < rest) {
+                    ma = qg[2 * (n + lane)];
+                    mb = qg[2 * (n + lane) + 1];
+                    mo = qo[n + lane];
+                }
                 __syncwarp();
-                if ((uint32_t)lane < rest) q[lane] = moved_entry;
+                if ((uint32_t)lane < rest) {
+                    qg[2 * lane] = ma;
+                    qg[2 * lane + 1] = mb;
+                    qo[lane] = mo;
+                }
                 __syncwarp();
                 queued = rest;
             }
@@ -1529,6 +1623,14 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     cudaDeviceGetAttribute(&lp.num_sms, cudaDevAttrMultiProcessorCount, device);
     if (lp.num_sms <= 0) lp.num_sms = 148;
     lp.contact_group = 32;
+    // Absolute margin of the line-distance bound: 4e-6 of the largest box
+    // edge, above the f32 rounding of coordinates that are unwrapped by up to
+    // a box length either side.
+    {
+        float edge = 0.0f;
+        for (int a = 0; a < 3; ++a) edge = std::max(edge, w.grid.length[a]);
+        lp.line_eps = 4.0e-6f * edge;
+    }
     lp.contact_blocks = grid_for((w.S + 31) / 32, CONTACT_WARPS, lp.num_sms * 3);
     // Update kernel: as many warps per block as fit 96 KB of staged fibers.
     size_t per_warp = (size_t)3 * w.max_fiber * sizeof(float4);
@@ -1611,7 +1713,7 @@ int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
 }
 
 int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, bool gate, cudaStream_t st) {
-    contact_kernel<<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, gate ? 1 : 0);
+    contact_kernel<<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, gate ? 1 : 0, lp.line_eps);
     return 1;
 }
 

@@ -64,6 +64,7 @@ struct LaunchPlan {
     int num_sms;
     int contact_group;      // lanes per segment in the contact pass (8, 16 or 32)
     int contact_blocks;
+    float line_eps;         // absolute margin of the contact pass's line-distance bound
     int fiber_warps;        // fibers per block of the update kernel
     int fiber_blocks;
     size_t fiber_smem;
