@@ -187,6 +187,43 @@ int tgl_set_kernel_timing(tgl_world *world, int enable);
 void *tgl_world_stream(const tgl_world *world);
 int tgl_last_kernel_times(tgl_world *world, tgl_kernel_times *times);
 
+/* Inputs of tgl_contact_pass_noalloc: device pointers the caller owns. */
+typedef struct {
+    const float *positions;          /* device, 3V interleaved xyz */
+    const uint32_t *segment_vertices;/* device, 2S */
+    const uint32_t *segment_fibers;  /* device, S */
+    const float *segment_radii;      /* device, S */
+    const float *vertex_arc_lengths; /* device, V: rest arc length from the fiber start */
+    uint32_t segment_count;          /* at most 262144 */
+    uint32_t cells[3];               /* cells per axis; product at most 262144 */
+    float cell_lower[3];
+    float cell_upper[3];
+    uint32_t cell_periodic[3];
+    float correction_fraction;
+    uint32_t contact_aggregation;
+    uint32_t reserved;
+} tgl_noalloc_inputs;
+
+/* One contact pass for callers that cannot allocate device memory: a host
+ * that manages a fixed device memory pool itself and hands this library
+ * only its own buffers, or a loop that must never wait on the allocator.
+ * It has no counterpart in the reference. Every candidate is found by the
+ * exact 27-cell scan of the reference's cell list (the result a world of
+ * neighbor_capacity 1 gives), from device arrays the caller owns, writing
+ * corrections [6S] and per-segment maximum penetration [S] to device
+ * buffers the caller owns. Its only working memory is a fixed 5 MiB array
+ * compiled into this library (so every GPU that loads it holds that array
+ * until the process exits); it calls no allocator. Limits: 262144 segments
+ * and 262144 cells; larger inputs are rejected with TGL_ERR_UNSUPPORTED.
+ * The kernels are queued on `stream` (a cudaStream_t, NULL = default) and
+ * the call returns without waiting. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture. All calls share the one
+ * array: two calls whose kernels overlap on the GPU (different streams, or
+ * different host threads) race and corrupt each other's results. */
+int tgl_contact_pass_noalloc(const tgl_noalloc_inputs *inputs, float *corrections, float *segment_max_penetration,
+                             void *stream);
+
 /* Thread-local message of the last failed call on this thread. */
 const char *tgl_last_error(void);
 

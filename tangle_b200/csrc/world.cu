@@ -70,6 +70,11 @@ void destroy_entry(GraphEntry &e) {
 
 }  // namespace
 
+namespace tgl {
+// Sets the calling thread's tgl_last_error() message (used by noalloc.cu).
+void set_last_error(const std::string &message) { g_error = message; }
+}  // namespace tgl
+
 struct tgl_world {
     int device = 0;
     cudaStream_t stream = nullptr;

@@ -33,7 +33,7 @@ EXPORTS = (
     "tgl_cell_size", "tgl_cell_count", "tgl_cell_dims", "tgl_neighbor_skin", "tgl_neighbor_block",
     "tgl_neighbor_list_rebuilds", "tgl_debug_rebuild", "tgl_debug_cell_list", "tgl_debug_neighbor_lists",
     "tgl_debug_corrections", "tgl_kernel_launches", "tgl_set_kernel_timing", "tgl_last_kernel_times",
-    "tgl_world_stream", "tgl_last_error",
+    "tgl_world_stream", "tgl_contact_pass_noalloc", "tgl_last_error",
 )
 
 
