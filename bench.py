@@ -60,7 +60,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tta", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-iterations", type=int, default=4)
+    ap.add_argument("--cpu-iterations", type=int, default=40)
+    ap.add_argument("--reference-iterations", type=int, default=4,
+                    help="relaxation iterations per step of the reference arm (CPU)")
     ap.add_argument("--save-positions", default=None, help="write the positions after the timed steps (.npy)")
     ap.add_argument("--load-positions", default=None, help="start from saved positions (.npy)")
     return ap.parse_args()
@@ -207,7 +209,7 @@ def run_reference(args):
     orc.set_threads(cores)
     world = orc.OracleWorld(packed, config.cell_list, config.max_step)
     fixed = type(config)(**{**config.__dict__, "force_full_iterations": True})
-    per_step = 1
+    per_step = args.reference_iterations
     for _ in range(max(args.warmup, 1)):
         world.run_batch(fixed, per_step)
     t0 = time.perf_counter()
@@ -225,7 +227,8 @@ def run_reference(args):
         "config": {"workload": name, "nodes": nodes, "segments": packed.segment_count,
                    "iterations_per_step": per_step, "neighbor_capacity": config.cell_list.neighbor_capacity},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} steps of {per_step} iteration of the same specimen"},
+                         "sample": f"{args.steps} steps of {per_step} iterations of the same specimen, "
+                                   f"OpenMP over {cores} threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -267,6 +270,11 @@ def run_cuda(args):
 
     for _ in range(args.warmup):
         world.run_batch(fixed, args.iterations)
+    # The state the timed steps start from; the end-to-end leg replays the
+    # same trajectory from it.
+    host = torch.empty(3 * nodes, dtype=torch.float32, pin_memory=True)
+    host_np = host.numpy()
+    world.download_positions(host_np)
     bytes_start = contact_bytes(world)
     launches0 = world.kernel_launches
     contact_ms = 0.0
@@ -323,16 +331,12 @@ def run_cuda(args):
                 "kernel": "contact_kernel (find_segment_corrections)",
                 "algorithmic_bytes_per_launch": algorithmic, "avg_launch_ms": avg_contact_s * 1000.0}
 
-    # End to end through the public API with pinned host buffers.
+    # End to end through the public API with pinned host buffers: the timed
+    # steps again, from the same start state, each step uploading the
+    # positions, running the batch and downloading the result (which the next
+    # step uploads). The batch's graph already exists, so no warm-up is needed.
     e2e = None
     if not args.no_e2e:
-        host = torch.empty(3 * nodes, dtype=torch.float32, pin_memory=True)
-        host_np = host.numpy()
-        world.download_positions(host_np)
-        for _ in range(max(1, args.warmup // 2)):
-            world.upload_positions(host_np)
-            world.run_batch(fixed, args.iterations)
-            world.download_positions(host_np)
         barrier()
         t0 = time.perf_counter()
         done = 0
