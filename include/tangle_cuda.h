@@ -118,6 +118,21 @@ int tgl_world_create(const tgl_packed *packed, const tgl_cell_list_config *cell_
 /* Drop of the world (frees every device buffer and captured graph). */
 void tgl_world_destroy(tgl_world *world);
 
+/* DeviceFiberWorld::checkpoint (world.rs:758-823; plugin.rs:393-404) for the
+ * plain path: the persistent state a restart needs, which is the current
+ * positions (interleaved xyz, len = 3 * vertex_count) and the lifetime
+ * iteration count. Scratch (cell and neighbor lists, corrections, gate
+ * metrics) is rebuilt by the first batch after a restore, as in the
+ * reference. */
+int tgl_world_checkpoint(tgl_world *world, float *xyz, size_t len, uint64_t *total_iterations);
+
+/* DeviceFiberWorld::restore (world.rs:693-756; plugin.rs:358-391): uploads
+ * `packed` (whose positions are the checkpoint's) as tgl_world_create does,
+ * and continues the lifetime iteration count from `total_iterations`, which
+ * must fit in 32 bits as the reference's control word requires. */
+int tgl_world_restore(const tgl_packed *packed, const tgl_cell_list_config *cell_list, float max_step,
+                      uint64_t total_iterations, tgl_world **out);
+
 /* DeviceFiberWorld::run_batch + read_status (world.rs:1020-1505,
  * :2337-2369; DeviceWorld::run_batch, plugin.rs:407-418): up to `iterations`
  * corrections plus one measure-only pass, stopping on the device as soon as
@@ -146,6 +161,21 @@ uint32_t tgl_neighbor_block(const tgl_world *world);
 /* DeviceFiberWorld::neighbor_list_rebuilds (world/neighbor_list.rs:167-176). */
 int tgl_neighbor_list_rebuilds(tgl_world *world, uint32_t *rebuilds);
 
+/* Contact lists (no reference counterpart: an internal second level under
+ * the Verlet lists that changes no result). Each cell-list slot keeps the
+ * entries of its segment's Verlet list that lie within `contact_skin` of
+ * touching at a snapshot of the positions, in the Verlet list's order; the
+ * contact pass reads them instead of the Verlet list until some vertex moves
+ * more than contact_skin / 2 from the snapshot or the Verlet lists are
+ * rebuilt. The skin is 0.1 of the neighbor skin unless the environment
+ * variable TGL_CONTACT_SKIN, read when a world is created, gives another
+ * fraction in (0, 1] (0 turns them off); they are also off when a periodic
+ * box edge is under about four segment lengths plus four radii, and every
+ * pass reads the Verlet lists while some segment is stretched that far.
+ * Reports the skin (0 when off), the entries per slot, and the refreshes
+ * done so far. */
+int tgl_contact_list_info(tgl_world *world, float *contact_skin, uint32_t *block, uint32_t *refreshes);
+
 /* Parity taps (no reference counterpart beyond its tests' readbacks,
  * world_tests.rs:1342-1363). Forces a neighbor-list rebuild from the current
  * positions now. */
@@ -157,6 +187,10 @@ int tgl_debug_cell_list(tgl_world *world, uint32_t *cell_counts, uint32_t *cell_
 /* True neighbor counts [S] and lists [S * block], segment-major; lists of
  * segments whose count exceeds the block are not meaningful. */
 int tgl_debug_neighbor_lists(tgl_world *world, uint32_t *counts, uint32_t *lists);
+/* Contact lists by cell-list slot: counts [S] (a count above the block means
+ * the slot's contact pass reads the Verlet list) and lists [S * block].
+ * TGL_ERR_UNSUPPORTED when contact lists are off. */
+int tgl_debug_contact_lists(tgl_world *world, uint32_t *counts, uint32_t *lists);
 /* One contact pass (find_segment_corrections, contact.rs:232-902) on the
  * current positions and lists, moving nothing: corrections [6S] and
  * per-segment maximum penetration [S]. */

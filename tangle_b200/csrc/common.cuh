@@ -224,7 +224,8 @@ struct Control {
     // Blocks of the contact kernel finished this pass (last-block gate).
     uint32_t done_blocks;
     uint32_t cell_overflow;
-    uint32_t pad[2];
+    // Contact lists: refresh pending, refreshes done.
+    uint32_t contact_state[2];
 };
 
 }  // namespace tgl

@@ -52,6 +52,45 @@ __device__ inline bool contact_reach(const Home &h, float4 oa, float4 ob, const 
     return mdx * mdx + mdy * mdy + mdz * mdz <= reach * reach;
 }
 
+// contact_reach and, in `wide`, the same test with `extra` added to the
+// reach (the sum is formed as contact_reach forms it, then `extra` added, so
+// a pair that passes the exact test always passes the wide one).
+__device__ inline bool contact_reach_wide(const Home &h, float4 oa, float4 ob, const Grid &g, float extra,
+                                          float &p2x, float &p2y, float &p2z, float &q2x, float &q2y, float &q2z,
+                                          bool &exact) {
+    p2x = oa.x, p2y = oa.y, p2z = oa.z, q2x = ob.x, q2y = ob.y, q2z = ob.z;
+    bool moved = minimum_image(h.p1x, h.p1y, h.p1z, h.q1x, h.q1y, h.q1z, p2x, p2y, p2z, q2x, q2y, q2z, g);
+    float d2x = q2x - p2x, d2y = q2y - p2y, d2z = q2z - p2z;
+    float mdx = 0.5f * (p2x + q2x - h.p1x - h.q1x);
+    float mdy = 0.5f * (p2y + q2y - h.p1y - h.q1y);
+    float mdz = 0.5f * (p2z + q2z - h.p1z - h.q1z);
+    float other_half = moved ? 0.5f * sqrtf(d2x * d2x + d2y * d2y + d2z * d2z) : ob.w;
+    float base = h.half_length + other_half + h.radius + oa.w;
+    float reach = base * (1.0f + 1.0e-4f);
+    float wide = (base + extra) * (1.0f + 1.0e-4f);
+    float m2 = mdx * mdx + mdy * mdy + mdz * mdz;
+    exact = m2 <= reach * reach;
+    return m2 <= wide * wide;
+}
+
+// Whether two segments (the second already at its minimum image) may come
+// within `extra` of touching: their f32 closest-point distance against
+// r1 + r2 + extra with margins for its rounding. The closest-point solve
+// returns a distance between two points of the segments, so it can only
+// overestimate the true distance, by rounding, or, for axes within 1e-3 rad
+// of parallel (where it takes an end point without solving), by at most
+// 1e-3 of a segment length; the margins (1 % relative, 2e-3 of the summed
+// half lengths, and `eps`) cover both.
+__device__ inline bool within_contact_skin(const Home &h, float p2x, float p2y, float p2z, float q2x, float q2y,
+                                           float q2z, float other_radius, float extra, float eps) {
+    const float d2x = q2x - p2x, d2y = q2y - p2y, d2z = q2z - p2z;
+    const float distance = axis_distance(h.p1x, h.p1y, h.p1z, h.d1x, h.d1y, h.d1z, p2x, p2y, p2z, d2x, d2y, d2z);
+    const float other_half = 0.5f * sqrtf(d2x * d2x + d2y * d2y + d2z * d2z);
+    const float threshold =
+        (h.radius + other_radius + extra) * 1.01f + 2.0e-3f * (h.half_length + other_half) + eps;
+    return distance <= threshold;
+}
+
 // A lower bound test on the capsules' overlap: the segments lie on their
 // axis lines, so their distance is at least the lines' distance
 // |(p2 - p1) . (d1 x d2)| / |d1 x d2|. When that exceeds r1 + r2 by a margin

@@ -43,17 +43,30 @@ __global__ void begin_batch_kernel(Control *ctl) {
     ctl->done_blocks = 0;
 }
 
-// neighbor.rs:446-465, over every vertex (all are active in the plain path).
+// Whether vertex v at (x, y, z) has moved more than half the contact skin
+// (less 0.1 %, a margin for rounding) from the contact lists' snapshot.
+__device__ inline bool contact_moved(const WorldDev &w, uint32_t v, float x, float y, float z) {
+    const float limit = 0.4995f * w.contact_skin;
+    const float4 c = w.contact_ref[v];
+    const float dx = x - c.x, dy = y - c.y, dz = z - c.z;
+    return dx * dx + dy * dy + dz * dz > limit * limit;
+}
+
+// neighbor.rs:446-465, over every vertex (all are active in the plain path),
+// and the same check against the contact lists' snapshot.
 __global__ void flag_displacement_kernel(WorldDev w) {
     uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    bool far = false;
+    bool far = false, contact_far = false;
     if (v < w.V) {
         float md = 0.5f * w.skin;
         float4 p = w.pos[v], r = w.ref_pos[v];
         float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
         far = dx * dx + dy * dy + dz * dz > md * md;
+        if (w.contact_skin > 0.0f) contact_far = contact_moved(w, v, p.x, p.y, p.z);
     }
+    if (w.contact_skin > 0.0f && v < w.S && w.geom[2 * (size_t)v + 1].w > w.contact_half_limit) contact_far = true;
     if (__any_sync(FULL, far) && (threadIdx.x & 31) == 0) w.ctl->neighbor_state[0] = 1;
+    if (__any_sync(FULL, contact_far) && (threadIdx.x & 31) == 0) w.ctl->contact_state[0] = 1;
 }
 
 // neighbor.rs:436-441.
@@ -410,10 +423,12 @@ __global__ void rb_snapshot_kernel(WorldDev w) {
 }
 
 // finish_neighbor_list_rebuild (neighbor.rs:424-432).
+// New Verlet lists (and slots) also call for new contact lists.
 __global__ void rb_finish_kernel(Control *ctl) {
     if (ctl->neighbor_state[0] == 0) return;
     ctl->neighbor_state[0] = 0;
     ctl->neighbor_state[1] += 1;
+    ctl->contact_state[0] = 1;
 }
 
 // ---------------------------------------------------------------- contact pass
@@ -510,6 +525,12 @@ __device__ inline float4 load_keep(const float4 *p, uint64_t policy) {
 
 constexpr int CONTACT_WARPS = 8;
 
+// Contact pass modes: the Verlet lists as they are (CONTACT_FULL); the
+// Verlet lists plus a refresh of the contact lists and their snapshot
+// (CONTACT_REFRESH, run when the refresh flag is set); the contact lists
+// (CONTACT_LISTED, run when it is clear).
+enum { CONTACT_FULL = 0, CONTACT_REFRESH = 1, CONTACT_LISTED = 2 };
+
 // find_segment_corrections (contact.rs:232-902) over warp-owned batches of 32
 // segments taken in cell-list order: lane i owns the i-th segment's sums. The batch's listed
 // candidates are walked as one flat sequence, 32 at a time, through the
@@ -518,26 +539,53 @@ constexpr int CONTACT_WARPS = 8;
 // its segment's sums in list order, as the reference's serial loop adds it.
 // Overflowed segments then take the exact cell scan. With `gate`, the last
 // block to finish runs assess_reduced_metrics (kernels.rs:129-162).
+//
+// Contact lists. A candidate can only produce a hit while its segments'
+// distance is below r1 + r2, and while no vertex has moved more than
+// contact_skin / 2 from a snapshot, no segment distance has shrunk by more
+// than contact_skin since it. So the Verlet-list entries whose distance at
+// the snapshot is within contact_skin of touching (within_contact_skin, a
+// conservative test) hold every hit of every pass until a vertex moves
+// farther; the update kernel flags that, as it flags Verlet rebuilds, and a
+// Verlet rebuild forces a refresh. Hits are summed in ascending segment
+// order from a sub-sequence of the same sorted list, so the sums are bit for
+// bit those of the full list. (The minimum image cannot change within the
+// window while every half length stays below contact_half_limit, which the
+// update kernel checks with the displacements.)
+template <int MODE>
 __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams sp, int gate, float line_eps) {
     __shared__ float4 home_geom[CONTACT_WARPS][64];
     __shared__ uint32_t prefix[CONTACT_WARPS][33];
     __shared__ float4 queue_geom[CONTACT_WARPS][128];  // 64 entries: {p2, r2}, {q2, other}
-    __shared__ uint8_t queue_owner[CONTACT_WARPS][64];
+    __shared__ uint8_t queue_owner[CONTACT_WARPS][64]; // owner lane; bit 7: passed the exact tests (refresh)
     __shared__ uint32_t segments[CONTACT_WARPS][32];
+    __shared__ const uint32_t *sources[CONTACT_WARPS][32];
+    __shared__ uint32_t kept_count[CONTACT_WARPS][32];
     __shared__ uint32_t warp_max[CONTACT_WARPS];
     __shared__ int is_last;
     if (gate && w.ctl->control[0] == 0) return;
+    if (MODE == CONTACT_REFRESH && w.ctl->contact_state[0] == 0) return;
+    if (MODE == CONTACT_LISTED && w.ctl->contact_state[0] != 0) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const Grid &g = w.grid;
     const uint32_t block = w.block;
+    const uint32_t cblock = w.contact_block;
+    const float cskin = w.contact_skin;
     float4 *hg = home_geom[warp];
     uint32_t *pre = prefix[warp];
     float4 *qg = queue_geom[warp];
     uint8_t *qo = queue_owner[warp];
     uint32_t *seg_of = segments[warp];
+    const uint32_t **src = sources[warp];
+    uint32_t *kept = kept_count[warp];
     uint32_t thread_max = 0;
     const uint32_t warps_total = gridDim.x * CONTACT_WARPS;
     const uint64_t geom_policy = make_keep_policy();
+    if (MODE == CONTACT_REFRESH) {
+        // The snapshot the next passes measure displacement against.
+        for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x)
+            w.contact_ref[v] = w.pos[v];
+    }
     for (uint32_t base = (blockIdx.x * CONTACT_WARPS + warp) * 32u; base < w.S; base += warps_total * 32u) {
         // Batches follow the cell list's slot order, so the 32 segments of a
         // batch are spatial neighbors and share most of their candidates.
@@ -546,6 +594,14 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         uint32_t count = valid ? w.nbr_count[segment] : 0u;
         const bool listed = valid && count <= block;
         uint32_t k = listed ? count : 0u;
+        const uint32_t *source = w.nbr_list + (size_t)segment * block;
+        if (MODE == CONTACT_LISTED && listed) {
+            const uint32_t listed_count = w.contact_count[base + lane];
+            if (listed_count <= cblock) {
+                k = listed_count;
+                source = w.contact_list + (size_t)(base + lane) * cblock;
+            }
+        }
         uint32_t incl = k;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -559,6 +615,8 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
             hg[2 * lane + 1] = w.geom[2 * (size_t)segment + 1];
         }
         seg_of[lane] = segment;
+        src[lane] = source;
+        kept[lane] = 0;
         __syncwarp();
         const uint32_t total = pre[32];
         ContactAcc acc = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
@@ -571,11 +629,11 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         float4 oa_next = make_float4(0.0f, 0.0f, 0.0f, 0.0f), ob_next = oa_next;
         if (lane < (int)total) {
             h_next = owner_of(pre, lane);
-            other_next = load_stream(w.nbr_list + (size_t)seg_of[h_next] * block + (lane - pre[h_next]));
+            other_next = load_stream(src[h_next] + (lane - pre[h_next]));
         }
         if (32u + lane < total) {
             h_next2 = owner_of(pre, 32u + lane);
-            other_next2 = load_stream(w.nbr_list + (size_t)seg_of[h_next2] * block + (32u + lane - pre[h_next2]));
+            other_next2 = load_stream(src[h_next2] + (32u + lane - pre[h_next2]));
         }
         if (lane < (int)total) {
             oa_next = load_keep(w.geom + 2 * (size_t)other_next, geom_policy);
@@ -596,16 +654,24 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
                 }
                 if (f + 64 < total) {
                     h_next2 = owner_of(pre, f + 64);
-                    other_next2 = load_stream(w.nbr_list + (size_t)seg_of[h_next2] * block + (f + 64 - pre[h_next2]));
+                    other_next2 = load_stream(src[h_next2] + (f + 64 - pre[h_next2]));
                 }
-                bool pass = false;
+                bool pass = false, exact = false;
                 float p2x = 0.0f, p2y = 0.0f, p2z = 0.0f, q2x = 0.0f, q2y = 0.0f, q2z = 0.0f, r2 = 0.0f;
                 uint32_t other_id = 0;
                 int owner = 0;
                 if (f < total) {
                     const Home home = make_home(hg[2 * h], hg[2 * h + 1], seg_of[h]);
-                    pass = contact_reach(home, oa, ob, g, p2x, p2y, p2z, q2x, q2y, q2z) &&
-                           lines_may_touch(home, p2x, p2y, p2z, q2x, q2y, q2z, oa.w, line_eps);
+                    if (MODE == CONTACT_REFRESH) {
+                        // Queue what may come within the contact skin; mark
+                        // what passes the pass's own exact tests.
+                        pass = contact_reach_wide(home, oa, ob, g, cskin, p2x, p2y, p2z, q2x, q2y, q2z, exact) &&
+                               lines_may_touch(home, p2x, p2y, p2z, q2x, q2y, q2z, oa.w + cskin, line_eps);
+                        exact = exact && pass && lines_may_touch(home, p2x, p2y, p2z, q2x, q2y, q2z, oa.w, line_eps);
+                    } else {
+                        pass = contact_reach(home, oa, ob, g, p2x, p2y, p2z, q2x, q2y, q2z) &&
+                               lines_may_touch(home, p2x, p2y, p2z, q2x, q2y, q2z, oa.w, line_eps);
+                    }
                     r2 = oa.w;
                     other_id = other;
                     owner = h;
@@ -615,7 +681,7 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
                     const uint32_t at = queued + __popc(ballot & ((1u << lane) - 1u));
                     qg[2 * at] = make_float4(p2x, p2y, p2z, r2);
                     qg[2 * at + 1] = make_float4(q2x, q2y, q2z, __uint_as_float(other_id));
-                    qo[at] = (uint8_t)owner;
+                    qo[at] = (uint8_t)(owner | (exact ? 0x80 : 0));
                 }
                 queued += __popc(ballot);
                 __syncwarp();
@@ -623,14 +689,31 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
             if (queued >= 32 || (f0 + 32 >= total && queued)) {
                 const uint32_t n = min(queued, 32u);
                 PairTerms pt;
-                bool hit = false;
+                bool hit = false, keep = false;
                 int h = 0;
                 if ((uint32_t)lane < n) {
                     const float4 ea = qg[2 * lane], eb = qg[2 * lane + 1];
-                    h = qo[lane];
+                    h = qo[lane] & 31;
                     const Home home = make_home(hg[2 * h], hg[2 * h + 1], seg_of[h]);
-                    hit = contact_solve(home, __float_as_uint(eb.w), ea.w, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z,
-                                        sp.correction_fraction, sp.contact_aggregation, pt);
+                    if (MODE != CONTACT_REFRESH || (qo[lane] & 0x80))
+                        hit = contact_solve(home, __float_as_uint(eb.w), ea.w, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z,
+                                            sp.correction_fraction, sp.contact_aggregation, pt);
+                    if (MODE == CONTACT_REFRESH)
+                        keep = within_contact_skin(home, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z, ea.w, cskin, line_eps);
+                }
+                if (MODE == CONTACT_REFRESH) {
+                    // Append the kept entries to their owners' contact lists
+                    // in queue (= list) order.
+                    const uint32_t peers = __match_any_sync(FULL, keep ? (uint32_t)h : 32u + (uint32_t)lane);
+                    uint32_t at = 0;
+                    if (keep) {
+                        at = kept[h] + __popc(peers & ((1u << lane) - 1u));
+                        if (at < cblock)
+                            w.contact_list[(size_t)(base + h) * cblock + at] = __float_as_uint(qg[2 * lane + 1].w);
+                    }
+                    __syncwarp();
+                    if (keep && lane == 31 - __clz(peers)) kept[h] += __popc(peers);
+                    __syncwarp();
                 }
                 uint32_t bits = __ballot_sync(FULL, hit);
                 while (bits) {
@@ -667,6 +750,7 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
             finish_segment(w, segment, acc, sp.contact_aggregation);
             thread_max = max(thread_max, __float_as_uint(fmaxf(acc.maxpen, 0.0f)));
         }
+        if (MODE == CONTACT_REFRESH && valid) w.contact_count[base + lane] = listed ? kept[lane] : 0u;
         uint32_t spill = __ballot_sync(FULL, valid && !listed);
         while (spill) {
             const int j = __ffs(spill) - 1;
@@ -715,6 +799,10 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         c->acc[1] = 0;
         c->acc[2] = 0;
         c->done_blocks = 0;
+        if (MODE == CONTACT_REFRESH) {
+            c->contact_state[0] = 0;
+            c->contact_state[1] += 1;
+        }
         __threadfence();
     }
 }
@@ -815,6 +903,8 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
     const float md = 0.5f * w.skin;
     uint32_t smax = 0, cmax = 0;
     bool far = false;
+    bool contact_far = false;
+    const bool contact_lists = w.contact_skin > 0.0f;
     for (uint32_t f = blockIdx.x * warps + warp; f < w.F; f += gridDim.x * warps) {
         const uint2 span = w.fiber_vspan[f];
         const uint32_t v0 = span.x;
@@ -984,6 +1074,7 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
             float4 r = w.ref_pos[v0 + i];
             float dx = x.x - r.x, dy = x.y - r.y, dz = x.z - r.z;
             if (dx * dx + dy * dy + dz * dz > md * md) far = true;
+            if (contact_lists && contact_moved(w, v0 + i, x.x, x.y, x.z)) contact_far = true;
             if (i > 0 && i + 1 < n) {
                 float maximum = St[i].x;
                 if (maximum > 0.0f) {
@@ -994,8 +1085,10 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
             if (i + 1 < n) {
                 float4 y = P[i + 1];
                 float dx = y.x - x.x, dy = y.y - x.y, dz = y.z - x.z;
+                const float half = 0.5f * sqrtf(dx * dx + dy * dy + dz * dz);
                 w.geom[2 * (size_t)(s0 + i)] = make_float4(x.x, x.y, x.z, radius);
-                w.geom[2 * (size_t)(s0 + i) + 1] = make_float4(y.x, y.y, y.z, 0.5f * sqrtf(dx * dx + dy * dy + dz * dz));
+                w.geom[2 * (size_t)(s0 + i) + 1] = make_float4(y.x, y.y, y.z, half);
+                if (contact_lists && half > w.contact_half_limit) contact_far = true;
             }
         }
         __syncwarp();
@@ -1003,10 +1096,12 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
     smax = warp_max_u32(smax);
     cmax = warp_max_u32(cmax);
     bool any_far = __any_sync(FULL, far);
+    bool any_contact_far = __any_sync(FULL, contact_far);
     if (lane == 0) {
         if (smax) atomicMax(&w.ctl->acc[1], smax);
         if (cmax) atomicMax(&w.ctl->acc[2], cmax);
         if (any_far) w.ctl->neighbor_state[0] = 1;
+        if (any_contact_far) w.ctl->contact_state[0] = 1;
     }
 }
 
@@ -1119,6 +1214,8 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
     const float md = 0.5f * w.skin;
     uint32_t smax = 0, cmax = 0;
     bool far = false;
+    bool contact_far = false;
+    const bool contact_lists = w.contact_skin > 0.0f;
     for (uint32_t batch = blockIdx.x; batch * FPW < w.F; batch += gridDim.x) {
         const uint32_t slot = batch * FPW + group;
         const uint32_t mine = slot < w.F ? w.fiber_order[slot] : TGL_NONE;
@@ -1312,6 +1409,7 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                 const float4 r = w.ref_pos[v0 + i];
                 const float dx = x.x - r.x, dy = x.y - r.y, dz = x.z - r.z;
                 if (dx * dx + dy * dy + dz * dz > md * md) far = true;
+                if (contact_lists && contact_moved(w, v0 + i, x.x, x.y, x.z)) contact_far = true;
                 if (i > 0 && i + 1 < n) {
                     const float maximum = lanes_limit(x);
                     if (maximum > 0.0f) {
@@ -1322,9 +1420,10 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                 if (i + 1 < n) {
                     const float4 y = P[i + 1];
                     const float ex = y.x - x.x, ey = y.y - x.y, ez = y.z - x.z;
+                    const float half = 0.5f * sqrtf(ex * ex + ey * ey + ez * ez);
                     w.geom[2 * (size_t)(s0 + i)] = make_float4(x.x, x.y, x.z, radius);
-                    w.geom[2 * (size_t)(s0 + i) + 1] =
-                        make_float4(y.x, y.y, y.z, 0.5f * sqrtf(ex * ex + ey * ey + ez * ez));
+                    w.geom[2 * (size_t)(s0 + i) + 1] = make_float4(y.x, y.y, y.z, half);
+                    if (contact_lists && half > w.contact_half_limit) contact_far = true;
                 }
             }
         }
@@ -1333,10 +1432,12 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
     smax = warp_max_u32(smax);
     cmax = warp_max_u32(cmax);
     const bool any_far = __any_sync(FULL, far);
+    const bool any_contact_far = __any_sync(FULL, contact_far);
     if (lane == 0) {
         if (smax) atomicMax(&w.ctl->acc[1], smax);
         if (cmax) atomicMax(&w.ctl->acc[2], cmax);
         if (any_far) w.ctl->neighbor_state[0] = 1;
+        if (any_contact_far) w.ctl->contact_state[0] = 1;
     }
 }
 
@@ -1422,6 +1523,7 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     lp.lanes_smem = (size_t)fpw * lp.lanes_stride * sizeof(float4);
     lp.fiber_lanes = w.max_fiber <= 32u * LANES_KMAX && lp.lanes_smem <= 200 * 1024;
     lp.lanes_blocks = (int)((w.F + fpw - 1) / fpw);
+    lp.contact_lists = w.contact_skin > 0.0f;
     lp.build_ch = 3072;
     lp.build_smem = (size_t)lp.build_ch * (sizeof(float4) + sizeof(uint32_t));
     // The sphere pre-test needs >= 3 cells on every periodic axis (see
@@ -1485,7 +1587,13 @@ int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
 }
 
 int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, bool gate, cudaStream_t st) {
-    contact_kernel<<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, gate ? 1 : 0, lp.line_eps);
+    if (gate && lp.contact_lists) {
+        // Listed first: the refresh pass clears the flag the listed pass reads.
+        contact_kernel<CONTACT_LISTED><<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, 1, lp.line_eps);
+        contact_kernel<CONTACT_REFRESH><<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, 1, lp.line_eps);
+        return 2;
+    }
+    contact_kernel<CONTACT_FULL><<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, gate ? 1 : 0, lp.line_eps);
     return 1;
 }
 

@@ -12,6 +12,14 @@ struct WorldDev {
     uint32_t block;      // neighbor slots per segment list
     uint32_t max_fiber;  // most vertices in one fiber
     float skin;          // neighbor skin
+    // Contact lists: per cell-list slot, the Verlet-list entries that lie
+    // within contact_skin of touching at the contact_ref snapshot (0 = off).
+    float contact_skin;
+    uint32_t contact_block;  // entries per slot
+    // Longest half length for which a pair within reach + contact_skin has
+    // one minimum image (L/2 > 2 H + 2 r_max + contact_skin on every periodic
+    // axis); a longer segment makes every pass refresh (read the Verlet list).
+    float contact_half_limit;
     Grid grid;
     // Static, uploaded once.
     const float4 *seg_static;   // [S] radius, arc(first vertex), arc(second vertex), fiber bits
@@ -39,6 +47,10 @@ struct WorldDev {
     // Verlet lists.
     uint32_t *nbr_count; // [S] true neighbor count
     uint32_t *nbr_list;  // [S * block]
+    // Contact lists (allocated only when contact_skin > 0).
+    uint32_t *contact_count; // [S] per slot; above contact_block = use the Verlet list
+    uint32_t *contact_list;  // [S * contact_block] per slot, ascending segment order
+    float4 *contact_ref;     // [V] positions the contact lists were filtered at
     Control *ctl;
     float *xyz_stage;    // [3V] interleaved staging for host copies
 };
@@ -73,6 +85,7 @@ struct LaunchPlan {
     int lanes_stride;
     size_t lanes_smem;
     int lanes_blocks;
+    bool contact_lists;     // contact lists on (contact_skin > 0)
     int build_ch;           // candidate slots staged per build chunk
     size_t build_smem;
     int build_prefilter;    // sphere pre-test on (needs >= 3 cells per periodic axis)
@@ -87,6 +100,9 @@ int launch_flag_displacement(const WorldDev &w, cudaStream_t st);
 int launch_measure_start(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 int launch_request_rebuild(const WorldDev &w, cudaStream_t st);
+// With the gate and contact lists on, enqueues the listed pass and the
+// refresh pass, each of which returns at once unless the device-side refresh
+// flag picks it; otherwise the full-list pass.
 int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, bool gate, cudaStream_t st);
 int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st);
 int launch_positions_from_stage(const WorldDev &w, cudaStream_t st);

@@ -7,6 +7,8 @@
 
 #include <cmath>
 #include <algorithm>
+#include <cstddef>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -21,6 +23,7 @@ namespace {
 
 thread_local std::string g_error;
 constexpr uint64_t REFERENCE_MAX_LIST_BYTES = 120ull << 20;  // world.rs:36
+constexpr uint32_t CONTACT_BLOCK = 32;  // contact-list entries per slot
 
 int set_error(int code, const std::string &message) {
     g_error = message;
@@ -387,6 +390,24 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
     d.max_fiber = max_fiber;
     d.skin = skin;
     d.grid = grid;
+    // Contact lists: on by default at a tenth of the skin (TGL_CONTACT_SKIN
+    // sets the fraction, 0 turns them off). A pair's minimum image must stay
+    // fixed while its vertices move less than the contact skin: with every
+    // half length below H, pairs within reach + contact skin are closer than
+    // half a box length on every periodic axis, so
+    // H = (L/2 - 2 r_max - contact_skin) / 2, less 0.1 %.
+    float contact_fraction = 0.1f;
+    if (const char *env = std::getenv("TGL_CONTACT_SKIN")) contact_fraction = std::strtof(env, nullptr);
+    if (!(contact_fraction > 0.0f && contact_fraction <= 1.0f) || !(skin > 0.0f)) contact_fraction = 0.0f;
+    d.contact_skin = contact_fraction * skin;
+    d.contact_half_limit = INFINITY;
+    for (int a = 0; a < 3; ++a)
+        if (grid.periodic[a])
+            d.contact_half_limit = std::fmin(
+                d.contact_half_limit, 0.999f * 0.5f * (0.5f * grid.length[a] - 2.0f * maximum_radius - d.contact_skin));
+    float longest_half = 0.5f * maximum_length;
+    if (!(d.contact_half_limit > longest_half)) d.contact_skin = 0.0f;  // no room: full lists every pass
+    d.contact_block = d.contact_skin > 0.0f ? CONTACT_BLOCK : 0u;
     int rc = 0;
     float4 *seg_static_d, *vtx_static_d;
     uint32_t *seg_v0_d, *fiber_s0_d, *pinned_d, *fiber_order_d;
@@ -405,6 +426,10 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
         (rc = w->alloc(&d.nbr_list, std::max<uint64_t>((uint64_t)S * block, 1))) || (rc = w->alloc(&d.ctl, 1)) ||
         (rc = w->alloc(&d.xyz_stage, 3 * (size_t)V)))
         return fail(rc);
+    if (d.contact_block &&
+        ((rc = w->alloc(&d.contact_count, S)) || (rc = w->alloc(&d.contact_list, (size_t)S * d.contact_block)) ||
+         (rc = w->upload(&d.contact_ref, pos))))
+        return fail(rc);
     d.seg_static = seg_static_d;
     d.seg_v0 = seg_v0_d;
     d.fiber_vspan = fiber_vspan_d;
@@ -418,6 +443,7 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
     ctl.metrics[1] = 0.0f;
     ctl.metrics[2] = INFINITY;
     ctl.neighbor_state[0] = 1;  // lists start stale (world.rs:516-517)
+    ctl.contact_state[0] = 1;
     if (cudaMemcpy(d.ctl, &ctl, sizeof(Control), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(d.corr, 0, 2 * (size_t)S * sizeof(float4)) != cudaSuccess ||
         cudaMemset(d.vertex_step, 0, V * sizeof(float)) != cudaSuccess ||
@@ -437,6 +463,34 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
 }
 
 void tgl_world_destroy(tgl_world *w) { delete w; }
+
+int tgl_world_checkpoint(tgl_world *w, float *xyz, size_t len, uint64_t *total_iterations) {
+    if (!w || !xyz || !total_iterations) return set_error(TGL_ERR_INVALID, "null argument");
+    if (int rc = tgl_download_positions(w, xyz, len)) return rc;
+    TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    *total_iterations = w->host_ctl->control[1];
+    return 0;
+}
+
+int tgl_world_restore(const tgl_packed *pk, const tgl_cell_list_config *cl, float max_step,
+                      uint64_t total_iterations, tgl_world **out) {
+    if (!out) return set_error(TGL_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (total_iterations > 0xFFFFFFFFull)  // world.rs:707
+        return set_error(TGL_ERR_INVALID, "checkpoint iteration count exceeds u32");
+    tgl_world *w = nullptr;
+    if (int rc = tgl_world_create(pk, cl, max_step, &w)) return rc;
+    const uint32_t lifetime = (uint32_t)total_iterations;
+    cudaError_t e = cudaMemcpy(reinterpret_cast<char *>(w->dev.ctl) + offsetof(Control, control) + sizeof(uint32_t),
+                               &lifetime, sizeof(uint32_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        tgl_world_destroy(w);
+        return set_error(TGL_ERR_CUDA, std::string("restore failed: ") + cudaGetErrorString(e));
+    }
+    *out = w;
+    return 0;
+}
 
 int tgl_run_batch(tgl_world *w, const tgl_relax_config *config, uint32_t iterations, tgl_batch_status *status) {
     if (!w || !config || !status) return set_error(TGL_ERR_INVALID, "null argument");
@@ -552,6 +606,26 @@ int tgl_neighbor_list_rebuilds(tgl_world *w, uint32_t *rebuilds) {
     TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
     TGL_CUDA(cudaStreamSynchronize(w->stream));
     *rebuilds = w->host_ctl->neighbor_state[1];
+    return 0;
+}
+
+int tgl_contact_list_info(tgl_world *w, float *contact_skin, uint32_t *block, uint32_t *refreshes) {
+    if (!w || !contact_skin || !block || !refreshes) return set_error(TGL_ERR_INVALID, "null argument");
+    TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    *contact_skin = w->dev.contact_skin;
+    *block = w->dev.contact_block;
+    *refreshes = w->host_ctl->contact_state[1];
+    return 0;
+}
+
+int tgl_debug_contact_lists(tgl_world *w, uint32_t *counts, uint32_t *lists) {
+    if (!w || !counts || !lists) return set_error(TGL_ERR_INVALID, "null argument");
+    if (!w->dev.contact_block) return set_error(TGL_ERR_UNSUPPORTED, "contact lists are off for this world");
+    TGL_CUDA(cudaMemcpyAsync(counts, w->dev.contact_count, w->dev.S * 4ull, cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaMemcpyAsync(lists, w->dev.contact_list, (size_t)w->dev.S * w->dev.contact_block * 4ull,
+                             cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
     return 0;
 }
 

@@ -29,11 +29,12 @@ TGL_ERR_UNSUPPORTED = 5
 
 #: Every symbol include/tangle_cuda.h declares.
 EXPORTS = (
-    "tgl_world_create", "tgl_world_destroy", "tgl_run_batch", "tgl_download_positions", "tgl_upload_positions",
+    "tgl_world_create", "tgl_world_destroy", "tgl_world_checkpoint", "tgl_world_restore", "tgl_run_batch", "tgl_download_positions", "tgl_upload_positions",
     "tgl_cell_size", "tgl_cell_count", "tgl_cell_dims", "tgl_neighbor_skin", "tgl_neighbor_block",
     "tgl_neighbor_list_rebuilds", "tgl_debug_rebuild", "tgl_debug_cell_list", "tgl_debug_neighbor_lists",
     "tgl_debug_corrections", "tgl_kernel_launches", "tgl_set_kernel_timing", "tgl_last_kernel_times",
-    "tgl_world_stream", "tgl_contact_pass_noalloc", "tgl_last_error",
+    "tgl_world_stream", "tgl_contact_pass_noalloc", "tgl_contact_list_info", "tgl_debug_contact_lists",
+    "tgl_last_error",
 )
 
 
@@ -139,6 +140,11 @@ def load_library():
     lib.tgl_world_create.restype = ctypes.c_int
     lib.tgl_world_destroy.argtypes = [P]
     lib.tgl_world_destroy.restype = None
+    lib.tgl_world_checkpoint.argtypes = [P, P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]
+    lib.tgl_world_checkpoint.restype = ctypes.c_int
+    lib.tgl_world_restore.argtypes = [ctypes.POINTER(Packed), ctypes.POINTER(CellList), ctypes.c_float,
+                                      ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]
+    lib.tgl_world_restore.restype = ctypes.c_int
     lib.tgl_run_batch.argtypes = [P, ctypes.POINTER(Config), ctypes.c_uint32, ctypes.POINTER(Status)]
     lib.tgl_run_batch.restype = ctypes.c_int
     lib.tgl_download_positions.argtypes = [P, P, ctypes.c_size_t]
@@ -157,6 +163,11 @@ def load_library():
     lib.tgl_neighbor_block.restype = ctypes.c_uint32
     lib.tgl_neighbor_list_rebuilds.argtypes = [P, ctypes.POINTER(ctypes.c_uint32)]
     lib.tgl_neighbor_list_rebuilds.restype = ctypes.c_int
+    lib.tgl_contact_list_info.argtypes = [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32),
+                                           ctypes.POINTER(ctypes.c_uint32)]
+    lib.tgl_contact_list_info.restype = ctypes.c_int
+    lib.tgl_debug_contact_lists.argtypes = [P, P, P]
+    lib.tgl_debug_contact_lists.restype = ctypes.c_int
     lib.tgl_debug_rebuild.argtypes = [P]
     lib.tgl_debug_rebuild.restype = ctypes.c_int
     lib.tgl_debug_cell_list.argtypes = [P, P, P, P]
@@ -237,18 +248,25 @@ def cell_list_struct(cell_list: CellListConfig) -> CellList:
 class DeviceWorld:
     """Resident relaxation world on the current CUDA device."""
 
-    def __init__(self, packed, cell_list: Optional[CellListConfig] = None, max_step: float = 0.006):
+    def __init__(self, packed, cell_list: Optional[CellListConfig] = None, max_step: float = 0.006,
+                 total_iterations: Optional[int] = None):
         lib = load_library()
         cell_list = cell_list or CellListConfig()
         keep: list = []
         pk = packed_struct(packed, keep)
         cl = cell_list_struct(cell_list)
         handle = ctypes.c_void_p()
-        rc = lib.tgl_world_create(ctypes.byref(pk), ctypes.byref(cl), ctypes.c_float(max_step), ctypes.byref(handle))
+        if total_iterations is None:
+            rc = lib.tgl_world_create(ctypes.byref(pk), ctypes.byref(cl), ctypes.c_float(max_step),
+                                      ctypes.byref(handle))
+        else:
+            rc = lib.tgl_world_restore(ctypes.byref(pk), ctypes.byref(cl), ctypes.c_float(max_step),
+                                       int(total_iterations), ctypes.byref(handle))
         if rc:
             _raise(lib, rc)
         self._lib = lib
         self._handle = handle
+        self._packed = packed
         self.vertex_count = packed.vertex_count
         self.segment_count = packed.segment_count
 
@@ -256,6 +274,29 @@ class DeviceWorld:
     def upload(cls, config: RelaxationConfig, packed) -> "DeviceWorld":
         """DeviceWorld::upload(config, packed) (plugin.rs:422-424)."""
         return cls(packed, config.cell_list, config.max_step)
+
+    @classmethod
+    def restore(cls, config: RelaxationConfig, checkpoint) -> "DeviceWorld":
+        """DeviceWorld::restore(config, checkpoint) (plugin.rs:358-391): a
+        world uploaded from the checkpoint's packed assembly whose lifetime
+        iteration count continues from the checkpoint's."""
+        return cls(checkpoint.packed, config.cell_list, config.max_step, checkpoint.total_iterations)
+
+    def checkpoint(self):
+        """DeviceWorld::checkpoint() (plugin.rs:393-404): the packed assembly
+        with the current positions, and the lifetime iteration count."""
+        import dataclasses
+
+        from .checkpoint import DeviceWorldCheckpoint
+
+        xyz = np.empty(3 * self.vertex_count, dtype=np.float32)
+        total = ctypes.c_uint64()
+        self._check(self._lib.tgl_world_checkpoint(self._handle, _ptr(xyz), xyz.size, ctypes.byref(total)))
+        return DeviceWorldCheckpoint(dataclasses.replace(self._packed, positions=xyz), int(total.value))
+
+    def packed(self):
+        """DeviceWorld::packed() (plugin.rs:619-636): the uploaded host assembly."""
+        return self._packed
 
     def close(self) -> None:
         if getattr(self, "_handle", None):
@@ -340,6 +381,28 @@ class DeviceWorld:
         out = ctypes.c_uint32()
         self._check(self._lib.tgl_neighbor_list_rebuilds(self._handle, ctypes.byref(out)))
         return int(out.value)
+
+    def contact_list_info(self) -> dict:
+        """Contact-list skin (0 when off), entries per slot and refreshes so far."""
+        skin = ctypes.c_float()
+        block = ctypes.c_uint32()
+        refreshes = ctypes.c_uint32()
+        self._check(self._lib.tgl_contact_list_info(self._handle, ctypes.byref(skin), ctypes.byref(block),
+                                                    ctypes.byref(refreshes)))
+        return {"skin": float(skin.value), "block": int(block.value), "refreshes": int(refreshes.value)}
+
+    def debug_contact_lists(self):
+        """Contact lists by cell-list slot: counts [S] and a list per slot
+        (None where the count exceeds the block and the Verlet list is read)."""
+        block = self.contact_list_info()["block"]
+        counts = np.empty(self.segment_count, dtype=np.uint32)
+        lists = np.empty(max(block * self.segment_count, 1), dtype=np.uint32)
+        self._check(self._lib.tgl_debug_contact_lists(self._handle, _ptr(counts), _ptr(lists)))
+        out = []
+        for s in range(self.segment_count):
+            n = int(counts[s])
+            out.append(lists[block * s: block * s + n].copy() if n <= block else None)
+        return counts, out
 
     def debug_rebuild(self) -> None:
         self._check(self._lib.tgl_debug_rebuild(self._handle))

@@ -22,7 +22,9 @@ from typing import List, Optional, Union
 
 import numpy as np
 
+from . import checkpoint as ckpt
 from .assembly import Cell, FiberAssembly, PackedAssembly
+from .checkpoint import CheckpointReport, CheckpointSettings
 from .device import DeviceWorld
 from .generate import FiberPopulation, generate_fiber_population
 from .settings import BatchStatus, RelaxationSettings
@@ -58,7 +60,7 @@ class RunResult:
     """The relaxed fibers and run statistics (_tangle.pyi:1003-1014)."""
 
     def __init__(self, assembly: FiberAssembly, status: BatchStatus, uploaded_bytes: int, downloaded_bytes: int,
-                 cell_size: float, cell_count: int, rebuilds: int):
+                 cell_size: float, cell_count: int, rebuilds: int, report: Optional[CheckpointReport] = None):
         self.assembly = assembly
         self._status = status
         self.uploaded_bytes = uploaded_bytes
@@ -66,6 +68,12 @@ class RunResult:
         self.cell_size = cell_size
         self.cell_count = cell_count
         self.neighbor_list_rebuilds = rebuilds
+        report = report or CheckpointReport()
+        self.resumed = report.resumed
+        self.resumed_iteration = report.resumed_iteration
+        self.checkpoint_saves = report.saves
+        self.last_checkpoint_iteration = report.last_saved_iteration
+        self.last_checkpoint_bytes = report.last_saved_bytes
 
     fiber_count = property(lambda self: self.assembly.fiber_count)
     iterations = property(lambda self: self._status.total_iterations)
@@ -135,7 +143,16 @@ class Recipe:
     def centerlines(self) -> List[List[List[float]]]:
         return self._assembly.centerlines()
 
-    def run(self, settings: Optional[RelaxationSettings] = None) -> RunResult:
+    def run(self, settings: Optional[RelaxationSettings] = None, *,
+            checkpoint: Optional[CheckpointSettings] = None) -> RunResult:
+        """Simulates every recorded step and returns the relaxed fibers.
+
+        With `checkpoint`, the run saves a restart file whenever the lifetime
+        iteration count crosses a multiple of `interval_iterations` and when
+        it ends; with `checkpoint.resume` it first restores the world and the
+        recipe's progress from `resume_path` (or `path`), or only the world
+        when `fresh_formation_on_resume` (tangle_checkpoint lib.rs:214-345).
+        """
         if not self._assembly.fibers:
             raise ValueError("recipe contains no fibers")
         if not self._operations:
@@ -152,14 +169,52 @@ class Recipe:
             descriptions.append("relax until converged")
         assembly = copy.deepcopy(self._assembly)
         packed = PackedAssembly.from_assembly(assembly, config.pin_fiber_ends)
-        world = DeviceWorld.upload(config, packed)
         status = BatchStatus(max_penetration=float("inf"), max_curvature_ratio=float("inf"))
+        report = CheckpointReport()
+        first_operation, first_completed = 0, 0
+        if checkpoint is not None and checkpoint.resume:
+            source = checkpoint.resume_path or checkpoint.path
+            saved = ckpt.load(source, checkpoint.resume_case_id or checkpoint.case_id)
+            if saved.device.packed.vertex_count != packed.vertex_count or \
+                    saved.device.packed.segment_count != packed.segment_count:
+                raise ckpt.CheckpointError("checkpoint assembly does not match the recipe's fibers")
+            world = DeviceWorld.restore(config, saved.device)
+            packed = saved.device.packed
+            status = BatchStatus(total_iterations=saved.device.total_iterations, max_penetration=float("inf"),
+                                 max_curvature_ratio=float("inf"))
+            if not checkpoint.fresh_formation_on_resume:
+                first_operation, first_completed = saved.operation, saved.operation_iterations
+                status.converged = saved.converged
+            report.resumed = True
+            report.resumed_iteration = saved.device.total_iterations
+            report.last_saved_iteration = saved.device.total_iterations
+        else:
+            world = DeviceWorld.upload(config, packed)
         downloaded = 0
+
+        def save(index: int, completed: int, terminal: bool) -> None:
+            nonlocal downloaded
+            if checkpoint is None:
+                return
+            iteration = status.total_iterations
+            if iteration == 0 or report.last_saved_iteration == iteration:
+                return
+            if not terminal and not ckpt.crossed_interval(iteration, report.last_saved_iteration,
+                                                          checkpoint.interval_iterations):
+                return
+            state = world.checkpoint()
+            downloaded += state.packed.positions.nbytes + 8
+            size = ckpt.save(checkpoint.path, ckpt.RunCheckpoint(checkpoint.case_id, state, index, completed,
+                                                                   status.converged))
+            report.saves += 1
+            report.last_saved_iteration = iteration
+            report.last_saved_bytes = size
+
         try:
             for index, op in enumerate(operations):
-                if isinstance(op, _Insert):
+                if isinstance(op, _Insert) or index < first_operation:
                     continue
-                started = status.total_iterations
+                started = status.total_iterations - (first_completed if index == first_operation else 0)
                 force = isinstance(op, _RelaxFor)
                 budget = op.iterations if force else op.maximum_iterations
                 while True:
@@ -183,13 +238,16 @@ class Recipe:
                     status = world.run_batch(batch_config, batch)
                     downloaded += 11 * 4 + 3 * 4
                     if status.cell_list_overflow:
+                        save(index, status.total_iterations - started, True)
                         raise RecipeError(index, descriptions[index], status.total_iterations, "cell list overflow")
+                    save(index, status.total_iterations - started, False)
                 if force:
                     status.converged = False
+            save(len(operations), 0, True)
             positions = world.download_positions()
             downloaded += positions.nbytes
             packed.unpack_positions(positions, assembly)
             return RunResult(assembly, status, _upload_bytes(packed), downloaded, world.cell_size, world.cell_count,
-                             world.neighbor_list_rebuilds())
+                             world.neighbor_list_rebuilds(), report)
         finally:
             world.close()
