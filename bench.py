@@ -188,13 +188,17 @@ def contact_bytes(world):
     return listed, refresh
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the contact pass from the committed ncu summary."""
+def ncu_traffic(refresh_share: float, lists_on: bool):
+    """Per-pass DRAM bytes of the contact pass from the committed ncu summary
+    (listed and refresh passes weighted by their share of the passes)."""
     path = os.path.join(ROOT, "profiles", "contact_traffic.json")
     try:
         with open(path) as fh:
             data = json.load(fh)
-        return float(data["dram_bytes_per_launch_full_size"])
+        if not lists_on:
+            return float(data["dram_bytes_per_full_pass"])
+        return (refresh_share * float(data["dram_bytes_per_refresh_pass"]) +
+                (1.0 - refresh_share) * float(data["dram_bytes_per_listed_pass"]))
     except (OSError, KeyError, ValueError):
         return None
 
@@ -360,7 +364,7 @@ def run_cuda(args):
     peak, peak_kind = measured_peak()
     achieved = algorithmic / avg_contact_s / 1.0e9 if avg_contact_s > 0 else 0.0
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": ncu_traffic(), "peak_source": f"{peak_kind} hbm_gbs",
+                "traffic": ncu_traffic(refresh_share, contact_info["block"] > 0), "peak_source": f"{peak_kind} hbm_gbs",
                 "kernel": "contact_kernel (find_segment_corrections)",
                 "algorithmic_bytes_per_launch": algorithmic, "avg_launch_ms": avg_contact_s * 1000.0,
                 "contact_passes": contact_passes, "refresh_passes": refreshes,

@@ -1027,7 +1027,11 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
         // reproduces the serial sweep exactly.
         if (n >= 3) {
             const int last = n - 3;  // triplets t = 0..last: (t, t+1, t+2)
+            // A pass that moves nothing leaves the positions as they were, so
+            // every later pass would test the same triplets and move nothing
+            // either: the sweeps end there.
             for (uint32_t sweep = 0; sweep < sp.curvature_cleanup_sweeps; ++sweep) {
+                bool moved = false;
                 int t0 = 0;
                 while (t0 <= last) {
                     int t = t0 + lane;
@@ -1040,11 +1044,14 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
                         t0 += 32;
                         continue;
                     }
+                    moved = true;
                     int j = __ffs(ballot) - 1;
                     if (lane == j) curvature_triplet_apply(P, St, t, t + 1, t + 2, tr, g);
                     __syncwarp();
                     t0 += j + 1;
                 }
+                if (!moved) break;
+                moved = false;
                 t0 = last;
                 while (t0 >= 0) {
                     int t = t0 - lane;
@@ -1057,11 +1064,13 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
                         t0 -= 32;
                         continue;
                     }
+                    moved = true;
                     int j = __ffs(ballot) - 1;
                     if (lane == j) curvature_triplet_apply(P, St, t, t + 1, t + 2, tr, g);
                     __syncwarp();
                     t0 -= j + 1;
                 }
+                if (!moved) break;
             }
         }
         __syncwarp();
@@ -1354,7 +1363,10 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             const int last = (int)span.y - 3;
             const float extent = w.seg_static[w.fiber_s0[mine]].x;
             float4 *P = lanes_smem + (size_t)group * stride;
+            // A pass that moves nothing ends the sweeps (every later pass
+            // would test the same positions).
             for (uint32_t sweep = 0; sweep < sp.curvature_cleanup_sweeps; ++sweep) {
+                bool moved = false;
                 int t0 = 0;
                 while (t0 <= last) {
                     const int t = t0 + gl;
@@ -1367,11 +1379,14 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                         t0 += LPF;
                         continue;
                     }
+                    moved = true;
                     const int first = __ffs(bits) - 1;
                     if (gl == first) lanes_apply(P, t, tr, extent, g);
                     __syncwarp(gmask);
                     t0 += first + 1;
                 }
+                if (!moved) break;
+                moved = false;
                 t0 = last;
                 while (t0 >= 0) {
                     const int t = t0 - gl;
@@ -1384,11 +1399,13 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                         t0 -= LPF;
                         continue;
                     }
+                    moved = true;
                     const int first = __ffs(bits) - 1;
                     if (gl == first) lanes_apply(P, t, tr, extent, g);
                     __syncwarp(gmask);
                     t0 -= first + 1;
                 }
+                if (!moved) break;
             }
         }
         __syncwarp();
