@@ -258,6 +258,39 @@ typedef struct {
 int tgl_contact_pass_noalloc(const tgl_noalloc_inputs *inputs, float *corrections, float *segment_max_penetration,
                              void *stream);
 
+/* ---- Learned warm start (no reference counterpart: an addition on top of
+ * the plain method, which stays the drop-in and runs after it to the same
+ * gates). */
+
+/* One BF16 matrix product on the tensor cores (tcgen05.mma, f32 accumulate
+ * in tensor memory): D[m x n] = sum_k A[m, k] B[n, k], then + bias[n],
+ * then max(0, .) when relu, stored as f32 (out_f32[i * ldo + j]) and/or
+ * bf16 (out_bf16[i * ldo_bf16 + j]). A and B are device bf16 arrays, each
+ * K-major (A[i * lda + k]) or MN-major (A[k * lda + i]); n is a multiple of
+ * 16 in [16, 256]; leading dimensions are multiples of 8, and so is k when
+ * an operand is K-major; pointers are 16-byte aligned. With k_split > 0
+ * (a multiple of 64) the contraction is split over CTAs and split s writes
+ * its partial product to out_f32 + s * m * ldo (no bias, relu or bf16).
+ * `error` (device u32, may be null) is set to 1 if a wait for the tensor
+ * cores gave up. Queued on `stream`; returns without waiting. */
+typedef struct tgl_gemm {
+    const void *a;
+    const void *b;
+    int64_t lda, ldb;
+    int32_t m, n;
+    int64_t k;
+    int32_t a_mn, b_mn;
+    int64_t k_split;
+    const float *bias;
+    int32_t relu, reserved;
+    float *out_f32;
+    int64_t ldo;
+    void *out_bf16;
+    int64_t ldo_bf16;
+    unsigned int *error;
+} tgl_gemm;
+int tgl_gemm_bf16(const tgl_gemm *gemm, void *stream);
+
 /* Thread-local message of the last failed call on this thread. */
 const char *tgl_last_error(void);
 

@@ -34,6 +34,7 @@ EXPORTS = (
     "tgl_neighbor_list_rebuilds", "tgl_debug_rebuild", "tgl_debug_cell_list", "tgl_debug_neighbor_lists",
     "tgl_debug_corrections", "tgl_kernel_launches", "tgl_set_kernel_timing", "tgl_last_kernel_times",
     "tgl_world_stream", "tgl_contact_pass_noalloc", "tgl_contact_list_info", "tgl_debug_contact_lists",
+    "tgl_gemm_bf16",
     "tgl_last_error",
 )
 

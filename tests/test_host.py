@@ -139,7 +139,7 @@ def test_c_abi_library_loads_and_exports_every_declared_symbol():
     build()
     lib = ctypes.CDLL(LIB)
     header = open(os.path.join(ROOT, "include", "tangle_cuda.h")).read()
-    declared = set(re.findall(r"\b(tgl_[a-z_]+)\s*\(", header))
+    declared = set(re.findall(r"\b(tgl_[a-z0-9_]+)\s*\(", header))
     assert declared == set(EXPORTS)
     for name in declared:
         assert hasattr(lib, name), name
