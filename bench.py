@@ -19,8 +19,10 @@ Printed JSON line (rank 0):
   region, against the measured HBM copy bandwidth;
 * cpu_baseline -- the CPU oracle on the same specimen, all host threads,
   a bounded sample of iterations;
-* time_to_admissible -- seconds for plain PBD from the initial specimen to
-  max overlap < 1e-3 d with curvature <= limit.
+* time_to_admissible -- seconds from the initial specimen to max overlap
+  < 1e-3 d with curvature <= limit (or the iteration cap), for plain PBD and
+  for the learned warm start followed by plain PBD, with the time at which
+  the max overlap first fell below 0.1, 0.05, 0.03, 0.02, 0.01 and 0.001 d.
 
 `--impl reference` times the reference algorithm's CPU restatement (the
 oracle; the reference is Rust and cannot be built here) on the same
@@ -59,6 +61,7 @@ def parse():
     ap.add_argument("--capacity", type=int, default=256, help="neighbor slots per segment")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tta", action="store_true")
+    ap.add_argument("--tta-iterations", type=int, default=20000, help="iteration cap of each time-to-admissible run")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-iterations", type=int, default=40)
     ap.add_argument("--reference-iterations", type=int, default=4,
@@ -201,6 +204,57 @@ def ncu_traffic(refresh_share: float, lists_on: bool):
                 (1.0 - refresh_share) * float(data["dram_bytes_per_listed_pass"]))
     except (OSError, KeyError, ValueError):
         return None
+
+
+MILESTONES = (0.1, 0.05, 0.03, 0.02, 0.01, 0.001)  # max overlap / d
+
+
+def time_to_admissible(packed, config, d_min, net, limit):
+    """Relaxes a fresh world to the gate (max overlap < tolerance, curvature
+    within its limit) or `limit` iterations, recording when the max overlap
+    first falls below each milestone; with `net`, the warm start runs first
+    (its time included)."""
+    import torch
+
+    from tangle_b200.device import DeviceWorld
+
+    world = DeviceWorld(packed, config.cell_list, config.max_step)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    report = None
+    if net is not None:
+        from tangle_b200.warmstart import warm_start
+
+        report = warm_start(world, net, config)
+    reached = {}
+    status = None
+    while True:
+        status = world.run_batch(config, config.iterations_per_batch)
+        elapsed = time.perf_counter() - t0
+        for m in MILESTONES:
+            if m not in reached and status.max_penetration <= m * d_min:
+                reached[m] = {"seconds": elapsed, "iterations": status.total_iterations}
+        if status.converged or status.total_iterations >= limit:
+            break
+    out = {"seconds": time.perf_counter() - t0, "iterations": status.total_iterations, "converged": status.converged,
+           "max_penetration_over_d": status.max_penetration / d_min,
+           "max_curvature_ratio": status.max_curvature_ratio,
+           "milestones_over_d": {str(m): reached.get(m) for m in MILESTONES},
+           "method": "plain PBD" if net is None else "learned warm start, then plain PBD"}
+    if report is not None:
+        out["warm_start"] = {"accepted": report.accepted, "seconds": report.seconds, "edges": report.edges,
+                             "residual_before": report.residual_before, "residual_after": report.residual_after}
+    world.close()
+    return out
+
+
+def load_warmstart_net():
+    path = os.path.join(ROOT, "tangle_b200", "warmstart_net.npz")
+    if not os.path.exists(path):
+        return None
+    from tangle_b200.warmstart import WarmStartNet
+
+    return WarmStartNet.load(path)
 
 
 def cpu_baseline(packed, config, nodes, iterations):
@@ -398,20 +452,16 @@ def run_cuda(args):
                "d2h_bytes_per_step": 12 * nodes + 64}
     world.close()
 
-    # Time to admissible from the initial specimen (plain PBD, device-resident).
+    # Time to admissible from the initial specimen, plain PBD and with the
+    # learned warm start first (device-resident, same gates, same cap).
     tta = None
     if not args.no_tta:
-        fresh = DeviceWorld(packed, config.cell_list, config.max_step)
-        t0 = time.perf_counter()
-        status = None
-        while True:
-            status = fresh.run_batch(config, config.iterations_per_batch)
-            if status.converged or status.total_iterations >= 20000:
-                break
-        tta = {"seconds": time.perf_counter() - t0, "iterations": status.total_iterations,
-               "converged": status.converged, "max_penetration_over_d": status.max_penetration / d_min,
-               "max_curvature_ratio": status.max_curvature_ratio, "method": "plain PBD"}
-        fresh.close()
+        tta = {"plain": time_to_admissible(packed, config, d_min, None, args.tta_iterations)}
+        net = load_warmstart_net()
+        if net is not None:
+            tta["warm_start"] = time_to_admissible(packed, config, d_min, net, args.tta_iterations)
+        else:
+            tta["warm_start"] = {"unavailable": "no trained network (tangle_b200/warmstart_net.npz)"}
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu:

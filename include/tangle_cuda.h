@@ -118,6 +118,24 @@ int tgl_world_create(const tgl_packed *packed, const tgl_cell_list_config *cell_
 /* Drop of the world (frees every device buffer and captured graph). */
 void tgl_world_destroy(tgl_world *world);
 
+/* Batched relaxation (no reference counterpart: the reference relaxes one
+ * world at a time). Packs `count` specimens into one arena: their vertices,
+ * segments, fibers and cells concatenated in order (specimen i's vertex v
+ * is arena vertex v + the vertex counts of specimens 0..i-1), each with its
+ * own box, cell grid, neighbor skin, lists and control word, sized exactly
+ * as tgl_world_create sizes it alone. tgl_run_batch then advances every
+ * specimen in one captured graph; each specimen's gate stops it on its own
+ * (its convergence mask), as a batch of its own world would, and the batch
+ * status covers all of them (largest counts and metrics; converged when all
+ * are). One neighbor-list block serves every specimen: the capacity within
+ * max_list_bytes (8 GiB when 0). Contact lists are off; fibers of at most
+ * 256 vertices. Checkpoints, residuals and the warm start take single
+ * worlds. */
+int tgl_arena_create(const tgl_packed *specimens, uint32_t count, const tgl_cell_list_config *cell_list,
+                     float max_step, tgl_world **out);
+/* Each specimen's status after the last batch (statuses[count]). */
+int tgl_arena_status(tgl_world *world, const tgl_relax_config *config, tgl_batch_status *statuses, uint32_t count);
+
 /* DeviceFiberWorld::checkpoint (world.rs:758-823; plugin.rs:393-404) for the
  * plain path: the persistent state a restart needs, which is the current
  * positions (interleaved xyz, len = 3 * vertex_count) and the lifetime
@@ -283,6 +301,10 @@ typedef struct tgl_gemm {
     int64_t k_split;
     const float *bias;
     int32_t relu, reserved;
+    const void *mask;         /* bf16 [m x ld_mask]: zero the result where mask <= 0 (after relu) */
+    int64_t ld_mask;
+    const float *residual;    /* f32 [m x ld_res]: added last */
+    int64_t ld_res;
     float *out_f32;
     int64_t ldo;
     void *out_bf16;
@@ -290,6 +312,93 @@ typedef struct tgl_gemm {
     unsigned int *error;
 } tgl_gemm;
 int tgl_gemm_bf16(const tgl_gemm *gemm, void *stream);
+
+/* The contact graph of a world for message passing: nodes are vertices;
+ * edges are directed segment pairs (dst <- src) whose gap is within a
+ * cutoff, both directions of every pair present, grouped by destination
+ * segment (CSR `offsets`) and by ascending source within one. All pointers
+ * are device memory owned by the world (valid until its next graph build). */
+typedef struct tgl_mp_graph {
+    int32_t vertex_count, segment_count, edge_count, reserved;
+    const int32_t *seg_v0;   /* [S] first vertex of each segment (the second is the next) */
+    const int32_t *links;    /* [4 V] previous vertex, next vertex, segment before, segment after; -1 = none */
+    const int32_t *offsets;  /* [S + 1] */
+    const int32_t *dst, *src, *twin;  /* [E]; twin = the reverse edge */
+    const float *s, *t;      /* [E] closest-point parameters on dst / src */
+} tgl_mp_graph;
+
+/* Device buffers a contact graph is written into (sizes: V vertices, S
+ * segments, E edges). */
+typedef struct tgl_mp_graph_out {
+    int32_t *seg_v0;       /* [S] */
+    int32_t *links;        /* [4 V] */
+    int32_t *offsets;      /* [S + 1] */
+    int32_t *dst, *src, *twin;  /* [E] */
+    float *s, *t;          /* [E] */
+    void *node_features;   /* bf16 [V x 16] */
+    void *edge_features;   /* bf16 [E x 16] */
+} tgl_mp_graph_out;
+
+/* The contact graph of the world's current positions, in two calls: the
+ * first rebuilds the neighbor lists from the positions and counts the
+ * edges (pairs of the Verlet lists whose closest-point gap is at most
+ * `cutoff`, both directions); the second, with the same world and nothing
+ * run in between, writes the graph and its features into `out`:
+ * node features (unit tangent, curvature x d, rest curvature x d,
+ * d / 10 um, overlap depth / d, and the push: the depth-weighted unit
+ * normals away from the vertex's contacts / d) and edge features
+ * (closest-point offset / d,
+ * overlap depth / d, s, t), each padded with zeros to 16. Both wait for
+ * completion. */
+int tgl_warmstart_graph_count(tgl_world *world, float cutoff, int64_t *edge_count);
+int tgl_warmstart_graph_fill(tgl_world *world, const tgl_mp_graph_out *out);
+
+/* Moves every unpinned vertex by scale * dx[v * ld .. v * ld + 2] (device
+ * f32; times the vertex's fiber diameter when in_diameters), each move
+ * capped at max_step, walls respected; queued on the world's stream. The
+ * next batch's displacement checks see the move. */
+int tgl_world_displace(tgl_world *world, const float *dx, int64_t ld, float scale, int32_t in_diameters,
+                       float max_step);
+
+/* The residual of the current positions without moving them (one contact
+ * pass on lists valid for them): maximum penetration, maximum curvature
+ * ratio, and the sum over segments of their deepest penetration divided by
+ * their diameter. */
+int tgl_world_residual(tgl_world *world, const tgl_relax_config *config, float *max_penetration,
+                       float *max_curvature_ratio, float *total_penetration);
+
+/* Message-passing steps over a graph, hidden width 64, queued on `stream`.
+ * x_edge[e, 0:64] = bf16((1 - t_e) h[first vertex of src] + t_e h[second]). */
+int tgl_mp_edge_inputs(const tgl_mp_graph *graph, const float *h, void *x_edge, int64_t ld_x, void *stream);
+/* x_node[v] (bf16, 192 wide) = [h_v, the mean of the messages m (f32
+ * [E x 64]) into the vertex's two segments weighted by the vertex's share
+ * (1 - s or s; divided by the total share, at least 1), mean of the fiber
+ * neighbors' h]. */
+int tgl_mp_node_inputs(const tgl_mp_graph *graph, const float *h, const float *m, void *x_node, void *stream);
+/* Backward of tgl_mp_node_inputs: dh (f32 [V x 64]) += the h and
+ * neighbor-mean parts of dx_node (f32 [V x 192]); dm (bf16 [E x 64], and
+ * f32 when dm_f32 is not null) = the message gradient. */
+int tgl_mp_node_inputs_backward(const tgl_mp_graph *graph, const float *dx_node, float *dh, void *dm, float *dm_f32,
+                                void *stream);
+/* dst (bf16) = src (f32), n elements. */
+int tgl_convert_bf16(int64_t n, const float *src, void *dst, void *stream);
+/* Backward of tgl_mp_edge_inputs: dh += the shares of dx_edge[:, 0:64]. */
+int tgl_mp_edge_inputs_backward(const tgl_mp_graph *graph, const float *dx_edge, int64_t ld_dx, float *dh,
+                                void *stream);
+/* out[j] (+)= sum_i x[i * ld + j] for j < n, in a fixed order; scratch holds
+ * tgl_column_sums_scratch(rows, n) floats. */
+int64_t tgl_column_sums_scratch(int64_t rows, int32_t n);
+int tgl_column_sums(const float *x, int64_t rows, int32_t n, int64_t ld, float *out, int32_t accumulate,
+                    float *scratch, void *stream);
+/* One Adam step (bias-corrected; step counts from 1) on n f32 weights, and
+ * their bf16 copy when w_bf16 is not null. */
+int tgl_adam_step(int64_t n, float *w, const float *g, float *m, float *v, void *w_bf16, float lr, float beta1,
+                  float beta2, float eps, int32_t step, void *stream);
+/* Mean squared error of y[:, 0:cols] against target [rows x cols] into
+ * *loss, and dy = its gradient (f32 and/or bf16, zero past cols); scratch
+ * holds 1024 floats. */
+int tgl_mse(int64_t rows, const float *y, int64_t ld_y, const float *target, int32_t cols, float *loss, float *dy,
+            int64_t ld_dy, void *dy_bf16, float *scratch, void *stream);
 
 /* Thread-local message of the last failed call on this thread. */
 const char *tgl_last_error(void);

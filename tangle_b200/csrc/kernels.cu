@@ -31,16 +31,58 @@ constexpr int CELL_SORT_CAP = 512;  // slots sorted in shared memory per cell
 
 __device__ inline uint32_t warp_max_u32(uint32_t v) { return __reduce_max_sync(FULL, v); }
 
+// Specimen accessors. A single world is specimen 0 with the world's own
+// grid, skin and control word (the ARENA = false instantiations compile to
+// exactly that); an arena looks each element's specimen up.
+template <bool A> __device__ inline uint32_t spec_of_seg(const WorldDev &w, uint32_t s) { return A ? w.seg_spec[s] : 0u; }
+template <bool A> __device__ inline uint32_t spec_of_fiber(const WorldDev &w, uint32_t f) {
+    return A ? w.fiber_spec[f] : 0u;
+}
+template <bool A> __device__ inline uint32_t spec_of_vtx(const WorldDev &w, uint32_t v) { return A ? w.vtx_spec[v] : 0u; }
+template <bool A> __device__ inline uint32_t spec_of_cell(const WorldDev &w, uint32_t c) {
+    return A ? w.cell_spec[c] : 0u;
+}
+template <bool A> __device__ inline const Grid &grid_of(const WorldDev &w, uint32_t p) {
+    return A ? w.specs[p].grid : w.grid;
+}
+template <bool A> __device__ inline float skin_of(const WorldDev &w, uint32_t p) { return A ? w.specs[p].skin : w.skin; }
+template <bool A> __device__ inline uint32_t cell_base_of(const WorldDev &w, uint32_t p) {
+    return A ? w.specs[p].cell_base : 0u;
+}
+template <bool A> __device__ inline Control *ctl_of(const WorldDev &w, uint32_t p) { return A ? w.ctl + 1 + p : w.ctl; }
+// Whether specimen p's rebuild is pending (an arena rebuilds per specimen).
+template <bool A> __device__ inline bool rebuilding(const WorldDev &w, uint32_t p) {
+    return ctl_of<A>(w, p)->neighbor_state[0] != 0;
+}
+// Raises specimen p's rebuild flag (and, in an arena, the any-specimen one).
+template <bool A> __device__ inline void flag_rebuild(const WorldDev &w, uint32_t p) {
+    ctl_of<A>(w, p)->neighbor_state[0] = 1;
+    if (A) w.ctl->neighbor_state[0] = 1;
+}
+
 // ---------------------------------------------------------------- batch control
 
 // kernels.rs:3-12 begin_relaxation_batch; also clears the gate accumulators.
-__global__ void begin_batch_kernel(Control *ctl) {
+__device__ inline void begin_batch(Control *ctl) {
     ctl->control[2] = 0;
     if (ctl->control[3] == 0) ctl->control[0] = 1;
     ctl->acc[0] = 0;
     ctl->acc[1] = 0;
     ctl->acc[2] = 0;
     ctl->done_blocks = 0;
+}
+
+template <bool A>
+__global__ void begin_batch_kernel(WorldDev w) {
+    if (!A) {
+        if (threadIdx.x == 0) begin_batch(w.ctl);
+        return;
+    }
+    for (uint32_t p = threadIdx.x; p < w.P; p += blockDim.x) begin_batch(w.ctl + 1 + p);
+    if (threadIdx.x == 0) {
+        w.ctl->control[0] = 1;  // some specimen may run; the first gate refines it
+        w.ctl->done_blocks = 0;
+    }
 }
 
 // Whether vertex v at (x, y, z) has moved more than half the contact skin
@@ -54,23 +96,32 @@ __device__ inline bool contact_moved(const WorldDev &w, uint32_t v, float x, flo
 
 // neighbor.rs:446-465, over every vertex (all are active in the plain path),
 // and the same check against the contact lists' snapshot.
+template <bool A>
 __global__ void flag_displacement_kernel(WorldDev w) {
     uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     bool far = false, contact_far = false;
     if (v < w.V) {
-        float md = 0.5f * w.skin;
+        const uint32_t spec = spec_of_vtx<A>(w, v);
+        float md = 0.5f * skin_of<A>(w, spec);
         float4 p = w.pos[v], r = w.ref_pos[v];
         float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
         far = dx * dx + dy * dy + dz * dz > md * md;
-        if (w.contact_skin > 0.0f) contact_far = contact_moved(w, v, p.x, p.y, p.z);
+        if (A && far) flag_rebuild<A>(w, spec);
+        if (!A && w.contact_skin > 0.0f) contact_far = contact_moved(w, v, p.x, p.y, p.z);
     }
+    if (A) return;
     if (w.contact_skin > 0.0f && v < w.S && w.geom[2 * (size_t)v + 1].w > w.contact_half_limit) contact_far = true;
     if (__any_sync(FULL, far) && (threadIdx.x & 31) == 0) w.ctl->neighbor_state[0] = 1;
     if (__any_sync(FULL, contact_far) && (threadIdx.x & 31) == 0) w.ctl->contact_state[0] = 1;
 }
 
-// neighbor.rs:436-441.
-__global__ void request_rebuild_kernel(Control *ctl) { ctl->neighbor_state[0] = 1; }
+// neighbor.rs:436-441 (every specimen of an arena).
+template <bool A>
+__global__ void request_rebuild_kernel(WorldDev w) {
+    if (A)
+        for (uint32_t p = threadIdx.x; p < w.P; p += blockDim.x) w.ctl[1 + p].neighbor_state[0] = 1;
+    if (threadIdx.x == 0) w.ctl->neighbor_state[0] = 1;
+}
 
 // kernels.rs:925-980 at one interior vertex of a fiber whose positions are
 // p(local index).
@@ -94,12 +145,15 @@ __device__ inline float curvature_ratio_at(Fetch p, int i, float maximum) {
 
 // Gate inputs for the first step of a batch: curvature ratio of the current
 // positions and the last applied step (kernels.rs:112-127).
+template <bool A>
 __global__ void measure_start_kernel(WorldDev w) {
     if (w.ctl->control[0] == 0) return;
     const int lane = threadIdx.x & 31;
     const int warps = blockDim.x >> 5;
     uint32_t cmax = 0, smax = 0;
     for (uint32_t f = blockIdx.x * warps + (threadIdx.x >> 5); f < w.F; f += gridDim.x * warps) {
+        const uint32_t spec = spec_of_fiber<A>(w, f);
+        if (A && ctl_of<A>(w, spec)->control[0] == 0) continue;
         uint2 span = w.fiber_vspan[f];
         const float4 *P = w.pos + span.x;
         for (uint32_t i = lane; i < span.y; i += 32) {
@@ -113,7 +167,17 @@ __global__ void measure_start_kernel(WorldDev w) {
                 }
             }
         }
+        if (A) {  // per fiber: its specimen's maxima
+            cmax = warp_max_u32(cmax);
+            smax = warp_max_u32(smax);
+            if (lane == 0) {
+                if (smax) atomicMax(&ctl_of<A>(w, spec)->acc[1], smax);
+                if (cmax) atomicMax(&ctl_of<A>(w, spec)->acc[2], cmax);
+            }
+            cmax = smax = 0;
+        }
     }
+    if (A) return;
     cmax = warp_max_u32(cmax);
     smax = warp_max_u32(smax);
     if (lane == 0) {
@@ -125,19 +189,27 @@ __global__ void measure_start_kernel(WorldDev w) {
 // ---------------------------------------------------------------- cell list
 // cell_list.rs:63-434 / world/cell_list.rs:94-209, gated on the rebuild flag.
 
+// (In an arena, only the cells, segments and vertices of specimens whose
+// rebuild is pending are touched: each specimen owns a contiguous cell range
+// and the slot range of its own segment ids, so the other specimens' lists
+// stay as they are.)
+template <bool A>
 __global__ void rb_clear_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < w.C; c += gridDim.x * blockDim.x)
-        w.cell_counts[c] = 0;
+        if (!A || rebuilding<A>(w, spec_of_cell<A>(w, c))) w.cell_counts[c] = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) w.ctl->cell_overflow = 0;
 }
 
 // count_cell_segments: each segment's midpoint cell, and its arrival ticket.
+template <bool A>
 __global__ void rb_count_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < w.S; s += gridDim.x * blockDim.x) {
+        const uint32_t spec = spec_of_seg<A>(w, s);
+        if (A && !rebuilding<A>(w, spec)) continue;
         float4 a = w.geom[2 * (size_t)s], b = w.geom[2 * (size_t)s + 1];
-        uint32_t cell = proxy_cell(a.x, a.y, a.z, b.x, b.y, b.z, w.grid);
+        uint32_t cell = cell_base_of<A>(w, spec) + proxy_cell(a.x, a.y, a.z, b.x, b.y, b.z, grid_of<A>(w, spec));
         w.cell_of[s] = cell;
         w.ticket[s] = atomicAdd(&w.cell_counts[cell], 1u);
     }
@@ -192,15 +264,17 @@ __global__ void __launch_bounds__(1024) rb_scan_kernel(WorldDev w) {
 }
 
 // scatter_cell_segments.
+template <bool A>
 __global__ void rb_scatter_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < w.S; s += gridDim.x * blockDim.x)
-        w.cell_segments[w.cell_offsets[w.cell_of[s]] + w.ticket[s]] = s;
+        if (!A || rebuilding<A>(w, spec_of_seg<A>(w, s))) w.cell_segments[w.cell_offsets[w.cell_of[s]] + w.ticket[s]] = s;
 }
 
 // rank_cell_segments (cell_list.rs:392-434): ascending segment order inside
 // every cell. One warp per cell; a rank sort in shared memory, or over the
 // global range (into the free ticket array) for very crowded cells.
+template <bool A>
 __global__ void rb_sort_cells_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     extern __shared__ uint32_t sort_smem[];
@@ -208,6 +282,7 @@ __global__ void rb_sort_cells_kernel(WorldDev w) {
     const int warps = blockDim.x >> 5;
     uint32_t *buf = sort_smem + warp * CELL_SORT_CAP;
     for (uint32_t c = blockIdx.x * warps + warp; c < w.C; c += gridDim.x * warps) {
+        if (A && !rebuilding<A>(w, spec_of_cell<A>(w, c))) continue;
         uint32_t n = w.cell_counts[c];
         if (n < 2) continue;
         uint32_t off = w.cell_offsets[c];
@@ -238,10 +313,12 @@ __global__ void rb_sort_cells_kernel(WorldDev w) {
 // gather_cell_slot_geometry (neighbor.rs:107-153): geometry in slot order,
 // plus each slot's bounding sphere (midpoint, half length + radius) for the
 // build's pre-test.
+template <bool A>
 __global__ void rb_gather_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.S; slot += gridDim.x * blockDim.x) {
         uint32_t s = w.cell_segments[slot];
+        if (A && !rebuilding<A>(w, spec_of_seg<A>(w, s))) continue;
         float4 a = w.geom[2 * (size_t)s], b = w.geom[2 * (size_t)s + 1];
         w.slot_geom[2 * (size_t)slot] = a;
         w.slot_geom[2 * (size_t)slot + 1] = b;
@@ -251,16 +328,16 @@ __global__ void rb_gather_kernel(WorldDev w) {
 
 // The exact pair test of build_segment_neighbor_lists (neighbor.rs:282-359)
 // for home segment 1 against the segment in `slot`.
-__device__ inline bool build_pair(const WorldDev &w, float p1x, float p1y, float p1z, float q1x, float q1y,
-                                  float q1z, float d1x, float d1y, float d1z, float radius, float half_length,
-                                  uint32_t segment, float4 own, uint32_t slot, uint32_t &other) {
+__device__ inline bool build_pair(const WorldDev &w, const Grid &grid, float skin, float p1x, float p1y, float p1z,
+                                  float q1x, float q1y, float q1z, float d1x, float d1y, float d1z, float radius,
+                                  float half_length, uint32_t segment, float4 own, uint32_t slot, uint32_t &other) {
     const float4 oa = w.slot_geom[2 * (size_t)slot], ob = w.slot_geom[2 * (size_t)slot + 1];
     other = w.cell_segments[slot];
     float p2x = oa.x, p2y = oa.y, p2z = oa.z, q2x = ob.x, q2y = ob.y, q2z = ob.z;
     const float other_radius = oa.w;
-    bool moved = minimum_image(p1x, p1y, p1z, q1x, q1y, q1z, p2x, p2y, p2z, q2x, q2y, q2z, w.grid);
+    bool moved = minimum_image(p1x, p1y, p1z, q1x, q1y, q1z, p2x, p2y, p2z, q2x, q2y, q2z, grid);
     float d2x = q2x - p2x, d2y = q2y - p2y, d2z = q2z - p2z;
-    float interaction = (radius + other_radius + w.skin) * (1.0f + 1.0e-4f);
+    float interaction = (radius + other_radius + skin) * (1.0f + 1.0e-4f);
     float mdx = 0.5f * (p2x + q2x - p1x - q1x);
     float mdy = 0.5f * (p2y + q2y - p1y - q1y);
     float mdz = 0.5f * (p2z + q2z - p1z - q1z);
@@ -287,7 +364,8 @@ __device__ inline bool build_pair(const WorldDev &w, float p1x, float p1y, float
 // unwrapped, so a segment's cell says nothing about its image.) Survivors
 // queue up and get the exact test 32 at a time; hits append in scan order
 // and are sorted later.
-__global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int prefilter, float sphere_eps) {
+template <bool A>
+__global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int prefilter_world, float sphere_eps_world) {
     if (w.ctl->neighbor_state[0] == 0) return;
     extern __shared__ float4 build_smem[];
     uint32_t *slot_of = reinterpret_cast<uint32_t *>(build_smem + ch);
@@ -295,16 +373,22 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
     __shared__ uint32_t queue[8][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int warps = blockDim.x >> 5;
-    const float skin = w.skin;
     const uint32_t block = w.block;
-    const Grid &g = w.grid;
     uint32_t *q = queue[warp];
     for (uint32_t h = blockIdx.x; h < w.C; h += gridDim.x) {
+        const uint32_t spec = spec_of_cell<A>(w, h);
+        if (A && !rebuilding<A>(w, spec)) continue;
+        const Grid &g = grid_of<A>(w, spec);
+        const float skin = skin_of<A>(w, spec);
+        const uint32_t cell_base = cell_base_of<A>(w, spec);
+        const int prefilter = A ? (int)w.specs[spec].build_prefilter : prefilter_world;
+        const float sphere_eps = A ? w.specs[spec].build_sphere_eps : sphere_eps_world;
         uint32_t nh = w.cell_counts[h];
         if (nh == 0) continue;
         uint32_t hoff = w.cell_offsets[h];
         if (threadIdx.x < 27) {
-            uint32_t cell = stencil_cell(h, threadIdx.x, g);
+            uint32_t cell = stencil_cell(h - cell_base, threadIdx.x, g);
+            if (cell != TGL_NONE) cell += cell_base;
             st_count[threadIdx.x] = cell == TGL_NONE ? 0u : w.cell_counts[cell];
             st_off[threadIdx.x] = cell == TGL_NONE ? 0u : w.cell_offsets[cell];
         }
@@ -370,8 +454,8 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
                         bool hit = false;
                         uint32_t other = 0;
                         if ((uint32_t)lane < n)
-                            hit = build_pair(w, p1x, p1y, p1z, q1x, q1y, q1z, d1x, d1y, d1z, radius, half_length,
-                                             segment, own, slot_of[q[lane]], other);
+                            hit = build_pair(w, g, skin, p1x, p1y, p1z, q1x, q1y, q1z, d1x, d1y, d1z, radius,
+                                             half_length, segment, own, slot_of[q[lane]], other);
                         uint32_t ballot = __ballot_sync(FULL, hit);
                         uint32_t rank = __popc(ballot & ((1u << lane) - 1u));
                         if (hit && count + rank < block) list[count + rank] = other;
@@ -394,6 +478,7 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
 
 // sort_neighbor_lists (neighbor.rs:366-408): ascending segment order for
 // every list that fits its block; overflowed lists are never read.
+template <bool A>
 __global__ void rb_sort_lists_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     extern __shared__ uint32_t list_smem[];
@@ -401,6 +486,7 @@ __global__ void rb_sort_lists_kernel(WorldDev w) {
     const int warps = blockDim.x >> 5;
     uint32_t *buf = list_smem + (size_t)warp * w.block;
     for (uint32_t s = blockIdx.x * warps + warp; s < w.S; s += gridDim.x * warps) {
+        if (A && !rebuilding<A>(w, spec_of_seg<A>(w, s))) continue;
         uint32_t n = w.nbr_count[s];
         if (n < 2 || n > w.block) continue;
         uint32_t *list = w.nbr_list + (size_t)s * w.block;
@@ -416,19 +502,32 @@ __global__ void rb_sort_lists_kernel(WorldDev w) {
 }
 
 // snapshot_neighbor_reference_positions (neighbor.rs:410-422).
+template <bool A>
 __global__ void rb_snapshot_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x)
-        w.ref_pos[v] = w.pos[v];
+        if (!A || rebuilding<A>(w, spec_of_vtx<A>(w, v))) w.ref_pos[v] = w.pos[v];
 }
 
 // finish_neighbor_list_rebuild (neighbor.rs:424-432).
 // New Verlet lists (and slots) also call for new contact lists.
-__global__ void rb_finish_kernel(Control *ctl) {
+__device__ inline void finish_rebuild(Control *ctl) {
     if (ctl->neighbor_state[0] == 0) return;
     ctl->neighbor_state[0] = 0;
     ctl->neighbor_state[1] += 1;
     ctl->contact_state[0] = 1;
+}
+
+template <bool A>
+__global__ void rb_finish_kernel(WorldDev w) {
+    if (!A) {
+        if (threadIdx.x == 0) finish_rebuild(w.ctl);
+        return;
+    }
+    if (w.ctl->neighbor_state[0] == 0) return;
+    for (uint32_t p = threadIdx.x; p < w.P; p += blockDim.x) finish_rebuild(w.ctl + 1 + p);
+    __syncthreads();
+    if (threadIdx.x == 0) w.ctl->neighbor_state[0] = 0;
 }
 
 // ---------------------------------------------------------------- contact pass
@@ -450,8 +549,11 @@ __device__ inline void finish_segment(const WorldDev &w, uint32_t segment, Conta
 // A segment whose list overflowed: the whole warp scans the 27 cells around
 // the home cell of the positions the lists were built from
 // (contact.rs:365-437), 32 candidates at a time, summing hits in scan order.
+template <bool A>
 __device__ ContactAcc overflow_segment(const WorldDev &w, const StepParams &sp, uint32_t segment, int lane) {
-    const Grid &g = w.grid;
+    const uint32_t spec = spec_of_seg<A>(w, segment);
+    const Grid &g = grid_of<A>(w, spec);
+    const uint32_t cell_base = cell_base_of<A>(w, spec);
     const Home h = make_home(w.geom[2 * (size_t)segment], w.geom[2 * (size_t)segment + 1], segment);
     const float4 own = w.seg_static[segment];
     const uint32_t owner = __float_as_uint(own.w);
@@ -462,6 +564,7 @@ __device__ ContactAcc overflow_segment(const WorldDev &w, const StepParams &sp, 
     for (uint32_t n = 0; n < 27; ++n) {
         uint32_t cell = stencil_cell(home, n, g);
         if (cell == TGL_NONE) continue;
+        cell += cell_base;
         const uint32_t count = w.cell_counts[cell];
         const uint32_t start = w.cell_offsets[cell];
         for (uint32_t k0 = 0; k0 < count; k0 += 32) {
@@ -525,6 +628,30 @@ __device__ inline float4 load_keep(const float4 *p, uint64_t policy) {
 
 constexpr int CONTACT_WARPS = 8;
 
+// kernels.rs:129-162 assess_reduced_metrics on one control word: publish the
+// gate metrics, stop or count the iteration, clear the accumulators.
+__device__ inline void assess_reduced_metrics(Control *c, const StepParams &sp, uint32_t overflow) {
+    float maximum_penetration = __uint_as_float(atomicAdd(&c->acc[0], 0u));
+    float maximum_step = __uint_as_float(atomicAdd(&c->acc[1], 0u));
+    float maximum_curvature_ratio = __uint_as_float(atomicAdd(&c->acc[2], 0u));
+    c->metrics[0] = maximum_penetration;
+    c->metrics[1] = maximum_step;
+    c->metrics[2] = maximum_curvature_ratio;
+    if (overflow != 0 ||
+        (sp.force_full_iterations == 0 && maximum_penetration <= sp.penetration_tolerance &&
+         maximum_curvature_ratio <= 1.0f + sp.curvature_ratio_tolerance) ||
+        c->control[2] >= sp.max_iterations) {
+        if (overflow != 0) c->control[3] = 1;
+        c->control[0] = 0;
+    } else {
+        c->control[1] += 1;
+        c->control[2] += 1;
+    }
+    c->acc[0] = 0;
+    c->acc[1] = 0;
+    c->acc[2] = 0;
+}
+
 // Contact pass modes: the Verlet lists as they are (CONTACT_FULL); the
 // Verlet lists plus a refresh of the contact lists and their snapshot
 // (CONTACT_REFRESH, run when the refresh flag is set); the contact lists
@@ -552,8 +679,11 @@ enum { CONTACT_FULL = 0, CONTACT_REFRESH = 1, CONTACT_LISTED = 2 };
 // bit those of the full list. (The minimum image cannot change within the
 // window while every half length stays below contact_half_limit, which the
 // update kernel checks with the displacements.)
-template <int MODE>
-__global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams sp, int gate, float line_eps) {
+// In an arena (A, full lists only) every lane looks up its segment's
+// specimen: grid and line margin for its candidates, whether the specimen is
+// still active, and the specimen whose gate its penetration feeds.
+template <int MODE, bool A = false>
+__global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams sp, int gate, float line_eps_world) {
     __shared__ float4 home_geom[CONTACT_WARPS][64];
     __shared__ uint32_t prefix[CONTACT_WARPS][33];
     __shared__ float4 queue_geom[CONTACT_WARPS][128];  // 64 entries: {p2, r2}, {q2, other}
@@ -561,13 +691,13 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     __shared__ uint32_t segments[CONTACT_WARPS][32];
     __shared__ const uint32_t *sources[CONTACT_WARPS][32];
     __shared__ uint32_t kept_count[CONTACT_WARPS][32];
+    __shared__ uint32_t lane_spec[A ? CONTACT_WARPS : 1][32];
     __shared__ uint32_t warp_max[CONTACT_WARPS];
     __shared__ int is_last;
     if (gate && w.ctl->control[0] == 0) return;
     if (MODE == CONTACT_REFRESH && w.ctl->contact_state[0] == 0) return;
     if (MODE == CONTACT_LISTED && w.ctl->contact_state[0] != 0) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const Grid &g = w.grid;
     const uint32_t block = w.block;
     const uint32_t cblock = w.contact_block;
     const float cskin = w.contact_skin;
@@ -589,10 +719,14 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     for (uint32_t base = (blockIdx.x * CONTACT_WARPS + warp) * 32u; base < w.S; base += warps_total * 32u) {
         // Batches follow the cell list's slot order, so the 32 segments of a
         // batch are spatial neighbors and share most of their candidates.
-        const bool valid = base + lane < w.S;
-        const uint32_t segment = valid ? w.cell_segments[base + lane] : 0u;
+        const bool in_range = base + lane < w.S;
+        const uint32_t segment = in_range ? w.cell_segments[base + lane] : 0u;
+        const uint32_t my_spec = A && in_range ? spec_of_seg<A>(w, segment) : 0u;
+        // Segments of an arena specimen whose gate has stopped it are skipped.
+        const bool valid = in_range && (!A || ctl_of<A>(w, my_spec)->control[0] != 0);
         uint32_t count = valid ? w.nbr_count[segment] : 0u;
         const bool listed = valid && count <= block;
+        if (A) lane_spec[A ? warp : 0][lane] = my_spec;
         uint32_t k = listed ? count : 0u;
         const uint32_t *source = w.nbr_list + (size_t)segment * block;
         if (MODE == CONTACT_LISTED && listed) {
@@ -662,6 +796,9 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
                 int owner = 0;
                 if (f < total) {
                     const Home home = make_home(hg[2 * h], hg[2 * h + 1], seg_of[h]);
+                    const uint32_t hspec = A ? lane_spec[A ? warp : 0][h] : 0u;
+                    const Grid &g = grid_of<A>(w, hspec);
+                    const float line_eps = A ? w.specs[hspec].line_eps : line_eps_world;
                     if (MODE == CONTACT_REFRESH) {
                         // Queue what may come within the contact skin; mark
                         // what passes the pass's own exact tests.
@@ -699,7 +836,7 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
                         hit = contact_solve(home, __float_as_uint(eb.w), ea.w, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z,
                                             sp.correction_fraction, sp.contact_aggregation, pt);
                     if (MODE == CONTACT_REFRESH)
-                        keep = within_contact_skin(home, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z, ea.w, cskin, line_eps);
+                        keep = within_contact_skin(home, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z, ea.w, cskin, line_eps_world);
                 }
                 if (MODE == CONTACT_REFRESH) {
                     // Append the kept entries to their owners' contact lists
@@ -750,15 +887,24 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
             finish_segment(w, segment, acc, sp.contact_aggregation);
             thread_max = max(thread_max, __float_as_uint(fmaxf(acc.maxpen, 0.0f)));
         }
+        if (A && gate && listed && thread_max) {  // each specimen's own maximum
+            atomicMax(&ctl_of<A>(w, my_spec)->acc[0], thread_max);
+            thread_max = 0;
+        }
         if (MODE == CONTACT_REFRESH && valid) w.contact_count[base + lane] = listed ? kept[lane] : 0u;
         uint32_t spill = __ballot_sync(FULL, valid && !listed);
         while (spill) {
             const int j = __ffs(spill) - 1;
             spill &= spill - 1u;
             const uint32_t spilled = __shfl_sync(FULL, segment, j);
-            ContactAcc o = overflow_segment(w, sp, spilled, lane);
+            ContactAcc o = overflow_segment<A>(w, sp, spilled, lane);
             if (lane == 0) finish_segment(w, spilled, o, sp.contact_aggregation);
-            thread_max = max(thread_max, __float_as_uint(fmaxf(o.maxpen, 0.0f)));
+            if (A) {
+                const uint32_t bits = __float_as_uint(fmaxf(o.maxpen, 0.0f));
+                if (gate && lane == 0 && bits) atomicMax(&ctl_of<A>(w, spec_of_seg<A>(w, spilled))->acc[0], bits);
+            } else {
+                thread_max = max(thread_max, __float_as_uint(fmaxf(o.maxpen, 0.0f)));
+            }
         }
         __syncwarp();
     }
@@ -769,40 +915,42 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     if (threadIdx.x == 0) {
         uint32_t m = 0;
         for (int k = 0; k < CONTACT_WARPS; ++k) m = max(m, warp_max[k]);
-        if (m) atomicMax(&w.ctl->acc[0], m);
+        if (!A && m) atomicMax(&w.ctl->acc[0], m);
         __threadfence();
         is_last = atomicAdd(&w.ctl->done_blocks, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (is_last && threadIdx.x == 0) {
-        __threadfence();
-        Control *c = w.ctl;
-        // kernels.rs:129-162 assess_reduced_metrics.
-        float maximum_penetration = __uint_as_float(atomicAdd(&c->acc[0], 0u));
-        float maximum_step = __uint_as_float(atomicAdd(&c->acc[1], 0u));
-        float maximum_curvature_ratio = __uint_as_float(atomicAdd(&c->acc[2], 0u));
-        c->metrics[0] = maximum_penetration;
-        c->metrics[1] = maximum_step;
-        c->metrics[2] = maximum_curvature_ratio;
-        uint32_t overflow = c->cell_overflow;
-        if (overflow != 0 ||
-            (sp.force_full_iterations == 0 && maximum_penetration <= sp.penetration_tolerance &&
-             maximum_curvature_ratio <= 1.0f + sp.curvature_ratio_tolerance) ||
-            c->control[2] >= sp.max_iterations) {
-            if (overflow != 0) c->control[3] = 1;
-            c->control[0] = 0;
-        } else {
-            c->control[1] += 1;
-            c->control[2] += 1;
+    if (!is_last) return;
+    if (!A) {
+        if (threadIdx.x == 0) {
+            __threadfence();
+            Control *c = w.ctl;
+            assess_reduced_metrics(c, sp, c->cell_overflow);
+            c->done_blocks = 0;
+            if (MODE == CONTACT_REFRESH) {
+                c->contact_state[0] = 0;
+                c->contact_state[1] += 1;
+            }
+            __threadfence();
         }
-        c->acc[0] = 0;
-        c->acc[1] = 0;
-        c->acc[2] = 0;
-        c->done_blocks = 0;
-        if (MODE == CONTACT_REFRESH) {
-            c->contact_state[0] = 0;
-            c->contact_state[1] += 1;
-        }
+        return;
+    }
+    // Arena: every still-active specimen's own gate; the world stays active
+    // while any specimen is.
+    __shared__ int any_active;
+    if (threadIdx.x == 0) any_active = 0;
+    __threadfence();
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < w.P; p += blockDim.x) {
+        Control *c = w.ctl + 1 + p;
+        if (c->control[0] == 0) continue;
+        assess_reduced_metrics(c, sp, w.ctl->cell_overflow);
+        if (c->control[0]) any_active = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        w.ctl->control[0] = any_active ? 1u : 0u;
+        w.ctl->done_blocks = 0;
         __threadfence();
     }
 }
@@ -1211,7 +1359,10 @@ __device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float ex
 // warp writes the fibers back with the displacement check
 // (neighbor.rs:446-465) and the next gate's curvature and step maxima
 // (:925-980, :95-127).
-template <int LPF>
+// In an arena (A) each fiber takes its specimen's grid and skin, fibers of
+// stopped specimens are skipped, and the maxima and flags go to each
+// fiber's specimen.
+template <int LPF, bool A = false>
 __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepParams sp, int stride) {
     constexpr int FPW = 32 / LPF;  // fibers per warp
     if (w.ctl->control[0] == 0) return;
@@ -1219,18 +1370,19 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
     const int lane = threadIdx.x;
     const int group = lane / LPF, gl = lane % LPF;
     const uint32_t gmask = LPF == 32 ? FULL : (((1u << LPF) - 1u) << (group * LPF));
-    const Grid &g = w.grid;
-    const float md = 0.5f * w.skin;
     uint32_t smax = 0, cmax = 0;
     bool far = false;
     bool contact_far = false;
-    const bool contact_lists = w.contact_skin > 0.0f;
+    const bool contact_lists = !A && w.contact_skin > 0.0f;
     for (uint32_t batch = blockIdx.x; batch * FPW < w.F; batch += gridDim.x) {
         const uint32_t slot = batch * FPW + group;
-        const uint32_t mine = slot < w.F ? w.fiber_order[slot] : TGL_NONE;
+        uint32_t mine = slot < w.F ? w.fiber_order[slot] : TGL_NONE;
+        if (A && mine != TGL_NONE && ctl_of<A>(w, spec_of_fiber<A>(w, mine))->control[0] == 0) mine = TGL_NONE;
         for (int j = 0; j < FPW; ++j) {
             const uint32_t f = __shfl_sync(FULL, mine, j * LPF);
             if (f == TGL_NONE) continue;
+            const uint32_t fspec = spec_of_fiber<A>(w, f);
+            const Grid &g = grid_of<A>(w, fspec);
             const uint2 span = w.fiber_vspan[f];
             const uint32_t v0 = span.x;
             const int n = (int)span.y;
@@ -1356,9 +1508,15 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                 smax = max(smax, __float_as_uint(fmaxf(step, 0.0f)));
             }
             __syncwarp();
+            if (A) {
+                smax = warp_max_u32(smax);
+                if (lane == 0 && smax) atomicMax(&ctl_of<A>(w, fspec)->acc[1], smax);
+                smax = 0;
+            }
         }
         // Curvature Gauss-Seidel, LPF lanes per fiber, forward then backward.
         if (mine != TGL_NONE) {
+            const Grid &g = grid_of<A>(w, spec_of_fiber<A>(w, mine));
             const uint2 span = w.fiber_vspan[mine];
             const int last = (int)span.y - 3;
             const float extent = w.seg_static[w.fiber_s0[mine]].x;
@@ -1414,6 +1572,8 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
         for (int j = 0; j < FPW; ++j) {
             const uint32_t f = __shfl_sync(FULL, mine, j * LPF);
             if (f == TGL_NONE) continue;
+            const uint32_t fspec = spec_of_fiber<A>(w, f);
+            const float md = 0.5f * skin_of<A>(w, fspec);
             const uint2 span = w.fiber_vspan[f];
             const uint32_t v0 = span.x;
             const int n = (int)span.y;
@@ -1443,9 +1603,20 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                     if (contact_lists && half > w.contact_half_limit) contact_far = true;
                 }
             }
+            if (A) {
+                cmax = warp_max_u32(cmax);
+                const bool fiber_far = __any_sync(FULL, far);
+                if (lane == 0) {
+                    if (cmax) atomicMax(&ctl_of<A>(w, fspec)->acc[2], cmax);
+                    if (fiber_far) flag_rebuild<A>(w, fspec);
+                }
+                cmax = 0;
+                far = false;
+            }
         }
         __syncwarp();
     }
+    if (A) return;
     smax = warp_max_u32(smax);
     cmax = warp_max_u32(cmax);
     const bool any_far = __any_sync(FULL, far);
@@ -1558,52 +1729,86 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     lp.sort_smem = (size_t)sw * w.block * 4;
     cudaFuncSetAttribute(fiber_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(lp.fiber_smem, 1));
     if (lp.fiber_lanes) {
-        cudaFuncSetAttribute(fiber_lanes_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.lanes_smem);
-        cudaFuncSetAttribute(fiber_lanes_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.lanes_smem);
-        cudaFuncSetAttribute(fiber_lanes_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.lanes_smem);
-        cudaFuncSetAttribute(fiber_lanes_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.lanes_smem);
+        const int smem = (int)lp.lanes_smem;
+        cudaFuncSetAttribute(fiber_lanes_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(fiber_lanes_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(fiber_lanes_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(fiber_lanes_kernel<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(fiber_lanes_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(fiber_lanes_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(fiber_lanes_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(fiber_lanes_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     }
-    cudaFuncSetAttribute(rb_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.build_smem);
-    cudaFuncSetAttribute(rb_sort_lists_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(lp.sort_smem, 1));
+    cudaFuncSetAttribute(rb_build_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.build_smem);
+    cudaFuncSetAttribute(rb_build_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.build_smem);
+    cudaFuncSetAttribute(rb_sort_lists_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)std::max<size_t>(lp.sort_smem, 1));
+    cudaFuncSetAttribute(rb_sort_lists_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)std::max<size_t>(lp.sort_smem, 1));
 }
 
-int launch_begin_batch(const WorldDev &w, cudaStream_t st) {
-    begin_batch_kernel<<<1, 1, 0, st>>>(w.ctl);
+int launch_begin_batch(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
+    if (lp.arena)
+        begin_batch_kernel<true><<<1, 256, 0, st>>>(w);
+    else
+        begin_batch_kernel<false><<<1, 32, 0, st>>>(w);
     return 1;
 }
 
-int launch_flag_displacement(const WorldDev &w, cudaStream_t st) {
-    flag_displacement_kernel<<<grid_for(w.V, 256, 1 << 30), 256, 0, st>>>(w);
+int launch_flag_displacement(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
+    if (lp.arena)
+        flag_displacement_kernel<true><<<grid_for(w.V, 256, 1 << 30), 256, 0, st>>>(w);
+    else
+        flag_displacement_kernel<false><<<grid_for(w.V, 256, 1 << 30), 256, 0, st>>>(w);
     return 1;
 }
 
 int launch_measure_start(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
-    measure_start_kernel<<<grid_for(w.F, 8, lp.num_sms * 16), 256, 0, st>>>(w);
+    if (lp.arena)
+        measure_start_kernel<true><<<grid_for(w.F, 8, lp.num_sms * 16), 256, 0, st>>>(w);
+    else
+        measure_start_kernel<false><<<grid_for(w.F, 8, lp.num_sms * 16), 256, 0, st>>>(w);
     return 1;
 }
 
-int launch_request_rebuild(const WorldDev &w, cudaStream_t st) {
-    request_rebuild_kernel<<<1, 1, 0, st>>>(w.ctl);
+int launch_request_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
+    if (lp.arena)
+        request_rebuild_kernel<true><<<1, 256, 0, st>>>(w);
+    else
+        request_rebuild_kernel<false><<<1, 32, 0, st>>>(w);
     return 1;
+}
+
+template <bool A>
+static void enqueue_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
+    const int cap = lp.num_sms * 16;
+    rb_clear_kernel<A><<<grid_for(w.C, 256, cap), 256, 0, st>>>(w);
+    rb_count_kernel<A><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
+    rb_scan_kernel<<<1, 1024, 0, st>>>(w);
+    rb_scatter_kernel<A><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
+    rb_sort_cells_kernel<A><<<grid_for(w.C, 8, cap), 256, 8 * CELL_SORT_CAP * sizeof(uint32_t), st>>>(w);
+    rb_gather_kernel<A><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
+    rb_build_kernel<A><<<(int)std::min<uint64_t>(w.C, (uint64_t)lp.num_sms * 64), 256, lp.build_smem, st>>>(
+        w, lp.build_ch, lp.build_prefilter, lp.build_sphere_eps);
+    rb_sort_lists_kernel<A><<<grid_for(w.S, lp.sort_warps, cap), lp.sort_warps * 32, lp.sort_smem, st>>>(w);
+    rb_snapshot_kernel<A><<<grid_for(w.V, 256, cap), 256, 0, st>>>(w);
+    rb_finish_kernel<A><<<1, A ? 256 : 32, 0, st>>>(w);
 }
 
 int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
-    const int cap = lp.num_sms * 16;
-    rb_clear_kernel<<<grid_for(w.C, 256, cap), 256, 0, st>>>(w);
-    rb_count_kernel<<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
-    rb_scan_kernel<<<1, 1024, 0, st>>>(w);
-    rb_scatter_kernel<<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
-    rb_sort_cells_kernel<<<grid_for(w.C, 8, cap), 256, 8 * CELL_SORT_CAP * sizeof(uint32_t), st>>>(w);
-    rb_gather_kernel<<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
-    rb_build_kernel<<<(int)std::min<uint64_t>(w.C, (uint64_t)lp.num_sms * 64), 256, lp.build_smem, st>>>(
-        w, lp.build_ch, lp.build_prefilter, lp.build_sphere_eps);
-    rb_sort_lists_kernel<<<grid_for(w.S, lp.sort_warps, cap), lp.sort_warps * 32, lp.sort_smem, st>>>(w);
-    rb_snapshot_kernel<<<grid_for(w.V, 256, cap), 256, 0, st>>>(w);
-    rb_finish_kernel<<<1, 1, 0, st>>>(w.ctl);
+    if (lp.arena)
+        enqueue_rebuild<true>(w, lp, st);
+    else
+        enqueue_rebuild<false>(w, lp, st);
     return 10;
 }
 
 int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, bool gate, cudaStream_t st) {
+    if (lp.arena) {
+        contact_kernel<CONTACT_FULL, true><<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, gate ? 1 : 0,
+                                                                                            lp.line_eps);
+        return 1;
+    }
     if (gate && lp.contact_lists) {
         // Listed first: the refresh pass clears the flag the listed pass reads.
         contact_kernel<CONTACT_LISTED><<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, 1, lp.line_eps);
@@ -1614,16 +1819,25 @@ int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp
     return 1;
 }
 
+template <bool A>
+static void enqueue_lanes(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st) {
+    switch (lp.lanes_per_fiber) {
+        case 2: fiber_lanes_kernel<2, A><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+        case 8: fiber_lanes_kernel<8, A><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+        case 32: fiber_lanes_kernel<32, A><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+        default: fiber_lanes_kernel<4, A><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+    }
+}
+
 int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st) {
     if (lp.fiber_lanes) {
-        switch (lp.lanes_per_fiber) {
-            case 2: fiber_lanes_kernel<2><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
-            case 8: fiber_lanes_kernel<8><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
-            case 32: fiber_lanes_kernel<32><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
-            default: fiber_lanes_kernel<4><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
-        }
-    } else
+        if (lp.arena)
+            enqueue_lanes<true>(w, lp, sp, st);
+        else
+            enqueue_lanes<false>(w, lp, sp, st);
+    } else {
         fiber_kernel<<<lp.fiber_blocks, lp.fiber_warps * 32, lp.fiber_smem, st>>>(w, sp);
+    }
     return 1;
 }
 

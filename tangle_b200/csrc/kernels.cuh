@@ -6,6 +6,17 @@
 
 namespace tgl {
 
+// One specimen of an arena: its box, neighbor skin and cell range.
+struct SpecimenDev {
+    Grid grid;
+    float skin;
+    uint32_t cell_base;       // first cell of the specimen in the arena's cell numbering
+    uint32_t build_prefilter; // sphere pre-test on (>= 3 cells on every periodic axis)
+    float build_sphere_eps;
+    float line_eps;
+    uint32_t pad[3];
+};
+
 // Every device pointer and size a kernel needs, passed by value.
 struct WorldDev {
     uint32_t V, S, F, C;
@@ -30,6 +41,8 @@ struct WorldDev {
     const float4 *vtx_static;   // [V] max curvature, rest chord to v-2, rest chord to v+2, wall extent
     const uint32_t *pinned;     // [V]
     const float *rest;          // [S] rest lengths
+    const int4 *links;          // [V] previous vertex, next vertex, segment before, segment after (-1 = none)
+    const float *rest_curvature; // [V] discrete curvature of the intrinsic shape (0 at fiber ends)
     // Resident state.
     float4 *pos;      // [V] xyz, w = 0
     float4 *ref_pos;  // [V] positions the lists were built from
@@ -53,6 +66,16 @@ struct WorldDev {
     float4 *contact_ref;     // [V] positions the contact lists were filtered at
     Control *ctl;
     float *xyz_stage;    // [3V] interleaved staging for host copies
+    // Arena (several specimens relaxed together; the kernels' ARENA
+    // instantiations only): specimen tables, the specimen of every segment,
+    // fiber, vertex and cell, and a control word per specimen at ctl + 1 + p
+    // (ctl[0] then holds the any-specimen flags: active, rebuild pending).
+    uint32_t P;
+    const SpecimenDev *specs;  // [P]
+    const uint32_t *seg_spec;  // [S]
+    const uint32_t *fiber_spec; // [F]
+    const uint32_t *vtx_spec;  // [V]
+    const uint32_t *cell_spec; // [C]
 };
 
 struct StepParams {
@@ -73,6 +96,7 @@ struct StepParams {
 
 // Launch plans, fixed per world.
 struct LaunchPlan {
+    bool arena;             // the kernels' arena instantiations (several specimens)
     int num_sms;
     int contact_group;      // lanes per segment in the contact pass (8, 16 or 32)
     int contact_blocks;
@@ -95,11 +119,11 @@ struct LaunchPlan {
 };
 
 // Each launcher returns the number of kernels it enqueued.
-int launch_begin_batch(const WorldDev &w, cudaStream_t st);
-int launch_flag_displacement(const WorldDev &w, cudaStream_t st);
+int launch_begin_batch(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
+int launch_flag_displacement(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 int launch_measure_start(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
-int launch_request_rebuild(const WorldDev &w, cudaStream_t st);
+int launch_request_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 // With the gate and contact lists on, enqueues the listed pass and the
 // refresh pass, each of which returns at once unless the device-side refresh
 // flag picks it; otherwise the full-list pass.

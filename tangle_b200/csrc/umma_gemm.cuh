@@ -38,6 +38,12 @@ struct GemmArgs {
     // out_bf16[m * ldo_bf16 + n]; with split K, out_f32 + blockIdx.y * m * ldo.
     const float *bias;
     int relu;
+    // Optional: v *= (mask[m * ld_mask + n] > 0) (the ReLU derivative of a
+    // stored activation), then v += residual[m * ld_res + n].
+    const __nv_bfloat16 *mask;
+    int64_t ld_mask;
+    const float *residual;
+    int64_t ld_res;
     float *out_f32;
     int64_t ldo;
     __nv_bfloat16 *out_bf16;
@@ -227,6 +233,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) umma_gemm_kernel(GemmArgs g) 
                     float x = __uint_as_float(r[j]);
                     if (g.bias) x += g.bias[c0 + j];
                     if (g.relu) x = fmaxf(x, 0.0f);
+                    if (g.mask && !(__bfloat162float(g.mask[row * g.ld_mask + c0 + j]) > 0.0f)) x = 0.0f;
+                    if (g.residual) x += g.residual[row * g.ld_res + c0 + j];
                     v[j] = x;
                 }
                 if (out_f32) {

@@ -16,6 +16,7 @@
 
 #include "../../include/tangle_cuda.h"
 #include "kernels.cuh"
+#include "warmstart.cuh"
 
 using namespace tgl;
 
@@ -78,6 +79,29 @@ namespace tgl {
 void set_last_error(const std::string &message) { g_error = message; }
 }  // namespace tgl
 
+// Scratch of the warm-start contact graph (counts, offsets, overlap depths),
+// grown on demand; the graph itself goes to the caller's buffers.
+struct WarmGraph {
+    GraphBuffers b{};
+    int32_t *offsets = nullptr;  // [S + 1]
+    float *depth = nullptr;      // [depth_capacity]
+    int64_t depth_capacity = 0;
+    float *residual = nullptr;   // [2]
+    int64_t edges = 0;
+    float cutoff = 0.0f;
+    bool ready = false, counted = false;
+
+    ~WarmGraph() {
+        cudaFree(b.fwd_count);
+        cudaFree(b.in_count);
+        cudaFree(b.fill);
+        cudaFree(b.block_sums);
+        cudaFree(offsets);
+        cudaFree(depth);
+        cudaFree(residual);
+    }
+};
+
 struct tgl_world {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -90,8 +114,11 @@ struct tgl_world {
     std::map<GraphKey, GraphEntry> graphs;
     uint64_t launches = 0;
     bool timing = false;
+    bool arena = false;
+    uint32_t specimens = 1;
     const GraphEntry *last = nullptr;  // graph of the last batch
     uint64_t last_batch_iterations = 0;
+    WarmGraph warm;
 
     ~tgl_world() {
         for (auto &kv : graphs) destroy_entry(kv.second);
@@ -169,8 +196,8 @@ int validate_config(const tgl_relax_config &c) {
 // has stopped the batch.
 int enqueue_batch(tgl_world *w, const StepParams &sp, uint32_t iterations, std::vector<cudaEvent_t> *events) {
     int kernels = 0;
-    kernels += launch_begin_batch(w->dev, w->stream);
-    kernels += launch_flag_displacement(w->dev, w->stream);
+    kernels += launch_begin_batch(w->dev, w->lp, w->stream);
+    kernels += launch_flag_displacement(w->dev, w->lp, w->stream);
     kernels += launch_measure_start(w->dev, w->lp, w->stream);
     for (uint32_t step = 0; step <= iterations; ++step) {
         if (events) cudaEventRecordWithFlags((*events)[4 * step], w->stream, cudaEventRecordExternal);
@@ -184,10 +211,8 @@ int enqueue_batch(tgl_world *w, const StepParams &sp, uint32_t iterations, std::
     return kernels;
 }
 
-int read_status(tgl_world *w, const tgl_relax_config &c, tgl_batch_status *status) {
-    TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
-    TGL_CUDA(cudaStreamSynchronize(w->stream));
-    const Control &h = *w->host_ctl;
+// world.rs:2337-2369 for one control word.
+void status_of(const Control &h, const tgl_relax_config &c, tgl_batch_status *status) {
     bool overflow = h.cell_overflow != 0 || h.control[3] != 0;
     status->total_iterations = h.control[1];
     status->batch_iterations = h.control[2];
@@ -200,6 +225,32 @@ int read_status(tgl_world *w, const tgl_relax_config &c, tgl_batch_status *statu
                             : 0u;
     status->cell_list_overflow = overflow ? 1u : 0u;
     status->reserved = 0;
+}
+
+// The batch status; for an arena, over all specimens: the largest
+// iteration counts and metrics, converged when every specimen is.
+int read_status(tgl_world *w, const tgl_relax_config &c, tgl_batch_status *status) {
+    const size_t words = w->arena ? (size_t)w->specimens + 1 : 1;
+    TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, words * sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    if (!w->arena) {
+        status_of(*w->host_ctl, c, status);
+        return 0;
+    }
+    tgl_batch_status total{};
+    total.converged = 1;
+    for (uint32_t p = 0; p < w->specimens; ++p) {
+        tgl_batch_status one{};
+        status_of(w->host_ctl[1 + p], c, &one);
+        total.total_iterations = std::max(total.total_iterations, one.total_iterations);
+        total.batch_iterations = std::max(total.batch_iterations, one.batch_iterations);
+        total.max_penetration = std::fmax(total.max_penetration, one.max_penetration);
+        total.max_displacement = std::fmax(total.max_displacement, one.max_displacement);
+        total.max_curvature_ratio = std::fmax(total.max_curvature_ratio, one.max_curvature_ratio);
+        total.converged &= one.converged;
+        total.cell_list_overflow |= one.cell_list_overflow;
+    }
+    *status = total;
     return 0;
 }
 
@@ -209,9 +260,26 @@ extern "C" {
 
 const char *tgl_last_error(void) { return g_error.c_str(); }
 
-int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float max_step, tgl_world **out) {
-    if (!pk || !cl || !out) return set_error(TGL_ERR_INVALID, "null argument");
-    *out = nullptr;
+namespace {
+
+// One specimen prepared on the host: sizing and static data, its indices
+// local to the specimen.
+struct HostSpecimen {
+    uint32_t V = 0, S = 0, F = 0, max_fiber = 0;
+    float cell_size = 0.0f, skin = 0.0f, maximum_radius = 0.0f, maximum_length = 0.0f;
+    Grid grid{};
+    uint64_t C = 0, neighbor_slots = 0;
+    uint32_t block = 0;
+    std::vector<float4> vtx_static, seg_static, geom, pos;
+    std::vector<uint32_t> pinned, seg_v0, fiber_s0;
+    std::vector<uint2> fiber_vspan;
+    std::vector<float> rest, rest_curvature;
+    std::vector<int4> links;
+};
+
+// Upload validation (world.rs:314-319) and the layout the reference's
+// packing produces (packed.rs:200-248).
+int validate_packed(const tgl_packed *pk, const tgl_cell_list_config *cl, float max_step, HostSpecimen &h) {
     const uint32_t V = pk->vertex_count, S = pk->segment_count, F = pk->fiber_count;
     // world.rs:314-319 upload assertions.
     if (S == 0 || F == 0) return set_error(TGL_ERR_INVALID, "assembly has no segments or fibers");
@@ -229,7 +297,8 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
             return set_error(TGL_ERR_INVALID, "cell bounds must be finite with upper > lower");
     // The layout the reference's packing produces (packed.rs:200-248).
     uint64_t vsum = 0, ssum = 0;
-    uint32_t max_fiber = 0;
+    uint32_t &max_fiber = h.max_fiber;
+    max_fiber = 0;
     for (uint32_t f = 0; f < F; ++f) {
         uint32_t v0 = pk->fiber_vertex_spans[2 * f], n = pk->fiber_vertex_spans[2 * f + 1];
         uint32_t s0 = pk->fiber_segment_spans[2 * f], m = pk->fiber_segment_spans[2 * f + 1];
@@ -263,24 +332,15 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
     if ((size_t)max_fiber * 3 * sizeof(float4) > 200 * 1024)
         return set_error(TGL_ERR_UNSUPPORTED, "a fiber has more vertices than one warp can stage in shared memory");
 
-    int device_count = 0;
-    if (cudaGetDeviceCount(&device_count) != cudaSuccess || device_count == 0)
-        return set_error(TGL_ERR_NO_DEVICE, "no CUDA device");
+    return 0;
+}
 
-    tgl_world *w = new tgl_world();
-    auto fail = [&](int rc) {
-        delete w;
-        return rc;
-    };
-    cudaGetDevice(&w->device);
-    cudaDeviceProp prop{};
-    cudaGetDeviceProperties(&prop, w->device);
-    if (prop.major < 10) return fail(set_error(TGL_ERR_NO_DEVICE, "the relaxation kernels are built for sm_100a"));
-    if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess)
-        return fail(set_error(TGL_ERR_CUDA, "cudaStreamCreate failed"));
-    if (cudaMallocHost(&w->host_ctl, sizeof(Control)) != cudaSuccess)
-        return fail(set_error(TGL_ERR_MEMORY, "cudaMallocHost failed"));
-
+// world.rs:321-417 sizing and the static per-segment / per-vertex records.
+int prepare_specimen(const tgl_packed *pk, const tgl_cell_list_config *cl, float max_step, HostSpecimen &h) {
+    const uint32_t V = pk->vertex_count, S = pk->segment_count, F = pk->fiber_count;
+    h.V = V;
+    h.S = S;
+    h.F = F;
     // ---- world.rs:321-417: grid sizing for a uniform layout, in f32.
     const float *P = pk->positions;
     float maximum_rest_length = 0.0f, maximum_initial_length = 0.0f, maximum_radius = 0.0f;
@@ -296,7 +356,7 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
     float interaction_margin = 2.0f * maximum_radius + std::fmax(2.0f * max_step, skin);
     // Every segment is a leaf: one proxy piece and list weight 1 each.
     float piece_length = std::fmin(maximum_length, std::fmax(maximum_length, 2.0f * interaction_margin));
-    w->cell_size = (piece_length + interaction_margin) * cl->cell_size_scale;
+    h.cell_size = (piece_length + interaction_margin) * cl->cell_size_scale;
     Grid grid{};
     uint64_t C = 1;
     for (int a = 0; a < 3; ++a) {
@@ -304,25 +364,29 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
         grid.upper[a] = pk->cell_upper[a];
         grid.periodic[a] = pk->cell_periodic[a] ? 1u : 0u;
         float extent = pk->cell_upper[a] - pk->cell_lower[a];
-        grid.cells[a] = f32_to_u32_host(std::fmax(std::floor(extent / w->cell_size), 1.0f));
+        grid.cells[a] = f32_to_u32_host(std::fmax(std::floor(extent / h.cell_size), 1.0f));
         grid.length[a] = extent;
         grid.width[a] = extent / (float)grid.cells[a];
         grid.inv_length[a] = 1.0f / extent;
         C *= grid.cells[a];
     }
-    if (C > (1ull << 31)) return fail(set_error(TGL_ERR_UNSUPPORTED, "cell grid too large: the cell size is tiny against the box"));
+    if (C > (1ull << 31)) return set_error(TGL_ERR_UNSUPPORTED, "cell grid too large: the cell size is tiny against the box");
     // world.rs:476-509 and :874-917: list room and the byte cap.
     uint64_t max_bytes = cl->max_list_bytes ? cl->max_list_bytes : REFERENCE_MAX_LIST_BYTES;
     uint64_t slots = std::min<uint64_t>((uint64_t)cl->neighbor_capacity * S, max_bytes / 4);
-    w->neighbor_slots = std::max<uint64_t>(slots, 1);
-    uint32_t block = (uint32_t)std::min<uint64_t>(cl->neighbor_capacity, std::min<uint64_t>(w->neighbor_slots / S, 0xFFFFFFFFull));
+    h.neighbor_slots = std::max<uint64_t>(slots, 1);
+    uint32_t block = (uint32_t)std::min<uint64_t>(cl->neighbor_capacity, std::min<uint64_t>(h.neighbor_slots / S, 0xFFFFFFFFull));
 
     // ---- static per-segment and per-vertex data.
     std::vector<float> arc(V, 0.0f);  // packed.rs:561-580
-    std::vector<float4> vtx_static(V);
-    std::vector<uint32_t> pinned(V, 0);
-    std::vector<uint2> fiber_vspan(F);
-    std::vector<uint32_t> fiber_s0(F);
+    std::vector<float4> &vtx_static = h.vtx_static;
+    vtx_static.resize(V);
+    std::vector<uint32_t> &pinned = h.pinned;
+    pinned.assign(V, 0);
+    std::vector<uint2> &fiber_vspan = h.fiber_vspan;
+    fiber_vspan.resize(F);
+    std::vector<uint32_t> &fiber_s0 = h.fiber_s0;
+    fiber_s0.resize(F);
     const float *X = pk->intrinsic_positions;
     for (uint32_t f = 0; f < F; ++f) {
         uint32_t v0 = pk->fiber_vertex_spans[2 * f], n = pk->fiber_vertex_spans[2 * f + 1];
@@ -358,15 +422,13 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
             pinned[v] = pk->vertex_pinned && pk->vertex_pinned[v] ? 1u : 0u;
         }
     }
-    // Fibers by descending vertex count, so a warp's 32 fibers finish together.
-    std::vector<uint32_t> fiber_order(F);
-    for (uint32_t f = 0; f < F; ++f) fiber_order[f] = f;
-    std::stable_sort(fiber_order.begin(), fiber_order.end(),
-                     [&](uint32_t a, uint32_t b) { return fiber_vspan[a].y > fiber_vspan[b].y; });
-    std::vector<float4> seg_static(S);
-    std::vector<uint32_t> seg_v0(S);
-    std::vector<float> rest(pk->segment_rest_lengths, pk->segment_rest_lengths + S);
-    std::vector<float4> geom(2 * (size_t)S);
+    std::vector<float4> &seg_static = h.seg_static;
+    seg_static.resize(S);
+    std::vector<uint32_t> &seg_v0 = h.seg_v0;
+    seg_v0.resize(S);
+    h.rest.assign(pk->segment_rest_lengths, pk->segment_rest_lengths + S);
+    std::vector<float4> &geom = h.geom;
+    geom.resize(2 * (size_t)S);
     for (uint32_t s = 0; s < S; ++s) {
         uint32_t a = pk->segment_vertices[2 * s], b = pk->segment_vertices[2 * s + 1];
         uint32_t fiber = pk->segment_fibers[s];
@@ -378,9 +440,166 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
         geom[2 * (size_t)s] = make_float4(P[3 * a], P[3 * a + 1], P[3 * a + 2], pk->segment_radii[s]);
         geom[2 * (size_t)s + 1] = make_float4(P[3 * b], P[3 * b + 1], P[3 * b + 2], 0.5f * std::sqrt(dx * dx + dy * dy + dz * dz));
     }
-    std::vector<float4> pos(V);
+    std::vector<float4> &pos = h.pos;
+    pos.resize(V);
     for (uint32_t v = 0; v < V; ++v) pos[v] = make_float4(P[3 * v], P[3 * v + 1], P[3 * v + 2], 0.0f);
+    // Fiber links and the rest shape's discrete curvature (warm-start
+    // features; curvature.rs:21-55 form, f64 on the host).
+    std::vector<int4> &links = h.links;
+    links.resize(V);
+    std::vector<float> &rest_curvature = h.rest_curvature;
+    rest_curvature.assign(V, 0.0f);
+    for (uint32_t f = 0; f < F; ++f) {
+        const uint32_t v0 = fiber_vspan[f].x, n = fiber_vspan[f].y, s0 = fiber_s0[f];
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t v = v0 + k;
+            links[v] = make_int4(k > 0 ? (int)(v - 1) : -1, k + 1 < n ? (int)(v + 1) : -1,
+                                 k > 0 ? (int)(s0 + k - 1) : -1, k + 1 < n ? (int)(s0 + k) : -1);
+            if (k > 0 && k + 1 < n) {
+                double u[3], w3[3], lu = 0.0, lw = 0.0, dot = 0.0;
+                for (int a = 0; a < 3; ++a) {
+                    u[a] = (double)X[3 * (size_t)v + a] - (double)X[3 * (size_t)(v - 1) + a];
+                    w3[a] = (double)X[3 * (size_t)(v + 1) + a] - (double)X[3 * (size_t)v + a];
+                    lu += u[a] * u[a];
+                    lw += w3[a] * w3[a];
+                    dot += u[a] * w3[a];
+                }
+                lu = std::sqrt(lu);
+                lw = std::sqrt(lw);
+                if (lu > 0.0 && lw > 0.0) {
+                    double c = std::fmax(-1.0, std::fmin(1.0, dot / (lu * lw)));
+                    rest_curvature[v] = (float)(2.0 * std::sqrt(0.5 * (1.0 - c)) / (0.5 * (lu + lw)));
+                }
+            }
+        }
+    }
 
+    h.skin = skin;
+    h.maximum_radius = maximum_radius;
+    h.maximum_length = maximum_length;
+    h.grid = grid;
+    h.C = C;
+    h.block = block;
+    return 0;
+}
+
+}  // namespace
+
+namespace {
+
+// Device world from prepared specimens: one (a single world) or several (an
+// arena, relaxed together with a gate per specimen).
+int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl, bool arena, tgl_world **out) {
+    int device_count = 0;
+    if (cudaGetDeviceCount(&device_count) != cudaSuccess || device_count == 0)
+        return set_error(TGL_ERR_NO_DEVICE, "no CUDA device");
+
+    tgl_world *w = new tgl_world();
+    auto fail = [&](int rc) {
+        delete w;
+        return rc;
+    };
+    cudaGetDevice(&w->device);
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, w->device);
+    if (prop.major < 10) return fail(set_error(TGL_ERR_NO_DEVICE, "the relaxation kernels are built for sm_100a"));
+    if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(set_error(TGL_ERR_CUDA, "cudaStreamCreate failed"));
+    if (cudaMallocHost(&w->host_ctl, (hosts.size() > 1 || arena ? hosts.size() + 1 : 1) * sizeof(Control)) != cudaSuccess)
+        return fail(set_error(TGL_ERR_MEMORY, "cudaMallocHost failed"));
+
+    // ---- concatenate the specimens (a single world is one specimen).
+    const uint32_t count = (uint32_t)hosts.size();
+    uint64_t V64 = 0, S64 = 0, F64 = 0, C64 = 0;
+    uint32_t max_fiber = 0;
+    for (const HostSpecimen &h : hosts) {
+        V64 += h.V;
+        S64 += h.S;
+        F64 += h.F;
+        C64 += h.C;
+        max_fiber = std::max(max_fiber, h.max_fiber);
+    }
+    if (V64 >= 0xFFFFFFFFull || S64 >= 0xFFFFFFFFull || C64 > (1ull << 31))
+        return fail(set_error(TGL_ERR_UNSUPPORTED, "arena too large for 32-bit indices"));
+    const uint32_t V = (uint32_t)V64, S = (uint32_t)S64, F = (uint32_t)F64;
+    const uint64_t C = C64;
+    std::vector<float4> vtx_static, seg_static, geom, pos;
+    std::vector<uint32_t> pinned, seg_v0, fiber_s0, seg_spec, fiber_spec, vtx_spec, cell_spec;
+    std::vector<uint2> fiber_vspan;
+    std::vector<float> rest, rest_curvature;
+    std::vector<int4> links;
+    std::vector<SpecimenDev> specs(count);
+    vtx_static.reserve(V);
+    uint32_t vbase = 0, sbase = 0, fbase = 0, cbase = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const HostSpecimen &h = hosts[i];
+        for (uint32_t v = 0; v < h.V; ++v) {
+            vtx_static.push_back(h.vtx_static[v]);
+            pinned.push_back(h.pinned[v]);
+            pos.push_back(h.pos[v]);
+            rest_curvature.push_back(h.rest_curvature[v]);
+            int4 l = h.links[v];
+            links.push_back(make_int4(l.x >= 0 ? l.x + (int)vbase : -1, l.y >= 0 ? l.y + (int)vbase : -1,
+                                      l.z >= 0 ? l.z + (int)sbase : -1, l.w >= 0 ? l.w + (int)sbase : -1));
+            vtx_spec.push_back(i);
+        }
+        for (uint32_t s = 0; s < h.S; ++s) {
+            float4 st = h.seg_static[s];
+            uint32_t fiber;
+            std::memcpy(&fiber, &st.w, 4);
+            fiber += fbase;
+            std::memcpy(&st.w, &fiber, 4);
+            seg_static.push_back(st);
+            seg_v0.push_back(h.seg_v0[s] + vbase);
+            rest.push_back(h.rest[s]);
+            geom.push_back(h.geom[2 * (size_t)s]);
+            geom.push_back(h.geom[2 * (size_t)s + 1]);
+            seg_spec.push_back(i);
+        }
+        for (uint32_t f = 0; f < h.F; ++f) {
+            fiber_vspan.push_back(make_uint2(h.fiber_vspan[f].x + vbase, h.fiber_vspan[f].y));
+            fiber_s0.push_back(h.fiber_s0[f] + sbase);
+            fiber_spec.push_back(i);
+        }
+        for (uint64_t c = 0; c < h.C; ++c) cell_spec.push_back(i);
+        SpecimenDev &sd = specs[i];
+        sd.grid = h.grid;
+        sd.skin = h.skin;
+        sd.cell_base = cbase;
+        float edge = 0.0f;
+        sd.build_prefilter = 1;
+        for (int a = 0; a < 3; ++a) {
+            if (h.grid.periodic[a] && h.grid.cells[a] < 3) sd.build_prefilter = 0;
+            edge = std::max(edge, h.grid.length[a]);
+        }
+        sd.build_sphere_eps = 1.0e-6f * edge;
+        sd.line_eps = 4.0e-6f * edge;
+        vbase += h.V;
+        sbase += h.S;
+        fbase += h.F;
+        cbase += (uint32_t)h.C;
+    }
+    // Fibers by descending vertex count, so a warp's fibers finish together.
+    std::vector<uint32_t> fiber_order(F);
+    for (uint32_t f = 0; f < F; ++f) fiber_order[f] = f;
+    std::stable_sort(fiber_order.begin(), fiber_order.end(),
+                     [&](uint32_t a, uint32_t b) { return fiber_vspan[a].y > fiber_vspan[b].y; });
+    const HostSpecimen &h0 = hosts[0];
+    w->cell_size = h0.cell_size;
+    w->neighbor_slots = h0.neighbor_slots;
+    uint32_t block = h0.block;
+    if (arena) {
+        // One list block for every specimen: the capacity, within the byte
+        // cap (8 GiB unless one is given).
+        uint64_t max_bytes = cl->max_list_bytes ? cl->max_list_bytes : (8ull << 30);
+        uint64_t slots = std::min<uint64_t>((uint64_t)cl->neighbor_capacity * S, max_bytes / 4);
+        w->neighbor_slots = std::max<uint64_t>(slots, 1);
+        block = (uint32_t)std::min<uint64_t>(cl->neighbor_capacity, std::max<uint64_t>(w->neighbor_slots / S, 1));
+    }
+    const float skin = h0.skin;
+    const float maximum_radius = h0.maximum_radius;
+    const float maximum_length = h0.maximum_length;
+    const Grid grid = h0.grid;
     WorldDev &d = w->dev;
     d.V = V;
     d.S = S;
@@ -398,6 +617,7 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
     // H = (L/2 - 2 r_max - contact_skin) / 2, less 0.1 %.
     float contact_fraction = 0.1f;
     if (const char *env = std::getenv("TGL_CONTACT_SKIN")) contact_fraction = std::strtof(env, nullptr);
+    if (arena) contact_fraction = 0.0f;  // the arena's contact pass reads the Verlet lists
     if (!(contact_fraction > 0.0f && contact_fraction <= 1.0f) || !(skin > 0.0f)) contact_fraction = 0.0f;
     d.contact_skin = contact_fraction * skin;
     d.contact_half_limit = INFINITY;
@@ -412,7 +632,12 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
     float4 *seg_static_d, *vtx_static_d;
     uint32_t *seg_v0_d, *fiber_s0_d, *pinned_d, *fiber_order_d;
     uint2 *fiber_vspan_d;
-    float *rest_d;
+    float *rest_d, *rest_curvature_d;
+    int4 *links_d;
+    if ((rc = w->upload(&links_d, links)) || (rc = w->upload(&rest_curvature_d, rest_curvature)))
+        return fail(rc);
+    d.links = links_d;
+    d.rest_curvature = rest_curvature_d;
     if ((rc = w->upload(&seg_static_d, seg_static)) || (rc = w->upload(&seg_v0_d, seg_v0)) ||
         (rc = w->upload(&fiber_vspan_d, fiber_vspan)) || (rc = w->upload(&fiber_s0_d, fiber_s0)) ||
         (rc = w->upload(&fiber_order_d, fiber_order)) ||
@@ -423,7 +648,8 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
         (rc = w->alloc(&d.cell_offsets, C)) || (rc = w->alloc(&d.cell_segments, S)) ||
         (rc = w->alloc(&d.cell_of, S)) || (rc = w->alloc(&d.ticket, S)) ||
         (rc = w->alloc(&d.slot_geom, 2 * (size_t)S)) || (rc = w->alloc(&d.slot_sphere, S)) || (rc = w->alloc(&d.nbr_count, S)) ||
-        (rc = w->alloc(&d.nbr_list, std::max<uint64_t>((uint64_t)S * block, 1))) || (rc = w->alloc(&d.ctl, 1)) ||
+        (rc = w->alloc(&d.nbr_list, std::max<uint64_t>((uint64_t)S * block, 1))) ||
+        (rc = w->alloc(&d.ctl, arena ? (size_t)count + 1 : 1)) ||
         (rc = w->alloc(&d.xyz_stage, 3 * (size_t)V)))
         return fail(rc);
     if (d.contact_block &&
@@ -438,13 +664,30 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
     d.vtx_static = vtx_static_d;
     d.pinned = pinned_d;
     d.rest = rest_d;
+    d.P = count;
+    w->arena = arena;
+    w->specimens = count;
+    if (arena) {
+        SpecimenDev *specs_d;
+        uint32_t *seg_spec_d, *fiber_spec_d, *vtx_spec_d, *cell_spec_d;
+        if ((rc = w->upload(&specs_d, specs)) || (rc = w->upload(&seg_spec_d, seg_spec)) ||
+            (rc = w->upload(&fiber_spec_d, fiber_spec)) || (rc = w->upload(&vtx_spec_d, vtx_spec)) ||
+            (rc = w->upload(&cell_spec_d, cell_spec)))
+            return fail(rc);
+        d.specs = specs_d;
+        d.seg_spec = seg_spec_d;
+        d.fiber_spec = fiber_spec_d;
+        d.vtx_spec = vtx_spec_d;
+        d.cell_spec = cell_spec_d;
+    }
     Control ctl{};
     ctl.metrics[0] = INFINITY;  // world.rs:470
     ctl.metrics[1] = 0.0f;
     ctl.metrics[2] = INFINITY;
     ctl.neighbor_state[0] = 1;  // lists start stale (world.rs:516-517)
     ctl.contact_state[0] = 1;
-    if (cudaMemcpy(d.ctl, &ctl, sizeof(Control), cudaMemcpyHostToDevice) != cudaSuccess ||
+    std::vector<Control> controls(arena ? count + 1 : 1, ctl);
+    if (cudaMemcpy(d.ctl, controls.data(), controls.size() * sizeof(Control), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(d.corr, 0, 2 * (size_t)S * sizeof(float4)) != cudaSuccess ||
         cudaMemset(d.vertex_step, 0, V * sizeof(float)) != cudaSuccess ||
         cudaMemset(d.cell_counts, 0, C * sizeof(uint32_t)) != cudaSuccess ||
@@ -457,15 +700,54 @@ int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float
         if (cudaMemcpy(d.cell_segments, iota.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess)
             return fail(set_error(TGL_ERR_CUDA, "device initialisation failed"));
     }
+    w->lp.arena = arena;
     plan_launches(d, w->lp);
+    if (arena && !w->lp.fiber_lanes)
+        return fail(set_error(TGL_ERR_UNSUPPORTED, "an arena needs fibers of at most 256 vertices"));
     *out = w;
     return 0;
 }
 
+}  // namespace
+
+int tgl_world_create(const tgl_packed *pk, const tgl_cell_list_config *cl, float max_step, tgl_world **out) {
+    if (!pk || !cl || !out) return set_error(TGL_ERR_INVALID, "null argument");
+    *out = nullptr;
+    std::vector<HostSpecimen> hosts(1);
+    if (int rc = validate_packed(pk, cl, max_step, hosts[0])) return rc;
+    if (int rc = prepare_specimen(pk, cl, max_step, hosts[0])) return rc;
+    return build_world(hosts, cl, false, out);
+}
+
+int tgl_arena_create(const tgl_packed *specimens, uint32_t count, const tgl_cell_list_config *cl, float max_step,
+                     tgl_world **out) {
+    if (!specimens || !cl || !out || count == 0) return set_error(TGL_ERR_INVALID, "null argument or no specimens");
+    *out = nullptr;
+    std::vector<HostSpecimen> hosts(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        int rc = validate_packed(&specimens[i], cl, max_step, hosts[i]);
+        if (!rc) rc = prepare_specimen(&specimens[i], cl, max_step, hosts[i]);
+        if (rc) return set_error(rc, "specimen " + std::to_string(i) + ": " + g_error);
+    }
+    return build_world(hosts, cl, true, out);
+}
+
 void tgl_world_destroy(tgl_world *w) { delete w; }
+
+int tgl_arena_status(tgl_world *w, const tgl_relax_config *config, tgl_batch_status *statuses, uint32_t count) {
+    if (!w || !config || !statuses) return set_error(TGL_ERR_INVALID, "null argument");
+    if (!w->arena) return set_error(TGL_ERR_INVALID, "not an arena");
+    if (count != w->specimens) return set_error(TGL_ERR_INVALID, "status array length differs from the specimen count");
+    TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, (count + 1) * sizeof(Control), cudaMemcpyDeviceToHost,
+                             w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    for (uint32_t p = 0; p < count; ++p) status_of(w->host_ctl[1 + p], *config, &statuses[p]);
+    return 0;
+}
 
 int tgl_world_checkpoint(tgl_world *w, float *xyz, size_t len, uint64_t *total_iterations) {
     if (!w || !xyz || !total_iterations) return set_error(TGL_ERR_INVALID, "null argument");
+    if (w->arena) return set_error(TGL_ERR_UNSUPPORTED, "checkpoints are per specimen; an arena has several");
     if (int rc = tgl_download_positions(w, xyz, len)) return rc;
     TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
     TGL_CUDA(cudaStreamSynchronize(w->stream));
@@ -494,6 +776,7 @@ int tgl_world_restore(const tgl_packed *pk, const tgl_cell_list_config *cl, floa
 
 int tgl_run_batch(tgl_world *w, const tgl_relax_config *config, uint32_t iterations, tgl_batch_status *status) {
     if (!w || !config || !status) return set_error(TGL_ERR_INVALID, "null argument");
+    w->warm.counted = false;
     if (iterations == 0) return set_error(TGL_ERR_INVALID, "iterations must be positive");  // world.rs:1021
     if (int rc = validate_config(*config)) return rc;
     StepParams sp = step_params(*config, iterations);
@@ -583,6 +866,7 @@ int tgl_download_positions(tgl_world *w, float *xyz, size_t len) {
 
 int tgl_upload_positions(tgl_world *w, const float *xyz, size_t len) {
     if (!w || !xyz) return set_error(TGL_ERR_INVALID, "null argument");
+    w->warm.counted = false;
     if (len != 3 * (size_t)w->dev.V) return set_error(TGL_ERR_INVALID, "position buffer has the wrong length");
     for (size_t i = 0; i < len; ++i)
         if (!std::isfinite(xyz[i])) return set_error(TGL_ERR_INVALID, "positions must be finite");
@@ -605,7 +889,16 @@ int tgl_neighbor_list_rebuilds(tgl_world *w, uint32_t *rebuilds) {
     if (!w || !rebuilds) return set_error(TGL_ERR_INVALID, "null argument");
     TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
     TGL_CUDA(cudaStreamSynchronize(w->stream));
-    *rebuilds = w->host_ctl->neighbor_state[1];
+    if (!w->arena) {
+        *rebuilds = w->host_ctl->neighbor_state[1];
+        return 0;
+    }
+    TGL_CUDA(cudaMemcpyAsync(w->host_ctl, w->dev.ctl, (w->specimens + 1) * sizeof(Control), cudaMemcpyDeviceToHost,
+                             w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    uint32_t total = 0;  // an arena: the specimens' rebuilds together
+    for (uint32_t p = 0; p < w->specimens; ++p) total += w->host_ctl[1 + p].neighbor_state[1];
+    *rebuilds = total;
     return 0;
 }
 
@@ -629,9 +922,127 @@ int tgl_debug_contact_lists(tgl_world *w, uint32_t *counts, uint32_t *lists) {
     return 0;
 }
 
+int tgl_warmstart_graph_count(tgl_world *w, float cutoff, int64_t *edge_count) {
+    if (!w || !edge_count) return set_error(TGL_ERR_INVALID, "null argument");
+    if (w->arena) return set_error(TGL_ERR_UNSUPPORTED, "the warm start takes one specimen");
+    if (!(cutoff >= 0.0f) || !std::isfinite(cutoff)) return set_error(TGL_ERR_INVALID, "cutoff must be finite and >= 0");
+    const WorldDev &d = w->dev;
+    GraphBuffers &b = w->warm.b;
+    if (!w->warm.ready) {
+        const size_t S = d.S;
+        if (cudaMalloc(&b.fwd_count, S * 4) != cudaSuccess || cudaMalloc(&b.in_count, S * 4) != cudaSuccess ||
+            cudaMalloc(&b.fill, S * 4) != cudaSuccess || cudaMalloc(&w->warm.offsets, (S + 1) * 4) != cudaSuccess ||
+            cudaMalloc(&b.block_sums, (S / 1024 + 2) * 4) != cudaSuccess)
+            return set_error(TGL_ERR_MEMORY, "warm-start graph allocation failed");
+        w->warm.ready = true;
+    }
+    b.offsets = w->warm.offsets;
+    // Lists from the current positions, then counts and offsets.
+    w->launches += launch_request_rebuild(d, w->lp, w->stream);
+    w->launches += launch_rebuild(d, w->lp, w->stream);
+    launch_graph_count(d, b, cutoff, w->stream);
+    w->launches += 1 + launch_graph_offsets(d, b, w->stream);
+    int32_t edges = 0;
+    TGL_CUDA(cudaMemcpyAsync(&edges, b.offsets + d.S, sizeof(int32_t), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    TGL_CUDA(cudaGetLastError());
+    if (edges < 0) return set_error(TGL_ERR_UNSUPPORTED, "contact graph too large for 32-bit edge indices");
+    if (edges > w->warm.depth_capacity) {
+        cudaFree(w->warm.depth);
+        w->warm.depth = nullptr;
+        w->warm.depth_capacity = 0;
+        const size_t cap = (size_t)edges + edges / 4 + 1024;
+        if (cudaMalloc(&w->warm.depth, cap * sizeof(float)) != cudaSuccess)
+            return set_error(TGL_ERR_MEMORY, "warm-start edge allocation failed");
+        w->warm.depth_capacity = (int64_t)cap;
+    }
+    w->warm.edges = edges;
+    w->warm.cutoff = cutoff;
+    w->warm.counted = true;
+    *edge_count = edges;
+    return 0;
+}
+
+int tgl_warmstart_graph_fill(tgl_world *w, const tgl_mp_graph_out *out) {
+    if (!w || !out || !out->seg_v0 || !out->links || !out->offsets || !out->node_features)
+        return set_error(TGL_ERR_INVALID, "null argument");
+    if (!w->warm.counted) return set_error(TGL_ERR_INVALID, "tgl_warmstart_graph_count must come first");
+    const int64_t E = w->warm.edges;
+    if (E > 0 && (!out->dst || !out->src || !out->twin || !out->s || !out->t || !out->edge_features))
+        return set_error(TGL_ERR_INVALID, "null edge buffer");
+    w->warm.counted = false;
+    const WorldDev &d = w->dev;
+    GraphBuffers b = w->warm.b;
+    b.offsets = w->warm.offsets;
+    b.dst = out->dst;
+    b.src = out->src;
+    b.twin = out->twin;
+    b.s = out->s;
+    b.t = out->t;
+    b.depth = w->warm.depth;
+    b.edge_features = static_cast<__nv_bfloat16 *>(out->edge_features);
+    b.node_features = static_cast<__nv_bfloat16 *>(out->node_features);
+    launch_graph_fill(d, b, w->warm.cutoff, w->stream);
+    MpGraph g{};
+    g.V = (int32_t)d.V;
+    g.S = (int32_t)d.S;
+    g.E = (int32_t)E;
+    g.seg_v0 = reinterpret_cast<const int32_t *>(d.seg_v0);
+    g.links = d.links;
+    g.offsets = b.offsets;
+    g.dst = b.dst;
+    g.src = b.src;
+    g.twin = b.twin;
+    g.s = b.s;
+    g.t = b.t;
+    launch_node_features(d, b, g, w->stream);
+    w->launches += 4;
+    TGL_CUDA(cudaMemcpyAsync(out->seg_v0, d.seg_v0, (size_t)d.S * 4, cudaMemcpyDeviceToDevice, w->stream));
+    TGL_CUDA(cudaMemcpyAsync(out->links, d.links, (size_t)d.V * 16, cudaMemcpyDeviceToDevice, w->stream));
+    TGL_CUDA(cudaMemcpyAsync(out->offsets, b.offsets, ((size_t)d.S + 1) * 4, cudaMemcpyDeviceToDevice, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    TGL_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int tgl_world_displace(tgl_world *w, const float *dx, int64_t ld, float scale, int32_t in_diameters, float max_step) {
+    if (!w || !dx) return set_error(TGL_ERR_INVALID, "null argument");
+    w->warm.counted = false;
+    if (ld < 3 || !std::isfinite(scale) || !(max_step > 0.0f)) return set_error(TGL_ERR_INVALID, "bad displacement arguments");
+    launch_displace(w->dev, dx, ld, scale, in_diameters, max_step, w->stream);
+    w->launches += 2;
+    TGL_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int tgl_world_residual(tgl_world *w, const tgl_relax_config *config, float *max_penetration,
+                       float *max_curvature_ratio, float *total_penetration) {
+    if (!w || !config || !max_penetration || !max_curvature_ratio || !total_penetration)
+        return set_error(TGL_ERR_INVALID, "null argument");
+    if (w->arena) return set_error(TGL_ERR_UNSUPPORTED, "the residual is per specimen; use tgl_arena_status");
+    if (int rc = validate_config(*config)) return rc;
+    if (!w->warm.residual && cudaMalloc(&w->warm.residual, (3 + RESIDUAL_BLOCKS) * sizeof(float)) != cudaSuccess)
+        return set_error(TGL_ERR_MEMORY, "cudaMalloc failed");
+    StepParams sp = step_params(*config, 1);
+    w->launches += launch_flag_displacement(w->dev, w->lp, w->stream);
+    w->launches += launch_rebuild(w->dev, w->lp, w->stream);
+    w->launches += launch_contact(w->dev, w->lp, sp, false, w->stream);
+    launch_residual(w->dev, w->warm.residual, w->stream);
+    w->launches += 1;
+    float out[3];
+    TGL_CUDA(cudaMemcpyAsync(out, w->warm.residual, sizeof(out), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    TGL_CUDA(cudaGetLastError());
+    *max_penetration = out[0];
+    *max_curvature_ratio = out[1];
+    *total_penetration = out[2];
+    return 0;
+}
+
 int tgl_debug_rebuild(tgl_world *w) {
     if (!w) return set_error(TGL_ERR_INVALID, "null argument");
-    w->launches += launch_request_rebuild(w->dev, w->stream);
+    w->warm.counted = false;
+    w->launches += launch_request_rebuild(w->dev, w->lp, w->stream);
     w->launches += launch_rebuild(w->dev, w->lp, w->stream);
     TGL_CUDA(cudaStreamSynchronize(w->stream));
     TGL_CUDA(cudaGetLastError());

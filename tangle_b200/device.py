@@ -14,7 +14,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from typing import Optional
+from typing import List, Optional
 
 import numpy as np
 
@@ -29,12 +29,16 @@ TGL_ERR_UNSUPPORTED = 5
 
 #: Every symbol include/tangle_cuda.h declares.
 EXPORTS = (
-    "tgl_world_create", "tgl_world_destroy", "tgl_world_checkpoint", "tgl_world_restore", "tgl_run_batch", "tgl_download_positions", "tgl_upload_positions",
+    "tgl_world_create", "tgl_world_destroy", "tgl_world_checkpoint", "tgl_world_restore", "tgl_run_batch",
+    "tgl_arena_create", "tgl_arena_status", "tgl_download_positions", "tgl_upload_positions",
     "tgl_cell_size", "tgl_cell_count", "tgl_cell_dims", "tgl_neighbor_skin", "tgl_neighbor_block",
     "tgl_neighbor_list_rebuilds", "tgl_debug_rebuild", "tgl_debug_cell_list", "tgl_debug_neighbor_lists",
     "tgl_debug_corrections", "tgl_kernel_launches", "tgl_set_kernel_timing", "tgl_last_kernel_times",
     "tgl_world_stream", "tgl_contact_pass_noalloc", "tgl_contact_list_info", "tgl_debug_contact_lists",
-    "tgl_gemm_bf16",
+    "tgl_gemm_bf16", "tgl_warmstart_graph_count", "tgl_warmstart_graph_fill", "tgl_world_displace",
+    "tgl_world_residual", "tgl_mp_edge_inputs", "tgl_mp_node_inputs", "tgl_mp_node_inputs_backward",
+    "tgl_mp_edge_inputs_backward", "tgl_column_sums_scratch", "tgl_column_sums", "tgl_adam_step", "tgl_mse",
+    "tgl_convert_bf16",
     "tgl_last_error",
 )
 
@@ -141,6 +145,11 @@ def load_library():
     lib.tgl_world_create.restype = ctypes.c_int
     lib.tgl_world_destroy.argtypes = [P]
     lib.tgl_world_destroy.restype = None
+    lib.tgl_arena_create.argtypes = [ctypes.POINTER(Packed), ctypes.c_uint32, ctypes.POINTER(CellList), ctypes.c_float,
+                                     ctypes.POINTER(ctypes.c_void_p)]
+    lib.tgl_arena_create.restype = ctypes.c_int
+    lib.tgl_arena_status.argtypes = [P, ctypes.POINTER(Config), ctypes.POINTER(Status), ctypes.c_uint32]
+    lib.tgl_arena_status.restype = ctypes.c_int
     lib.tgl_world_checkpoint.argtypes = [P, P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]
     lib.tgl_world_checkpoint.restype = ctypes.c_int
     lib.tgl_world_restore.argtypes = [ctypes.POINTER(Packed), ctypes.POINTER(CellList), ctypes.c_float,
@@ -275,6 +284,45 @@ class DeviceWorld:
     def upload(cls, config: RelaxationConfig, packed) -> "DeviceWorld":
         """DeviceWorld::upload(config, packed) (plugin.rs:422-424)."""
         return cls(packed, config.cell_list, config.max_step)
+
+    @classmethod
+    def arena(cls, packeds, cell_list: Optional[CellListConfig] = None, max_step: float = 0.006) -> "DeviceWorld":
+        """tgl_arena_create: several specimens relaxed together, each with its
+        own grid, lists and gate; positions are concatenated in order."""
+        lib = load_library()
+        cell_list = cell_list or CellListConfig()
+        keep: list = []
+        structs = (Packed * len(packeds))(*[packed_struct(p, keep) for p in packeds])
+        cl = cell_list_struct(cell_list)
+        handle = ctypes.c_void_p()
+        rc = lib.tgl_arena_create(structs, len(packeds), ctypes.byref(cl), ctypes.c_float(max_step),
+                                  ctypes.byref(handle))
+        if rc:
+            _raise(lib, rc)
+        world = cls.__new__(cls)
+        world._lib = lib
+        world._handle = handle
+        world._packed = None
+        world.vertex_count = sum(p.vertex_count for p in packeds)
+        world.segment_count = sum(p.segment_count for p in packeds)
+        world.specimen_vertices = [p.vertex_count for p in packeds]
+        return world
+
+    def specimen_statuses(self, config: RelaxationConfig) -> List[BatchStatus]:
+        """tgl_arena_status: each specimen's status after the last batch."""
+        n = len(self.specimen_vertices)
+        out = (Status * n)()
+        self._check(self._lib.tgl_arena_status(self._handle, ctypes.byref(config_struct(config)), out, n))
+        return [BatchStatus(total_iterations=int(st.total_iterations), batch_iterations=int(st.batch_iterations),
+                            max_penetration=float(st.max_penetration), max_displacement=float(st.max_displacement),
+                            max_curvature_ratio=float(st.max_curvature_ratio), converged=bool(st.converged),
+                            cell_list_overflow=bool(st.cell_list_overflow)) for st in out]
+
+    def specimen_positions(self) -> List[np.ndarray]:
+        """The arena's positions split per specimen (interleaved xyz each)."""
+        xyz = self.download_positions()
+        bounds = np.cumsum([0] + [3 * v for v in self.specimen_vertices])
+        return [xyz[a:b] for a, b in zip(bounds[:-1], bounds[1:])]
 
     @classmethod
     def restore(cls, config: RelaxationConfig, checkpoint) -> "DeviceWorld":

@@ -18,7 +18,8 @@ class Gemm(ctypes.Structure):
         ("a", ctypes.c_void_p), ("b", ctypes.c_void_p), ("lda", ctypes.c_int64), ("ldb", ctypes.c_int64),
         ("m", ctypes.c_int32), ("n", ctypes.c_int32), ("k", ctypes.c_int64), ("a_mn", ctypes.c_int32),
         ("b_mn", ctypes.c_int32), ("k_split", ctypes.c_int64), ("bias", ctypes.c_void_p),
-        ("relu", ctypes.c_int32), ("reserved", ctypes.c_int32), ("out_f32", ctypes.c_void_p),
+        ("relu", ctypes.c_int32), ("reserved", ctypes.c_int32), ("mask", ctypes.c_void_p),
+        ("ld_mask", ctypes.c_int64), ("residual", ctypes.c_void_p), ("ld_res", ctypes.c_int64), ("out_f32", ctypes.c_void_p),
         ("ldo", ctypes.c_int64), ("out_bf16", ctypes.c_void_p), ("ldo_bf16", ctypes.c_int64),
         ("error", ctypes.c_void_p),
     ]
@@ -31,7 +32,7 @@ def run(lib, torch, a, b, m, n, k, a_mn, b_mn, bias=None, relu=False, k_split=0,
     out_bf16 = torch.empty((m, n), dtype=torch.bfloat16, device=dev) if want_bf16 else None
     err = torch.zeros(1, dtype=torch.int32, device=dev)
     g = Gemm(a.data_ptr(), b.data_ptr(), a.shape[1], b.shape[1], m, n, k, a_mn, b_mn, k_split,
-             bias.data_ptr() if bias is not None else None, int(relu), 0, out.data_ptr(), n,
+             bias.data_ptr() if bias is not None else None, int(relu), 0, None, 0, None, 0, out.data_ptr(), n,
              out_bf16.data_ptr() if want_bf16 else None, n, err.data_ptr())
     fn = lib.tgl_gemm_bf16
     fn.argtypes = [ctypes.POINTER(Gemm), ctypes.c_void_p]
@@ -106,8 +107,30 @@ def test_rejects_bad_shapes(cuda_lib):
 
     a = torch.zeros(16, 16, device="cuda", dtype=torch.bfloat16)
     out = torch.zeros(16, 24, device="cuda")
-    g = Gemm(a.data_ptr(), a.data_ptr(), 16, 16, 16, 24, 16, 0, 0, 0, None, 0, 0, out.data_ptr(), 24, None, 0, None)
+    g = Gemm(a.data_ptr(), a.data_ptr(), 16, 16, 16, 24, 16, 0, 0, 0, None, 0, 0, None, 0, None, 0, out.data_ptr(), 24,
+             None, 0, None)
     fn = cuda_lib.tgl_gemm_bf16
     fn.argtypes = [ctypes.POINTER(Gemm), ctypes.c_void_p]
     fn.restype = ctypes.c_int
     assert fn(ctypes.byref(g), None) == 1  # n = 24 is not a multiple of 16
+
+
+def test_mask_and_residual_epilogue(cuda_lib):
+    import torch
+
+    m, n, k = 300, 64, 64
+    a = torch.randn(m, k, device="cuda").to(torch.bfloat16)
+    b = torch.randn(n, k, device="cuda").to(torch.bfloat16)
+    mask = torch.randn(m, n, device="cuda").to(torch.bfloat16)
+    res = torch.randn(m, n, device="cuda")
+    out = torch.full((m, n), float("nan"), device="cuda")
+    g = Gemm(a.data_ptr(), b.data_ptr(), k, k, m, n, k, 0, 0, 0, None, 0, 0, mask.data_ptr(), n, res.data_ptr(), n,
+             out.data_ptr(), n, None, 0, None)
+    fn = cuda_lib.tgl_gemm_bf16
+    fn.argtypes = [ctypes.POINTER(Gemm), ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    assert fn(ctypes.byref(g), torch.cuda.current_stream().cuda_stream) == 0
+    torch.cuda.synchronize()
+    ref = (a.float() @ b.float().T) * (mask.float() > 0) + res
+    scale = (a.float().abs() @ b.float().abs().T) + res.abs()
+    assert bool(((out - ref).abs() <= 1.0e-5 * scale + 1e-30).all())
