@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
-    ap.add_argument("--workload", choices=["mid_size", "cpu_runnable"], default="mid_size")
+    ap.add_argument("--workload", choices=["mid_size", "cpu_runnable", "batched"], default="mid_size")
+    ap.add_argument("--specimens", type=int, default=512, help="specimens of the batched workload")
     ap.add_argument("--iterations", type=int, default=128, help="relaxation iterations per step")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the mid-size cell (tests only)")
     ap.add_argument("--capacity", type=int, default=256, help="neighbor slots per segment")
@@ -64,6 +65,7 @@ def parse():
     ap.add_argument("--tta-iterations", type=int, default=20000, help="iteration cap of each time-to-admissible run")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-iterations", type=int, default=40)
+    ap.add_argument("--cpu-specimens", type=int, default=16, help="arena specimens the CPU baseline relaxes")
     ap.add_argument("--reference-iterations", type=int, default=4,
                     help="relaxation iterations per step of the reference arm (CPU)")
     ap.add_argument("--save-positions", default=None, help="write the positions after the timed steps (.npy)")
@@ -79,9 +81,19 @@ def dist_env():
 
 
 def workload(args, rank):
-    from tangle_b200.generate import cpu_runnable_specimen, mid_size_specimen
+    """(assembly or list of assemblies for the arena, config, name, smallest diameter)."""
+    from tangle_b200.generate import batched_specimens, cpu_runnable_specimen, mid_size_specimen
     from tangle_b200.settings import RelaxationSettings
 
+    if args.workload == "batched":
+        assemblies = batched_specimens(count=args.specimens, seed=1 + rank)
+        d_min = min(a.smallest_diameter() for a in assemblies)
+        name = (f"batched: {args.specimens} specimens in one arena, fiber count log-uniform 40-5,000, d 10 um, "
+                "length 0.3-1 mm, segment 2d, fiber volume fraction 5-25 %, isotropic, curvature limit 1/(5d)")
+        settings = RelaxationSettings(penetration_tolerance=1.0e-3 * d_min, neighbor_capacity=args.capacity,
+                                      max_list_bytes=32 << 30, iterations_per_batch=args.iterations,
+                                      max_iterations=100000)
+        return assemblies, settings.to_config(d_min), name, d_min
     if args.workload == "cpu_runnable":
         assembly = cpu_runnable_specimen(seed=1 + rank)
         name = "cpu_runnable: periodic 300 um cube, 40 straight 10 um fibers x 30 segments (1,240 nodes)"
@@ -248,6 +260,39 @@ def time_to_admissible(packed, config, d_min, net, limit):
     return out
 
 
+def arena_time_to_admissible(packs, config, limit):
+    """A fresh arena relaxed batch after batch until every specimen's gate
+    holds (or `limit` iterations): each specimen's iterations and the wall
+    time of the batch in which it first converged, as percentiles."""
+    import numpy as np
+    import torch
+
+    from tangle_b200.device import DeviceWorld
+
+    world = DeviceWorld.arena(packs, config.cell_list, config.max_step)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    seconds = [None] * len(packs)
+    iterations = [None] * len(packs)
+    while True:
+        status = world.run_batch(config, config.iterations_per_batch)
+        elapsed = time.perf_counter() - t0
+        for i, st in enumerate(world.specimen_statuses(config)):
+            if st.converged and seconds[i] is None:
+                seconds[i] = elapsed
+                iterations[i] = st.total_iterations
+        if all(s is not None for s in seconds) or status.total_iterations >= limit:
+            break
+    world.close()
+    done = [s for s in seconds if s is not None]
+    its = [i for i in iterations if i is not None]
+    pct = lambda xs, q: float(np.percentile(xs, q)) if xs else None
+    return {"specimens": len(packs), "converged": len(done), "seconds": time.perf_counter() - t0,
+            "iterations_cap": limit, "seconds_p50": pct(done, 50), "seconds_p90": pct(done, 90),
+            "seconds_max": max(done) if done else None, "iterations_p50": pct(its, 50),
+            "iterations_p90": pct(its, 90), "iterations_max": max(its) if its else None, "method": "plain PBD"}
+
+
 def load_warmstart_net():
     path = os.path.join(ROOT, "tangle_b200", "warmstart_net.npz")
     if not os.path.exists(path):
@@ -258,21 +303,28 @@ def load_warmstart_net():
 
 
 def cpu_baseline(packed, config, nodes, iterations):
+    """The oracle on the same specimen (or, for an arena, on the first
+    specimens of it, one after another), all host threads."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
 
     cores = os.cpu_count() or 1
     orc.set_threads(cores)
-    world = orc.OracleWorld(packed, config.cell_list, config.max_step)
+    packs = packed if isinstance(packed, list) else [packed]
     fixed = type(config)(**{**config.__dict__, "force_full_iterations": True})
-    world.run_batch(fixed, 1)  # builds the lists
-    t0 = time.perf_counter()
-    status = world.run_batch(fixed, iterations)
-    elapsed = time.perf_counter() - t0
-    done = max(status.batch_iterations, 1)
-    world.close()
-    return {"value": nodes * done / elapsed, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{done} plain iterations of the same specimen after one list-building iteration, "
+    work, elapsed, done = 0.0, 0.0, 0
+    for p in packs:
+        world = orc.OracleWorld(p, config.cell_list, config.max_step)
+        world.run_batch(fixed, 1)  # builds the lists
+        t0 = time.perf_counter()
+        status = world.run_batch(fixed, iterations)
+        elapsed += time.perf_counter() - t0
+        done = max(status.batch_iterations, 1)
+        work += p.vertex_count * done
+        world.close()
+    what = "the same specimen" if len(packs) == 1 else f"the first {len(packs)} specimens of the arena"
+    return {"value": work / elapsed, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{done} plain iterations of {what} after one list-building iteration, "
                       f"{elapsed:.1f} s, OpenMP over {cores} threads"}
 
 
@@ -286,32 +338,40 @@ def run_reference(args):
     import oracle as orc
 
     assembly, config, name, d_min = workload(args, 0)
-    packed = PackedAssembly.from_assembly(assembly)
-    nodes = packed.vertex_count
+    # The arena's reference is the same algorithm world by world: a bounded
+    # sample of its specimens relaxed one after another.
+    assemblies = assembly[: args.cpu_specimens] if isinstance(assembly, list) else [assembly]
+    packs = [PackedAssembly.from_assembly(a) for a in assemblies]
     cores = os.cpu_count() or 1
     orc.set_threads(cores)
-    world = orc.OracleWorld(packed, config.cell_list, config.max_step)
+    worlds = [orc.OracleWorld(p, config.cell_list, config.max_step) for p in packs]
     fixed = type(config)(**{**config.__dict__, "force_full_iterations": True})
     per_step = args.reference_iterations
     for _ in range(max(args.warmup, 1)):
-        world.run_batch(fixed, per_step)
+        for world in worlds:
+            world.run_batch(fixed, per_step)
     t0 = time.perf_counter()
-    done = 0
+    work = 0.0
     for _ in range(args.steps):
-        st = world.run_batch(fixed, per_step)
-        done += st.batch_iterations
+        for p, world in zip(packs, worlds):
+            st = world.run_batch(fixed, per_step)
+            work += p.vertex_count * st.batch_iterations
     elapsed = time.perf_counter() - t0
-    value = nodes * done / elapsed
+    nodes = sum(p.vertex_count for p in packs)
+    value = work / elapsed
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": name, "nodes": nodes, "segments": packed.segment_count,
-                   "iterations_per_step": per_step, "neighbor_capacity": config.cell_list.neighbor_capacity},
+        "config": {"workload": name, "nodes": nodes, "segments": sum(p.segment_count for p in packs),
+                   "specimens_timed": len(packs), "iterations_per_step": per_step,
+                   "neighbor_capacity": config.cell_list.neighbor_capacity},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} steps of {per_step} iterations of the same specimen, "
-                                   f"OpenMP over {cores} threads"},
+                         "sample": f"{args.steps} steps of {per_step} iterations of "
+                                   + ("the same specimen" if len(packs) == 1
+                                      else f"the first {len(packs)} specimens of the arena, one after another")
+                                   + f", OpenMP over {cores} threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -336,10 +396,17 @@ def run_cuda(args):
 
     build()
     assembly, config, name, d_min = workload(args, rank)
-    packed = PackedAssembly.from_assembly(assembly)
-    nodes = packed.vertex_count
+    batched = isinstance(assembly, list)
+    if batched:
+        packs = [PackedAssembly.from_assembly(a) for a in assembly]
+        packed = None
+        nodes = sum(p.vertex_count for p in packs)
+        world = DeviceWorld.arena(packs, config.cell_list, config.max_step)
+    else:
+        packed = PackedAssembly.from_assembly(assembly)
+        nodes = packed.vertex_count
+        world = DeviceWorld(packed, config.cell_list, config.max_step)
     fixed = type(config)(**{**config.__dict__, "force_full_iterations": True})
-    world = DeviceWorld(packed, config.cell_list, config.max_step)
     if args.load_positions:
         world.upload_positions(np.load(args.load_positions))
     world.set_kernel_timing(True)
@@ -455,7 +522,9 @@ def run_cuda(args):
     # Time to admissible from the initial specimen, plain PBD and with the
     # learned warm start first (device-resident, same gates, same cap).
     tta = None
-    if not args.no_tta:
+    if not args.no_tta and batched:
+        tta = {"plain": arena_time_to_admissible(packs, config, args.tta_iterations)}
+    elif not args.no_tta:
         tta = {"plain": time_to_admissible(packed, config, d_min, None, args.tta_iterations)}
         net = load_warmstart_net()
         if net is not None:
@@ -465,15 +534,17 @@ def run_cuda(args):
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu:
-        cpu = cpu_baseline(packed, config, nodes, args.cpu_iterations)
+        cpu = cpu_baseline(packs[: args.cpu_specimens] if batched else packed, config, None, args.cpu_iterations)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-            "config": {"workload": name, "nodes": nodes, "segments": packed.segment_count,
-                       "fibers": packed.fiber_count, "iterations_per_step": args.iterations,
+            "config": {"workload": name, "nodes": nodes,
+                       "segments": sum(p.segment_count for p in packs) if batched else packed.segment_count,
+                       "fibers": sum(p.fiber_count for p in packs) if batched else packed.fiber_count,
+                       "specimens": len(packs) if batched else 1, "iterations_per_step": args.iterations,
                        "neighbor_capacity": config.cell_list.neighbor_capacity,
                        "l2": "inputs larger than L2 (positions, geometry and lists exceed 126 MB)",
                        "parallelism": f"replicas x{world_size}"},
