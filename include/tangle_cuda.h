@@ -92,6 +92,8 @@ typedef struct {
     uint32_t curvature_cleanup_sweeps;
     uint32_t contact_aggregation;   /* 0 uniform average, 1 penetration weighted, 2 deepest only */
     uint32_t force_full_iterations; /* nonzero: ignore the tolerances */
+    uint32_t motion_model;          /* FiberMotion (plugin.rs:30-44): 0 flexible, 1 rigid translation */
+    uint32_t reserved;
 } tgl_relax_config;
 
 /* BatchStatus (crates/tangle_relax/src/device/world.rs:91-114). */
@@ -193,6 +195,21 @@ int tgl_neighbor_list_rebuilds(tgl_world *world, uint32_t *rebuilds);
  * Reports the skin (0 when off), the entries per slot, and the refreshes
  * done so far. */
 int tgl_contact_list_info(tgl_world *world, float *contact_skin, uint32_t *block, uint32_t *refreshes);
+
+/* DeviceFiberWorld::capture_contacts (world.rs:2195-2335) with
+ * capture_segment_contacts (crates/tangle_contact/src/device/contact.rs:9-230):
+ * every pair of segments of different fibers whose surfaces are at most
+ * `maximum_surface_gap` apart (negative gaps are overlaps), found on a
+ * whole-segment cell grid of cell size + gap. Writes up to `capacity` pairs
+ * (segments[2 i], segments[2 i + 1], first < second), their closest-point
+ * parameters (coordinates[2 i] on the first, [2 i + 1] on the second), the
+ * surface gaps and the crossing angles (radians, in [0, pi / 2]), sorted by
+ * (first, second, s, t); *count is the number written and *overflow is 1
+ * when more pairs existed. The next batch rebuilds the neighbor lists, as
+ * in the reference (the capture reuses their cell buffers). */
+int tgl_capture_contacts(tgl_world *world, float maximum_surface_gap, uint32_t capacity, uint32_t *segments,
+                         float *coordinates, float *surface_gaps, float *crossing_angles, uint32_t *count,
+                         uint32_t *overflow);
 
 /* Parity taps (no reference counterpart beyond its tests' readbacks,
  * world_tests.rs:1342-1363). Forces a neighbor-list rebuild from the current

@@ -75,6 +75,8 @@ class _Config(ctypes.Structure):
         ("curvature_cleanup_sweeps", ctypes.c_uint32),
         ("contact_aggregation", ctypes.c_uint32),
         ("force_full_iterations", ctypes.c_uint32),
+        ("motion_model", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 
@@ -277,5 +279,5 @@ def _config(config) -> _Config:
         float(config.bend_stiffness), float(config.curvature_limit_stiffness),
         float(config.curvature_limit_safety_margin), float(config.curvature_ratio_tolerance),
         float(config.max_step), int(config.constraint_iterations), int(config.curvature_cleanup_sweeps),
-        int(config.contact_aggregation), int(bool(config.force_full_iterations)),
+        int(config.contact_aggregation), int(bool(config.force_full_iterations)), int(config.motion_code), 0,
     )

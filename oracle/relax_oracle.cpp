@@ -10,7 +10,7 @@
  * Scope: round sections (segment_lane_offsets == 0, so the lane loop of
  * contact.rs:641-652 is one lane at zero offset and every director/turn term
  * vanishes), non-adaptive layouts (every segment one proxy piece, list
- * weight 1), flexible motion.
+ * weight 1), flexible and rigid-translation motion.
  */
 #include "relax_oracle.h"
 
@@ -1049,6 +1049,66 @@ void orc_world_destroy(orc_world *w) { delete w; }
 
 /* world.rs:1020-1505 for the plain flexible path, then read_status
  * (world.rs:2337-2369). */
+/* kernels.rs:1539-1646 apply_rigid_contact_corrections: each fiber moves as
+ * a whole by its deepest segment's mean end correction (the first segment
+ * with the largest squared length wins ties), capped at max_step, clamped
+ * on walled axes so that every vertex stays inside. */
+void apply_rigid_contact_corrections(orc_world &w, float max_step) {
+    const int64_t F = (int64_t)w.fiber_vertex_spans.size() / 2;
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < F; ++f) {
+        const uint32_t s0 = w.fiber_segment_spans[2 * f], m = w.fiber_segment_spans[2 * f + 1];
+        const uint32_t v0 = w.fiber_vertex_spans[2 * f], n = w.fiber_vertex_spans[2 * f + 1];
+        float tx = 0.0f, ty = 0.0f, tz = 0.0f, deepest_squared = 0.0f;
+        for (uint32_t local = 0; local < m; ++local) {
+            const size_t seg = s0 + local;
+            const float cx = 0.5f * (w.corrections[6 * seg] + w.corrections[6 * seg + 3]);
+            const float cy = 0.5f * (w.corrections[6 * seg + 1] + w.corrections[6 * seg + 4]);
+            const float cz = 0.5f * (w.corrections[6 * seg + 2] + w.corrections[6 * seg + 5]);
+            const float squared = cx * cx + cy * cy + cz * cz;
+            if (squared > deepest_squared) {
+                deepest_squared = squared;
+                tx = cx;
+                ty = cy;
+                tz = cz;
+            }
+        }
+        const float length = std::sqrt(tx * tx + ty * ty + tz * tz);
+        if (length > max_step) {
+            const float scale = max_step / length;
+            tx *= scale;
+            ty *= scale;
+            tz *= scale;
+        }
+        const float rx = tx, ry = ty, rz = tz;
+        float lower[3], upper[3];
+        for (int a = 0; a < 3; ++a) {
+            const size_t c = 3 * (size_t)v0 + a;
+            lower[a] = w.grid.lower[a] + w.wall_extents[c] - w.positions[c];
+            upper[a] = w.grid.upper[a] - w.wall_extents[c] - w.positions[c];
+        }
+        for (uint32_t local = 1; local < n; ++local)
+            for (int a = 0; a < 3; ++a) {
+                const size_t c = 3 * (size_t)(v0 + local) + a;
+                lower[a] = std::max(lower[a], w.grid.lower[a] + w.wall_extents[c] - w.positions[c]);
+                upper[a] = std::min(upper[a], w.grid.upper[a] - w.wall_extents[c] - w.positions[c]);
+            }
+        float t[3] = {tx, ty, tz};
+        for (int a = 0; a < 3; ++a)
+            if (!w.grid.periodic[a]) t[a] = t[a] < lower[a] ? lower[a] : (t[a] > upper[a] ? upper[a] : t[a]);
+        const float applied = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        const float reaction[3] = {(rx - t[0]) / (float)n, (ry - t[1]) / (float)n, (rz - t[2]) / (float)n};
+        for (uint32_t local = 0; local < n; ++local) {
+            const size_t v = v0 + local;
+            for (int a = 0; a < 3; ++a) {
+                w.positions[3 * v + a] += t[a];
+                w.wall_reactions[3 * v + a] += reaction[a];
+            }
+            w.vertex_step[v] = applied;
+        }
+    }
+}
+
 int orc_run_batch(orc_world *w, const orc_relax_config *config, uint32_t iterations, orc_batch_status *status) {
     if (!w || !config || !status) return fail("null argument");
     if (iterations == 0) return fail("iterations must be positive");
@@ -1064,11 +1124,15 @@ int orc_run_batch(orc_world *w, const orc_relax_config *config, uint32_t iterati
         }
         if (w->control[0]) {
             std::fill(w->wall_reactions.begin(), w->wall_reactions.end(), 0.0f);
-            for (uint32_t c = 0; c < config->constraint_iterations; ++c)
-                internal_pass(*w, config->stretch_stiffness, config->bend_stiffness);
-            apply_contact_corrections(*w, config->max_step);
-            project_fiber_curvature(*w, config->curvature_cleanup_sweeps, config->curvature_limit_stiffness,
-                                    config->curvature_limit_safety_margin);
+            if (config->motion_model == 1) {  // world.rs:1369-1404
+                apply_rigid_contact_corrections(*w, config->max_step);
+            } else {
+                for (uint32_t c = 0; c < config->constraint_iterations; ++c)
+                    internal_pass(*w, config->stretch_stiffness, config->bend_stiffness);
+                apply_contact_corrections(*w, config->max_step);
+                project_fiber_curvature(*w, config->curvature_cleanup_sweeps, config->curvature_limit_stiffness,
+                                        config->curvature_limit_safety_margin);
+            }
         }
         flag_neighbor_list_displacement(*w);
     }

@@ -81,6 +81,8 @@ typedef struct {
     uint32_t curvature_cleanup_sweeps;
     uint32_t contact_aggregation; /* 0 average, 1 penetration weighted, 2 deepest */
     uint32_t force_full_iterations;
+    uint32_t motion_model;        /* FiberMotion (plugin.rs:30-44): 0 flexible, 1 rigid translation */
+    uint32_t reserved;
 } orc_relax_config;
 
 /* BatchStatus (world.rs:91-114). */

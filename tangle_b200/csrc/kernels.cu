@@ -1629,6 +1629,147 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
     }
 }
 
+// ------------------------------------------------------ rigid translation
+
+// apply_rigid_contact_corrections (kernels.rs:1539-1646) for one fiber per
+// warp: the fiber moves as a whole by its deepest segment's mean end
+// correction (the first of equal maxima, as the serial loop picks it),
+// capped at max_step and clamped on walled axes so that every vertex stays
+// inside; pinned vertices move with it, as in the reference. Then the same
+// write-back as the flexible update: geometry records, the displacement
+// checks and the next gate's step and curvature maxima.
+template <bool A>
+__global__ void __launch_bounds__(256) rigid_kernel(WorldDev w, StepParams sp) {
+    if (w.ctl->control[0] == 0) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const bool contact_lists = !A && w.contact_skin > 0.0f;
+    uint32_t smax = 0, cmax = 0;
+    bool far = false, contact_far = false;
+    for (uint32_t f = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); f < w.F; f += warps) {
+        const uint32_t spec = spec_of_fiber<A>(w, f);
+        if (A && ctl_of<A>(w, spec)->control[0] == 0) continue;
+        const Grid &g = grid_of<A>(w, spec);
+        const uint2 span = w.fiber_vspan[f];
+        const uint32_t v0 = span.x, n = span.y, m = n - 1, s0 = w.fiber_s0[f];
+        // Deepest segment: each lane keeps its first strict maximum, then the
+        // warp takes the largest, the lowest segment on ties.
+        float best = 0.0f, bx = 0.0f, by = 0.0f, bz = 0.0f;
+        uint32_t best_index = 0xFFFFFFFFu;
+        for (uint32_t local = lane; local < m; local += 32) {
+            const float4 c0 = w.corr[2 * (size_t)(s0 + local)], c1 = w.corr[2 * (size_t)(s0 + local) + 1];
+            const float cx = 0.5f * (c0.x + c1.x), cy = 0.5f * (c0.y + c1.y), cz = 0.5f * (c0.z + c1.z);
+            const float squared = cx * cx + cy * cy + cz * cz;
+            if (squared > best) {
+                best = squared;
+                best_index = local;
+                bx = cx;
+                by = cy;
+                bz = cz;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ob = __shfl_xor_sync(FULL, best, o);
+            const uint32_t oi = __shfl_xor_sync(FULL, best_index, o);
+            const float ox = __shfl_xor_sync(FULL, bx, o), oy = __shfl_xor_sync(FULL, by, o),
+                        oz = __shfl_xor_sync(FULL, bz, o);
+            if (ob > best || (ob == best && oi < best_index)) {
+                best = ob;
+                best_index = oi;
+                bx = ox;
+                by = oy;
+                bz = oz;
+            }
+        }
+        float tx = bx, ty = by, tz = bz;
+        const float length = sqrtf(tx * tx + ty * ty + tz * tz);
+        if (length > sp.max_step) {
+            const float scale = sp.max_step / length;
+            tx *= scale;
+            ty *= scale;
+            tz *= scale;
+        }
+        // The translation that keeps every vertex inside the walls.
+        float lo[3] = {-INFINITY, -INFINITY, -INFINITY}, hi[3] = {INFINITY, INFINITY, INFINITY};
+        for (uint32_t local = lane; local < n; local += 32) {
+            const float4 x = w.pos[v0 + local];
+            const float extent = w.vtx_static[v0 + local].w;
+            const float xs[3] = {x.x, x.y, x.z};
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = fmaxf(lo[a], g.lower[a] + extent - xs[a]);
+                hi[a] = fminf(hi[a], g.upper[a] - extent - xs[a]);
+            }
+        }
+        for (int a = 0; a < 3; ++a)
+            for (int o = 16; o > 0; o >>= 1) {
+                lo[a] = fmaxf(lo[a], __shfl_xor_sync(FULL, lo[a], o));
+                hi[a] = fminf(hi[a], __shfl_xor_sync(FULL, hi[a], o));
+            }
+        float t[3] = {tx, ty, tz};
+        for (int a = 0; a < 3; ++a)
+            if (!g.periodic[a]) t[a] = t[a] < lo[a] ? lo[a] : (t[a] > hi[a] ? hi[a] : t[a]);
+        const float applied = sqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        for (uint32_t local = lane; local < n; local += 32) {
+            float4 x = w.pos[v0 + local];
+            x.x += t[0];
+            x.y += t[1];
+            x.z += t[2];
+            w.pos[v0 + local] = x;
+            w.vertex_step[v0 + local] = applied;
+        }
+        __syncwarp();
+        smax = max(smax, __float_as_uint(fmaxf(applied, 0.0f)));
+        const float md = 0.5f * skin_of<A>(w, spec);
+        const float radius = w.seg_static[s0].x;
+        const float4 *P = w.pos + v0;
+        for (uint32_t i = lane; i < n; i += 32) {
+            const float4 x = P[i];
+            const float4 r = w.ref_pos[v0 + i];
+            const float dx = x.x - r.x, dy = x.y - r.y, dz = x.z - r.z;
+            if (dx * dx + dy * dy + dz * dz > md * md) far = true;
+            if (contact_lists && contact_moved(w, v0 + i, x.x, x.y, x.z)) contact_far = true;
+            if (i > 0 && i + 1 < n) {
+                const float maximum = w.vtx_static[v0 + i].x;
+                if (maximum > 0.0f) {
+                    const float ratio = curvature_ratio_at([&](int k) { return P[k]; }, (int)i, maximum);
+                    cmax = max(cmax, __float_as_uint(fmaxf(ratio, 0.0f)));
+                }
+            }
+            if (i + 1 < n) {
+                const float4 y = P[i + 1];
+                const float ex = y.x - x.x, ey = y.y - x.y, ez = y.z - x.z;
+                const float half = 0.5f * sqrtf(ex * ex + ey * ey + ez * ez);
+                w.geom[2 * (size_t)(s0 + i)] = make_float4(x.x, x.y, x.z, radius);
+                w.geom[2 * (size_t)(s0 + i) + 1] = make_float4(y.x, y.y, y.z, half);
+                if (contact_lists && half > w.contact_half_limit) contact_far = true;
+            }
+        }
+        __syncwarp();
+        if (A) {
+            cmax = warp_max_u32(cmax);
+            const bool fiber_far = __any_sync(FULL, far);
+            if (lane == 0) {
+                if (smax) atomicMax(&ctl_of<A>(w, spec)->acc[1], smax);
+                if (cmax) atomicMax(&ctl_of<A>(w, spec)->acc[2], cmax);
+                if (fiber_far) flag_rebuild<A>(w, spec);
+            }
+            smax = cmax = 0;
+            far = false;
+        }
+    }
+    if (A) return;
+    smax = warp_max_u32(smax);
+    cmax = warp_max_u32(cmax);
+    const bool any_far = __any_sync(FULL, far);
+    const bool any_contact_far = __any_sync(FULL, contact_far);
+    if (lane == 0) {
+        if (smax) atomicMax(&w.ctl->acc[1], smax);
+        if (cmax) atomicMax(&w.ctl->acc[2], cmax);
+        if (any_far) w.ctl->neighbor_state[0] = 1;
+        if (any_contact_far) w.ctl->contact_state[0] = 1;
+    }
+}
+
 // ---------------------------------------------------------------- host copies
 
 __global__ void positions_from_stage_kernel(WorldDev w) {
@@ -1795,6 +1936,16 @@ static void enqueue_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_
     rb_finish_kernel<A><<<1, A ? 256 : 32, 0, st>>>(w);
 }
 
+int launch_cell_list(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
+    const int cap = lp.num_sms * 16;
+    rb_clear_kernel<false><<<grid_for(w.C, 256, cap), 256, 0, st>>>(w);
+    rb_count_kernel<false><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
+    rb_scan_kernel<<<1, 1024, 0, st>>>(w);
+    rb_scatter_kernel<false><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
+    rb_sort_cells_kernel<false><<<grid_for(w.C, 8, cap), 256, 8 * CELL_SORT_CAP * sizeof(uint32_t), st>>>(w);
+    return 5;
+}
+
 int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
     if (lp.arena)
         enqueue_rebuild<true>(w, lp, st);
@@ -1830,6 +1981,14 @@ static void enqueue_lanes(const WorldDev &w, const LaunchPlan &lp, const StepPar
 }
 
 int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st) {
+    if (sp.motion_model == 1) {
+        const int blocks = grid_for(w.F, 8, lp.num_sms * 16);
+        if (lp.arena)
+            rigid_kernel<true><<<blocks, 256, 0, st>>>(w, sp);
+        else
+            rigid_kernel<false><<<blocks, 256, 0, st>>>(w, sp);
+        return 1;
+    }
     if (lp.fiber_lanes) {
         if (lp.arena)
             enqueue_lanes<true>(w, lp, sp, st);

@@ -92,6 +92,7 @@ struct StepParams {
     uint32_t contact_aggregation;
     uint32_t force_full_iterations;
     uint32_t max_iterations;  // the batch size: the gate stops at this many
+    uint32_t motion_model;    // 0 flexible, 1 rigid translation
 };
 
 // Launch plans, fixed per world.
@@ -123,6 +124,14 @@ int launch_begin_batch(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st)
 int launch_flag_displacement(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 int launch_measure_start(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
+// The cell list alone (clear, count, scan, scatter, rank) on w's grid and
+// cell buffers, gated on the rebuild flag like the full rebuild.
+int launch_cell_list(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
+// capture_segment_contacts (contact.rs:9-230) on the cell list of w's grid:
+// pairs of different fibers within max_gap of touching, appended to the
+// output arrays (count[0]; count[1] set on overflow).
+void launch_capture(const WorldDev &w, float max_gap, uint32_t capacity, uint32_t *count, uint32_t *pairs,
+                    float *coordinates, float *gaps, float *angles, cudaStream_t st);
 int launch_request_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 // With the gate and contact lists on, enqueues the listed pass and the
 // refresh pass, each of which returns at once unless the device-side refresh

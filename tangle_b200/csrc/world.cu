@@ -165,6 +165,7 @@ StepParams step_params(const tgl_relax_config &c, uint32_t iterations) {
     sp.curvature_cleanup_sweeps = c.curvature_cleanup_sweeps;
     sp.contact_aggregation = c.contact_aggregation;
     sp.force_full_iterations = c.force_full_iterations ? 1u : 0u;
+    sp.motion_model = c.motion_model;
     sp.max_iterations = iterations;
     return sp;
 }
@@ -185,6 +186,7 @@ int validate_config(const tgl_relax_config &c) {
     if (!(c.curvature_ratio_tolerance >= 0.0f)) return set_error(TGL_ERR_INVALID, "curvature_ratio_tolerance must be non-negative");
     if (c.constraint_iterations == 0) return set_error(TGL_ERR_INVALID, "constraint_iterations must be positive");
     if (c.curvature_cleanup_sweeps == 0) return set_error(TGL_ERR_INVALID, "curvature_cleanup_sweeps must be positive");
+    if (c.motion_model > 1) return set_error(TGL_ERR_INVALID, "motion_model must be 0 (flexible) or 1 (rigid translation)");
     if (!(c.max_step > 0.0f)) return set_error(TGL_ERR_INVALID, "max_step must be positive");
     if (c.contact_aggregation > 2) return set_error(TGL_ERR_INVALID, "contact_aggregation must be 0, 1 or 2");
     return 0;
@@ -1036,6 +1038,91 @@ int tgl_world_residual(tgl_world *w, const tgl_relax_config *config, float *max_
     *max_penetration = out[0];
     *max_curvature_ratio = out[1];
     *total_penetration = out[2];
+    return 0;
+}
+
+int tgl_capture_contacts(tgl_world *w, float maximum_surface_gap, uint32_t capacity, uint32_t *segments,
+                         float *coordinates, float *surface_gaps, float *crossing_angles, uint32_t *count,
+                         uint32_t *overflow) {
+    if (!w || !segments || !coordinates || !surface_gaps || !crossing_angles || !count || !overflow)
+        return set_error(TGL_ERR_INVALID, "null argument");
+    if (!(std::isfinite(maximum_surface_gap) && maximum_surface_gap >= 0.0f))  // world.rs:2203
+        return set_error(TGL_ERR_INVALID, "maximum_surface_gap must be finite and non-negative");
+    if (capacity == 0) return set_error(TGL_ERR_INVALID, "capacity must be positive");
+    if (w->arena) return set_error(TGL_ERR_UNSUPPORTED, "contact capture takes one specimen");
+    w->warm.counted = false;
+    // world.rs:2209-2218: whole-segment cells grown by the gap (never finer
+    // than the neighbor grid, whose cell buffers the capture reuses).
+    WorldDev cap = w->dev;
+    const float cell = w->cell_size + maximum_surface_gap;
+    uint64_t C = 1;
+    for (int a = 0; a < 3; ++a) {
+        const float extent = cap.grid.length[a];
+        cap.grid.cells[a] = f32_to_u32_host(std::fmax(std::floor(extent / cell), 1.0f));
+        cap.grid.width[a] = extent / (float)cap.grid.cells[a];
+        C *= cap.grid.cells[a];
+    }
+    if (C > w->dev.C) return set_error(TGL_ERR_UNSUPPORTED, "capture grid finer than the neighbor grid");
+    cap.C = (uint32_t)C;
+    uint32_t *count_d = nullptr, *pairs_d = nullptr;
+    float *coords_d = nullptr, *gaps_d = nullptr, *angles_d = nullptr;
+    auto release = [&]() {
+        cudaFree(count_d);
+        cudaFree(pairs_d);
+        cudaFree(coords_d);
+        cudaFree(gaps_d);
+        cudaFree(angles_d);
+    };
+    if (cudaMalloc(&count_d, 2 * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&pairs_d, 2ull * capacity * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&coords_d, 2ull * capacity * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&gaps_d, (size_t)capacity * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&angles_d, (size_t)capacity * sizeof(float)) != cudaSuccess) {
+        release();
+        return set_error(TGL_ERR_MEMORY, "contact capture allocation failed");
+    }
+    // The shared cell buffers take the capture layout, so the next contact
+    // pass must rebuild its lists first: the rebuild flag stays raised.
+    w->launches += launch_request_rebuild(w->dev, w->lp, w->stream);
+    w->launches += launch_cell_list(cap, w->lp, w->stream);
+    cudaMemsetAsync(count_d, 0, 2 * sizeof(uint32_t), w->stream);
+    launch_capture(cap, maximum_surface_gap, capacity, count_d, pairs_d, coords_d, gaps_d, angles_d, w->stream);
+    w->launches += 1;
+    uint32_t counts[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(counts, count_d, sizeof(counts), cudaMemcpyDeviceToHost, w->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+    const uint32_t n = std::min(counts[0], capacity);
+    std::vector<uint32_t> pr(2 * (size_t)n);
+    std::vector<float> co(2 * (size_t)n), ga(n), an(n);
+    if (e == cudaSuccess && n) {
+        cudaMemcpy(pr.data(), pairs_d, pr.size() * 4, cudaMemcpyDeviceToHost);
+        cudaMemcpy(co.data(), coords_d, co.size() * 4, cudaMemcpyDeviceToHost);
+        cudaMemcpy(ga.data(), gaps_d, ga.size() * 4, cudaMemcpyDeviceToHost);
+        e = cudaMemcpy(an.data(), angles_d, an.size() * 4, cudaMemcpyDeviceToHost);
+    }
+    release();
+    if (e != cudaSuccess) return set_error(TGL_ERR_CUDA, std::string("contact capture: ") + cudaGetErrorString(e));
+    // world.rs:2314-2321: the device appends in a run-dependent order; sort by
+    // (first, second, s, t) so every run sees the same sequence.
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](uint32_t l, uint32_t r) {
+        if (pr[2 * l] != pr[2 * r]) return pr[2 * l] < pr[2 * r];
+        if (pr[2 * l + 1] != pr[2 * r + 1]) return pr[2 * l + 1] < pr[2 * r + 1];
+        if (co[2 * l] != co[2 * r]) return co[2 * l] < co[2 * r];
+        return co[2 * l + 1] < co[2 * r + 1];
+    });
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t k = order[i];
+        segments[2 * i] = pr[2 * k];
+        segments[2 * i + 1] = pr[2 * k + 1];
+        coordinates[2 * i] = co[2 * k];
+        coordinates[2 * i + 1] = co[2 * k + 1];
+        surface_gaps[i] = ga[k];
+        crossing_angles[i] = an[k];
+    }
+    *count = n;
+    *overflow = counts[1] != 0 ? 1u : 0u;
     return 0;
 }
 

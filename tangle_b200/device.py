@@ -13,6 +13,7 @@ CPU fallback: a missing library or device raises.
 from __future__ import annotations
 
 import ctypes
+from dataclasses import dataclass
 import os
 from typing import List, Optional
 
@@ -30,7 +31,7 @@ TGL_ERR_UNSUPPORTED = 5
 #: Every symbol include/tangle_cuda.h declares.
 EXPORTS = (
     "tgl_world_create", "tgl_world_destroy", "tgl_world_checkpoint", "tgl_world_restore", "tgl_run_batch",
-    "tgl_arena_create", "tgl_arena_status", "tgl_download_positions", "tgl_upload_positions",
+    "tgl_arena_create", "tgl_arena_status", "tgl_capture_contacts", "tgl_download_positions", "tgl_upload_positions",
     "tgl_cell_size", "tgl_cell_count", "tgl_cell_dims", "tgl_neighbor_skin", "tgl_neighbor_block",
     "tgl_neighbor_list_rebuilds", "tgl_debug_rebuild", "tgl_debug_cell_list", "tgl_debug_neighbor_lists",
     "tgl_debug_corrections", "tgl_kernel_launches", "tgl_set_kernel_timing", "tgl_last_kernel_times",
@@ -97,6 +98,8 @@ class Config(ctypes.Structure):
         ("curvature_cleanup_sweeps", ctypes.c_uint32),
         ("contact_aggregation", ctypes.c_uint32),
         ("force_full_iterations", ctypes.c_uint32),
+        ("motion_model", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 
@@ -145,6 +148,9 @@ def load_library():
     lib.tgl_world_create.restype = ctypes.c_int
     lib.tgl_world_destroy.argtypes = [P]
     lib.tgl_world_destroy.restype = None
+    lib.tgl_capture_contacts.argtypes = [P, ctypes.c_float, ctypes.c_uint32, P, P, P, P,
+                                         ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]
+    lib.tgl_capture_contacts.restype = ctypes.c_int
     lib.tgl_arena_create.argtypes = [ctypes.POINTER(Packed), ctypes.c_uint32, ctypes.POINTER(CellList), ctypes.c_float,
                                      ctypes.POINTER(ctypes.c_void_p)]
     lib.tgl_arena_create.restype = ctypes.c_int
@@ -246,13 +252,31 @@ def config_struct(config: RelaxationConfig) -> Config:
         float(config.bend_stiffness), float(config.curvature_limit_stiffness),
         float(config.curvature_limit_safety_margin), float(config.curvature_ratio_tolerance),
         float(config.max_step), int(config.constraint_iterations), int(config.curvature_cleanup_sweeps),
-        int(config.contact_aggregation), int(bool(config.force_full_iterations)),
+        int(config.contact_aggregation), int(bool(config.force_full_iterations)), int(config.motion_code), 0,
     )
 
 
 def cell_list_struct(cell_list: CellListConfig) -> CellList:
     return CellList(float(cell_list.cell_size_scale), float(cell_list.neighbor_skin_scale),
                     int(cell_list.neighbor_capacity), 0, int(cell_list.max_list_bytes))
+
+
+@dataclass
+class SegmentContactCandidate:
+    """One captured contact (world.rs SegmentContactCandidate)."""
+
+    first_segment: int
+    second_segment: int
+    first_coordinate: float
+    second_coordinate: float
+    surface_gap: float
+    crossing_angle: float
+
+
+@dataclass
+class ContactCapture:
+    candidates: List[SegmentContactCandidate]
+    overflow: bool
 
 
 class DeviceWorld:
@@ -307,6 +331,23 @@ class DeviceWorld:
         world.segment_count = sum(p.segment_count for p in packeds)
         world.specimen_vertices = [p.vertex_count for p in packeds]
         return world
+
+    def capture_contacts(self, maximum_surface_gap: float, capacity: int) -> "ContactCapture":
+        """DeviceWorld::capture_contacts (world.rs:2195-2335): current
+        inter-fiber contacts within the gap, sorted."""
+        segments = np.empty(2 * capacity, dtype=np.uint32)
+        coordinates = np.empty(2 * capacity, dtype=np.float32)
+        gaps = np.empty(capacity, dtype=np.float32)
+        angles = np.empty(capacity, dtype=np.float32)
+        count, overflow = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self._lib.tgl_capture_contacts(self._handle, ctypes.c_float(maximum_surface_gap), int(capacity),
+                                                   _ptr(segments), _ptr(coordinates), _ptr(gaps), _ptr(angles),
+                                                   ctypes.byref(count), ctypes.byref(overflow)))
+        n = int(count.value)
+        candidates = [SegmentContactCandidate(int(segments[2 * i]), int(segments[2 * i + 1]),
+                                              float(coordinates[2 * i]), float(coordinates[2 * i + 1]),
+                                              float(gaps[i]), float(angles[i])) for i in range(n)]
+        return ContactCapture(candidates, bool(overflow.value))
 
     def specimen_statuses(self, config: RelaxationConfig) -> List[BatchStatus]:
         """tgl_arena_status: each specimen's status after the last batch."""

@@ -89,8 +89,13 @@ class RelaxationConfig:
         for ok, message in checks:
             if not ok:
                 raise ValueError(message)
-        if self.motion_model != "flexible":
-            raise ValueError("motion_model='rigid_translation' is not provided by the CUDA relaxation path")
+        if self.motion_model not in _MOTION_MODELS:
+            raise ValueError(f"motion_model must be one of {', '.join(_MOTION_MODELS)}")
+
+    @property
+    def motion_code(self) -> int:
+        """FiberMotion as the C ABI's motion_model: 0 flexible, 1 rigid translation."""
+        return _MOTION_MODELS.index(self.motion_model)
 
 
 @dataclass
