@@ -216,20 +216,27 @@ __global__ void rb_count_kernel(WorldDev w) {
 }
 
 // Exclusive scan of the cell counts in one block (4096 cells per round).
+// In an arena, block p scans specimen p's cell range alone, starting at its
+// first slot (its first segment id), and only when its rebuild is pending.
+template <bool A>
 __global__ void __launch_bounds__(1024) rb_scan_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
+    const uint32_t spec = A ? blockIdx.x : 0u;
+    if (A && !rebuilding<A>(w, spec)) return;
+    const uint32_t first = A ? w.specs[spec].cell_base : 0u;
+    const uint32_t end = A ? first + w.specs[spec].cell_count : w.C;
     __shared__ uint32_t warp_sums[32];
     __shared__ uint32_t carry_s;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) carry_s = 0;
+    if (threadIdx.x == 0) carry_s = A ? w.specs[spec].seg_base : 0u;
     __syncthreads();
-    for (uint32_t base = 0; base < w.C; base += 4096) {
+    for (uint32_t base = first; base < end; base += 4096) {
         uint32_t idx = base + threadIdx.x * 4;
         uint32_t v[4];
         uint32_t local = 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            v[k] = (idx + k < w.C) ? w.cell_counts[idx + k] : 0u;
+            v[k] = (idx + k < end) ? w.cell_counts[idx + k] : 0u;
             local += v[k];
         }
         uint32_t incl = local;
@@ -254,7 +261,7 @@ __global__ void __launch_bounds__(1024) rb_scan_kernel(WorldDev w) {
         uint32_t run = carry_s + warp_sums[warp] + incl - local;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            if (idx + k < w.C) w.cell_offsets[idx + k] = run;
+            if (idx + k < end) w.cell_offsets[idx + k] = run;
             run += v[k];
         }
         __syncthreads();
@@ -1925,7 +1932,7 @@ static void enqueue_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_
     const int cap = lp.num_sms * 16;
     rb_clear_kernel<A><<<grid_for(w.C, 256, cap), 256, 0, st>>>(w);
     rb_count_kernel<A><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
-    rb_scan_kernel<<<1, 1024, 0, st>>>(w);
+    rb_scan_kernel<A><<<A ? (int)w.P : 1, 1024, 0, st>>>(w);
     rb_scatter_kernel<A><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
     rb_sort_cells_kernel<A><<<grid_for(w.C, 8, cap), 256, 8 * CELL_SORT_CAP * sizeof(uint32_t), st>>>(w);
     rb_gather_kernel<A><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
@@ -1940,7 +1947,7 @@ int launch_cell_list(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
     const int cap = lp.num_sms * 16;
     rb_clear_kernel<false><<<grid_for(w.C, 256, cap), 256, 0, st>>>(w);
     rb_count_kernel<false><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
-    rb_scan_kernel<<<1, 1024, 0, st>>>(w);
+    rb_scan_kernel<false><<<1, 1024, 0, st>>>(w);
     rb_scatter_kernel<false><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
     rb_sort_cells_kernel<false><<<grid_for(w.C, 8, cap), 256, 8 * CELL_SORT_CAP * sizeof(uint32_t), st>>>(w);
     return 5;

@@ -14,7 +14,9 @@ struct SpecimenDev {
     uint32_t build_prefilter; // sphere pre-test on (>= 3 cells on every periodic axis)
     float build_sphere_eps;
     float line_eps;
-    uint32_t pad[3];
+    uint32_t cell_count;      // cells of the specimen
+    uint32_t seg_base;        // first segment (= first cell-list slot) of the specimen
+    uint32_t pad;
 };
 
 // Every device pointer and size a kernel needs, passed by value.

@@ -568,6 +568,8 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
         sd.grid = h.grid;
         sd.skin = h.skin;
         sd.cell_base = cbase;
+        sd.cell_count = (uint32_t)h.C;
+        sd.seg_base = sbase;
         float edge = 0.0f;
         sd.build_prefilter = 1;
         for (int a = 0; a < 3; ++a) {

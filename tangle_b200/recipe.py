@@ -44,6 +44,7 @@ class RecipeError(RuntimeError):
 @dataclass
 class _Insert:
     assembly: FiberAssembly
+    count: int = 0  # fibers this step adds
 
 
 @dataclass
@@ -122,7 +123,7 @@ class Recipe:
         for fiber in collection.fibers:
             self._assembly.add_fiber(fiber.placed, fiber.intrinsic, radius=fiber.radius,
                                      min_bend_radius=fiber.min_bend_radius)
-        self._operations.append(_Insert(collection))
+        self._operations.append(_Insert(collection, collection.fiber_count))
         self._descriptions.append(f"insert {collection.fiber_count} fibers")
 
     def relax_until_converged(self, *, max_iterations: int = 2000) -> None:
@@ -168,18 +169,55 @@ class Recipe:
             operations.append(_RelaxUntilConverged(config.max_iterations))
             descriptions.append("relax until converged")
         assembly = copy.deepcopy(self._assembly)
-        packed = PackedAssembly.from_assembly(assembly, config.pin_fiber_ends)
+        # Staged activation (kernels.rs:164-221): the fibers of an insert step
+        # take part from that step on. The world holds the fibers active so
+        # far; when a relaxation step follows new inserts, it is re-created
+        # from the relaxed positions plus the new fibers (the lifetime
+        # iteration count carries over). Lists only need to be supersets of
+        # the contacts, so this moves nothing differently from masking.
+        active_after, active = [], 0
+        for op in operations:
+            if isinstance(op, _Insert):
+                active += op.count
+            active_after.append(active)
         status = BatchStatus(max_penetration=float("inf"), max_curvature_ratio=float("inf"))
         report = CheckpointReport()
         first_operation, first_completed = 0, 0
+        world, world_fibers, packed, uploaded = None, 0, None, 0
+
+        def first_fibers(k: int) -> FiberAssembly:
+            sub = FiberAssembly(assembly.cell)
+            for fiber in assembly.fibers[:k]:
+                sub.add_fiber(fiber.placed, fiber.intrinsic, radius=fiber.radius,
+                              min_bend_radius=fiber.min_bend_radius)
+            return sub
+
+        def activate(k: int) -> None:
+            nonlocal world, world_fibers, packed, uploaded
+            if world is not None:
+                if k == world_fibers:
+                    return
+                packed.unpack_positions(world.download_positions(), assembly)
+                world.close()
+            packed = PackedAssembly.from_assembly(first_fibers(k), config.pin_fiber_ends)
+            world = DeviceWorld(packed, config.cell_list, config.max_step,
+                                status.total_iterations if status.total_iterations else None)
+            uploaded += _upload_bytes(packed)
+            world_fibers = k
+
         if checkpoint is not None and checkpoint.resume:
             source = checkpoint.resume_path or checkpoint.path
             saved = ckpt.load(source, checkpoint.resume_case_id or checkpoint.case_id)
-            if saved.device.packed.vertex_count != packed.vertex_count or \
-                    saved.device.packed.segment_count != packed.segment_count:
+            k = saved.device.packed.fiber_count
+            expected = PackedAssembly.from_assembly(first_fibers(k), config.pin_fiber_ends) if k <= len(
+                assembly.fibers) else None
+            if expected is None or saved.device.packed.vertex_count != expected.vertex_count or \
+                    saved.device.packed.segment_count != expected.segment_count:
                 raise ckpt.CheckpointError("checkpoint assembly does not match the recipe's fibers")
             world = DeviceWorld.restore(config, saved.device)
             packed = saved.device.packed
+            world_fibers = k
+            uploaded += _upload_bytes(packed)
             status = BatchStatus(total_iterations=saved.device.total_iterations, max_penetration=float("inf"),
                                  max_curvature_ratio=float("inf"))
             if not checkpoint.fresh_formation_on_resume:
@@ -188,8 +226,6 @@ class Recipe:
             report.resumed = True
             report.resumed_iteration = saved.device.total_iterations
             report.last_saved_iteration = saved.device.total_iterations
-        else:
-            world = DeviceWorld.upload(config, packed)
         downloaded = 0
 
         def save(index: int, completed: int, terminal: bool) -> None:
@@ -214,6 +250,7 @@ class Recipe:
             for index, op in enumerate(operations):
                 if isinstance(op, _Insert) or index < first_operation:
                     continue
+                activate(active_after[index])
                 started = status.total_iterations - (first_completed if index == first_operation else 0)
                 force = isinstance(op, _RelaxFor)
                 budget = op.iterations if force else op.maximum_iterations
@@ -243,11 +280,14 @@ class Recipe:
                     save(index, status.total_iterations - started, False)
                 if force:
                     status.converged = False
+            if world is None:  # nothing to relax: the fibers stay where they were placed
+                activate(active_after[-1])
             save(len(operations), 0, True)
             positions = world.download_positions()
             downloaded += positions.nbytes
             packed.unpack_positions(positions, assembly)
-            return RunResult(assembly, status, _upload_bytes(packed), downloaded, world.cell_size, world.cell_count,
+            return RunResult(assembly, status, uploaded, downloaded, world.cell_size, world.cell_count,
                              world.neighbor_list_rebuilds(), report)
         finally:
-            world.close()
+            if world is not None:
+                world.close()

@@ -125,3 +125,40 @@ def test_recipe_saves_and_resumes(cuda_lib, tmp_path):
     # The recipe had finished: nothing more to run.
     assert resumed.iterations == 60
     np.testing.assert_array_equal(np.asarray(resumed.centerlines()), np.asarray(full.centerlines()))
+
+
+@pytest.mark.gpu
+def test_recipe_activates_inserted_fibers_step_by_step(cuda_lib):
+    """kernels.rs:164-221: fibers inserted after a relaxation step take no
+    part in it; the relaxation of the earlier fibers is that of a world
+    holding only them, and the lifetime iteration count runs on."""
+    from tangle_b200.assembly import Cell
+    from tangle_b200.device import DeviceWorld
+    from tangle_b200.recipe import Recipe
+
+    cell = Cell([300.0e-6] * 3, periodic="xyz")
+    first, second = cpu_runnable_specimen(seed=21), cpu_runnable_specimen(seed=22)
+    settings = RelaxationSettings(iterations_per_batch=16, penetration_tolerance=1.0e-8)
+    config = settings.to_config(first.smallest_diameter())
+
+    r = Recipe(cell)
+    r.insert(first)
+    r.relax_for(20)
+    r.insert(second)
+    staged = r.run(settings)
+    alone = DeviceWorld.upload(config, PackedAssembly.from_assembly(first))
+    fixed = RelaxationConfig(**{**config.__dict__, "force_full_iterations": True})
+    alone.run_batch(fixed, 16)
+    alone.run_batch(fixed, 4)
+    got = np.concatenate([np.asarray(c, dtype=np.float32).ravel() for c in staged.centerlines()[:first.fiber_count]])
+    np.testing.assert_array_equal(got.view(np.uint32), alone.download_positions().view(np.uint32))
+    for fiber, placed in zip(staged.assembly.fibers[first.fiber_count:], second.fibers):
+        np.testing.assert_array_equal(fiber.placed, placed.placed)
+    assert staged.iterations == 20
+
+    r.relax_for(10)
+    both = r.run(settings)
+    assert both.iterations == 30
+    moved = [not np.array_equal(f.placed, p.placed) for f, p in zip(both.assembly.fibers[first.fiber_count:],
+                                                                    second.fibers)]
+    assert any(moved)

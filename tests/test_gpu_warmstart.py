@@ -174,3 +174,29 @@ def test_residual_matches_the_contact_pass(cuda_lib):
     _, seg_pen = world.debug_corrections(config)
     assert np.float32(pen) == np.float32(seg_pen.max())
     assert total > 0.0 and ratio > 0.0
+
+
+def test_trained_network_gains_over_plain_relaxation(cuda_lib):
+    """The committed network, on specimens it was not trained on: its
+    proposal is accepted, and after the same 64 plain iterations the summed
+    overlap is at least 15 % below plain relaxation's."""
+    import os
+
+    from tangle_b200.device import DeviceWorld
+    from tangle_b200.warmstart import WarmStartNet, relaxation_config, residual, training_specimen, warm_start
+
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tangle_b200",
+                        "warmstart_net.npz")
+    net = WarmStartNet.load(path)
+    for index in (3, 7):
+        assembly = training_specimen(index, seed_base=700000)
+        config = relaxation_config(assembly)
+        fixed = RelaxationConfig(**{**config.__dict__, "force_full_iterations": True})
+        packed = PackedAssembly.from_assembly(assembly)
+        plain = DeviceWorld(packed, config.cell_list, config.max_step)
+        plain.run_batch(fixed, 64)
+        warm = DeviceWorld(packed, config.cell_list, config.max_step)
+        report = warm_start(warm, net, config)
+        assert report.accepted and report.residual_after < 0.6 * report.residual_before
+        warm.run_batch(fixed, 64)
+        assert residual(warm, config)[2] < 0.85 * residual(plain, config)[2]

@@ -74,8 +74,10 @@ def test_settings_validation_matches_the_reference(change, message):
 def test_settings_reject_what_the_plain_path_does_not_provide():
     with pytest.raises(ValueError):
         RelaxationSettings(backend="metal")
-    with pytest.raises(ValueError, match="rigid_translation"):
-        RelaxationSettings(motion_model="rigid_translation").to_config(1.0e-5)
+    with pytest.raises(ValueError, match="motion_model"):
+        RelaxationSettings(motion_model="wobble")
+    assert RelaxationSettings(motion_model="rigid_translation").to_config(1.0e-5).motion_code == 1
+    assert RelaxationSettings().to_config(1.0e-5).motion_code == 0
 
 
 def test_acos_f32_is_within_one_ulp():
