@@ -1522,55 +1522,54 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             }
         }
         // Curvature Gauss-Seidel, LPF lanes per fiber, forward then backward.
-        if (mine != TGL_NONE) {
-            const Grid &g = grid_of<A>(w, spec_of_fiber<A>(w, mine));
-            const uint2 span = w.fiber_vspan[mine];
-            const int last = (int)span.y - 3;
-            const float extent = w.seg_static[w.fiber_s0[mine]].x;
+        // The warp's groups step together: every round each unfinished group
+        // tests LPF triplets of its own fiber, one warp-wide ballot gives
+        // every group its bits, and each group applies its own first acting
+        // triplet. A group's sequence of tests and moves is exactly its
+        // serial sweep; stepping together only shares the instruction issue
+        // between the groups. A pass that moves nothing ends its group's
+        // sweeps (every later pass would test the same positions).
+        {
+            const Grid &g = grid_of<A>(w, mine != TGL_NONE ? spec_of_fiber<A>(w, mine) : 0u);
+            const int last = mine != TGL_NONE ? (int)w.fiber_vspan[mine].y - 3 : -1;
+            const float extent = mine != TGL_NONE ? w.seg_static[w.fiber_s0[mine]].x : 0.0f;
             float4 *P = lanes_smem + (size_t)group * stride;
-            // A pass that moves nothing ends the sweeps (every later pass
-            // would test the same positions).
-            for (uint32_t sweep = 0; sweep < sp.curvature_cleanup_sweeps; ++sweep) {
-                bool moved = false;
-                int t0 = 0;
-                while (t0 <= last) {
-                    const int t = t0 + gl;
-                    Triplet tr;
-                    const bool act = t <= last && lanes_test(P, t, sp.curvature_limit_stiffness,
-                                                             sp.curvature_limit_safety_margin, tr);
-                    const uint32_t bits = LPF == 32 ? __ballot_sync(gmask, act)
-                                                    : (__ballot_sync(gmask, act) >> (group * LPF)) & ((1u << LPF) - 1u);
-                    if (bits == 0) {
-                        t0 += LPF;
-                        continue;
+            bool done = mine == TGL_NONE || sp.curvature_cleanup_sweeps == 0;
+            bool forward = true, moved = false;
+            uint32_t sweep = 0;
+            int t0 = 0;
+            while (__any_sync(FULL, !done)) {
+                Triplet tr;
+                const int t = forward ? t0 + gl : t0 - gl;
+                const bool act = !done && (forward ? t <= last : t >= 0) &&
+                                 lanes_test(P, t, sp.curvature_limit_stiffness, sp.curvature_limit_safety_margin, tr);
+                const uint32_t ballot = __ballot_sync(FULL, act);
+                const uint32_t bits = LPF == 32 ? ballot : (ballot >> (group * LPF)) & ((1u << LPF) - 1u);
+                if (!done) {
+                    if (bits) {
+                        const int first = __ffs(bits) - 1;
+                        if (gl == first) lanes_apply(P, t, tr, extent, g);
+                        moved = true;
+                        t0 = forward ? t0 + first + 1 : t0 - first - 1;
+                    } else {
+                        t0 = forward ? t0 + LPF : t0 - LPF;
                     }
-                    moved = true;
-                    const int first = __ffs(bits) - 1;
-                    if (gl == first) lanes_apply(P, t, tr, extent, g);
-                    __syncwarp(gmask);
-                    t0 += first + 1;
-                }
-                if (!moved) break;
-                moved = false;
-                t0 = last;
-                while (t0 >= 0) {
-                    const int t = t0 - gl;
-                    Triplet tr;
-                    const bool act = t >= 0 && lanes_test(P, t, sp.curvature_limit_stiffness,
-                                                          sp.curvature_limit_safety_margin, tr);
-                    const uint32_t bits = LPF == 32 ? __ballot_sync(gmask, act)
-                                                    : (__ballot_sync(gmask, act) >> (group * LPF)) & ((1u << LPF) - 1u);
-                    if (bits == 0) {
-                        t0 -= LPF;
-                        continue;
+                    if (forward ? t0 > last : t0 < 0) {  // the pass is over
+                        if (!moved) {
+                            done = true;
+                        } else if (forward) {
+                            forward = false;
+                            moved = false;
+                            t0 = last;
+                        } else {
+                            moved = false;
+                            forward = true;
+                            t0 = 0;
+                            done = ++sweep >= sp.curvature_cleanup_sweeps;
+                        }
                     }
-                    moved = true;
-                    const int first = __ffs(bits) - 1;
-                    if (gl == first) lanes_apply(P, t, tr, extent, g);
-                    __syncwarp(gmask);
-                    t0 -= first + 1;
                 }
-                if (!moved) break;
+                __syncwarp();
             }
         }
         __syncwarp();
