@@ -211,6 +211,108 @@ int tgl_capture_contacts(tgl_world *world, float maximum_surface_gap, uint32_t c
                          float *coordinates, float *surface_gaps, float *crossing_angles, uint32_t *count,
                          uint32_t *overflow);
 
+/* ---- Formation hooks (single worlds; an arena returns TGL_ERR_UNSUPPORTED). */
+
+/* DeviceFiberWorld::activate_formation_step (world.rs:2139-2183;
+ * kernels.rs:164-221; plugin.rs:783-795) with the step comparison done by
+ * the caller: active[f] != 0 makes fiber f take part in every later kernel
+ * (cell list, contact pass, update, measurements), 0 freezes it where it is.
+ * A world starts with every fiber active. Requests a neighbor-list rebuild;
+ * writes the active segment and vertex counts. */
+int tgl_world_set_active_fibers(tgl_world *world, const uint8_t *active, uint64_t fiber_count,
+                                uint32_t *active_segments, uint32_t *active_vertices);
+
+/* A persistent formation layer target (apply_layer_targets /
+ * apply_single_layer_target, world.rs:1723-1804; kernels.rs:538-581): each
+ * active fiber whose layer lies in [first_layer, last_layer] and below
+ * `count` moves along `axis` so that its mean coordinate approaches
+ * targets[layer] by `stiffness` (in (0, 1]), at most `max_translation`
+ * (> 0) per application; applied once at once when `apply_now` is 1, and at
+ * the end of every update step until cleared. fiber_layers[f] is fiber f's
+ * layer, 0xFFFFFFFF for none. */
+typedef struct {
+    uint32_t axis;
+    uint32_t count;
+    const float *targets;
+    const uint32_t *fiber_layers;
+    uint32_t first_layer;
+    uint32_t last_layer;
+    float stiffness;
+    float max_translation;
+    uint32_t apply_now;
+    uint32_t reserved;
+} tgl_layer_targets;
+
+/* Installs (targets != NULL) or clears (NULL; clear_layer_targets,
+ * world.rs:1806-1810) the layer target. */
+int tgl_world_set_layer_targets(tgl_world *world, const tgl_layer_targets *targets);
+
+/* Persistent vertex displacement targets (apply_vertex_displacement_targets,
+ * world.rs:1811-1859; kernels.rs:583-634): each listed vertex (distinct
+ * indices) gets the target coordinate = its current coordinate along `axis`
+ * + `displacement` (finite, non-zero), and at the end of every update step
+ * its coordinate is set to a commanded value that advances toward the target
+ * by `stiffness` (in (0, 1]), at most `max_translation` (> 0) per step. With
+ * `coordinates` and `command_coordinates` given (a restore), those are the
+ * targets and commands instead. */
+typedef struct {
+    uint32_t axis;
+    uint32_t count;
+    const uint32_t *vertices;
+    float displacement;
+    float stiffness;
+    float max_translation;
+    uint32_t reserved;
+    const float *coordinates;
+    const float *command_coordinates;
+} tgl_vertex_targets;
+
+/* Installs (targets != NULL) or clears (NULL; clear_vertex_targets,
+ * world.rs:1861-1863) the vertex targets. */
+int tgl_world_set_vertex_targets(tgl_world *world, const tgl_vertex_targets *targets);
+
+/* The installed vertex targets' target and commanded coordinates (count ==
+ * the installed count), for a checkpoint (world.rs:260-279). */
+int tgl_world_vertex_target_state(tgl_world *world, float *coordinates, float *command_coordinates, uint32_t count);
+
+/* formation_target_error (world.rs:1865-1929): the largest distance of an
+ * active targeted fiber's centre from its layer target, and of an active
+ * targeted vertex from its target; has_layer / has_vertex say which targets
+ * are installed (the error is 0 when not). */
+int tgl_world_target_errors(tgl_world *world, float *layer_error, uint32_t *has_layer, float *vertex_error,
+                            uint32_t *has_vertex);
+
+/* compact_cell (world.rs:1931-2054; kernels.rs:712-818): the cell shrinks
+ * to [new_lower, new_upper] (inside the current cell, every edge above two
+ * largest radii) and the active fibers follow by `kinematics`: 0 rigid fiber
+ * centres (each fiber keeps its centre's fractional position), 1 moving
+ * walls (vertices projected inside the new walls, the projection recorded
+ * as wall reactions), 2 affine (every vertex scaled with the cell). The grid
+ * keeps its cell size with fewer cells; a list rebuild is requested. */
+int tgl_world_compact_cell(tgl_world *world, const float new_lower[3], const float new_upper[3],
+                           uint32_t kinematics);
+
+/* cell_bounds (world.rs:2133-2137). */
+int tgl_world_cell_bounds(tgl_world *world, float lower[3], float upper[3]);
+
+/* compaction_metrics + wall_face_pressures (world.rs:2056-2131;
+ * kernels.rs:820-923) for the last batch's state: out[0..3] pressure per
+ * axis, out[3] contact, out[4] stretch, out[5] bending, out[6] total penalty
+ * energy, out[7..13] lower/upper face pressure per axis. stiffness = {contact,
+ * stretch, bending} (each >= 0); correction_fraction > 0. The sums run in
+ * f64 in a fixed order over the reference's f32 terms. */
+int tgl_world_compaction_metrics(tgl_world *world, float correction_fraction, const float stiffness[3],
+                                 float out[13]);
+
+/* The wall reactions of the last update step (interleaved xyz, len == 3V),
+ * and their replacement (a restore, world.rs:693-712). */
+int tgl_world_wall_reactions(tgl_world *world, float *xyz, size_t len);
+int tgl_world_set_wall_reactions(tgl_world *world, const float *xyz, size_t len);
+
+/* set_fiber_maximum_curvatures (world.rs:2185-2194): every vertex of fiber f
+ * (its ends included) takes the limit values[f] (1 / length; 0 = none). */
+int tgl_world_set_fiber_max_curvatures(tgl_world *world, const float *values, size_t count);
+
 /* Parity taps (no reference counterpart beyond its tests' readbacks,
  * world_tests.rs:1342-1363). Forces a neighbor-list rebuild from the current
  * positions now. */

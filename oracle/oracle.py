@@ -15,14 +15,20 @@ from typing import Optional
 
 import numpy as np
 
+from tangle_b200.formation import FormationHooks
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 _lib = None
 
 
 def build(force: bool = False) -> str:
-    """Compiles liboracle.so with the committed Makefile."""
-    if force or not os.path.exists(_LIB_PATH):
+    """Compiles liboracle.so with the committed Makefile (when missing or
+    older than its sources)."""
+    sources = [os.path.join(_HERE, name) for name in ("relax_oracle.cpp", "relax_oracle.h", "Makefile")]
+    stale = not os.path.exists(_LIB_PATH) or any(
+        os.path.exists(p) and os.path.getmtime(p) > os.path.getmtime(_LIB_PATH) for p in sources)
+    if force or stale:
         subprocess.run(["make", "-C", _HERE, "CXX=g++"], check=True, capture_output=True)
     return _LIB_PATH
 
@@ -123,6 +129,20 @@ def _load():
     lib.orc_debug_neighbor_lists.argtypes = [P, P, P]
     lib.orc_debug_corrections.argtypes = [P, ctypes.POINTER(_Config), P, P]
     lib.orc_debug_rebuild.argtypes = [P]
+    lib.orc_set_active_fibers.argtypes = [P, P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32),
+                                          ctypes.POINTER(ctypes.c_uint32)]
+    lib.orc_set_layer_targets.argtypes = [P, ctypes.c_uint32, P, ctypes.c_uint32, P, ctypes.c_uint32,
+                                          ctypes.c_uint32, ctypes.c_float, ctypes.c_float, ctypes.c_int]
+    lib.orc_set_vertex_targets.argtypes = [P, ctypes.c_uint32, P, ctypes.c_uint32, ctypes.c_float, ctypes.c_float,
+                                           ctypes.c_float]
+    lib.orc_vertex_target_state.argtypes = [P, P, P, ctypes.c_uint32]
+    lib.orc_target_errors.argtypes = [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32),
+                                      ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32)]
+    lib.orc_compact_cell.argtypes = [P, P, P, ctypes.c_uint32]
+    lib.orc_cell_bounds.argtypes = [P, P, P]
+    lib.orc_compaction_metrics.argtypes = [P, ctypes.c_float, P, P]
+    lib.orc_wall_reactions.argtypes = [P, P, ctypes.c_size_t]
+    lib.orc_set_fiber_max_curvatures.argtypes = [P, P, ctypes.c_size_t]
     lib.orc_last_error.restype = ctypes.c_char_p
     _lib = lib
     return lib
@@ -136,8 +156,9 @@ def _ptr(array: Optional[np.ndarray]):
     return None if array is None else array.ctypes.data_as(ctypes.c_void_p)
 
 
-class OracleWorld:
-    """The oracle's resident world: upload, run_batch, download."""
+class OracleWorld(FormationHooks):
+    """The oracle's resident world: upload, run_batch, download, and the
+    formation hooks of tangle_b200.formation."""
 
     def __init__(self, packed, cell_list=None, max_step: float = 0.006):
         from tangle_b200.settings import CellListConfig
@@ -178,9 +199,75 @@ class OracleWorld:
             raise ValueError(lib.orc_last_error().decode())
         self._handle = handle
         self._lib = lib
+        self._packed = packed
         self.vertex_count = packed.vertex_count
         self.segment_count = packed.segment_count
         self._keep = None
+        if not np.all(np.asarray(packed.fiber_active)):
+            self.set_active_fibers(np.asarray(packed.fiber_active))
+
+    def _call(self, rc: int) -> None:
+        if rc:
+            raise ValueError(self._lib.orc_last_error().decode())
+
+    # ---- formation hooks (tangle_b200.formation.FormationHooks)
+
+    def _fh_set_active(self, flags):
+        segments, vertices = ctypes.c_uint32(), ctypes.c_uint32()
+        self._call(self._lib.orc_set_active_fibers(self._handle, _ptr(flags), flags.size, ctypes.byref(segments),
+                                                   ctypes.byref(vertices)))
+        return int(segments.value), int(vertices.value)
+
+    def _fh_set_layer_targets(self, axis, targets, layers, first, last, stiffness, max_translation, apply_now):
+        count = 0 if targets is None else targets.size
+        self._call(self._lib.orc_set_layer_targets(self._handle, axis, _ptr(targets), count, _ptr(layers), first, last,
+                                                   stiffness, max_translation, 1 if apply_now else 0))
+
+    def _fh_set_vertex_targets(self, axis, indices, displacement, stiffness, max_translation, coordinates, commands):
+        if coordinates is not None:
+            raise ValueError("the oracle installs vertex targets from the positions only")
+        count = 0 if indices is None else indices.size
+        self._call(self._lib.orc_set_vertex_targets(self._handle, axis, _ptr(indices), count, displacement, stiffness,
+                                                    max_translation))
+
+    def _fh_vertex_target_state(self, count):
+        coordinates = np.empty(count, dtype=np.float32)
+        commands = np.empty(count, dtype=np.float32)
+        self._call(self._lib.orc_vertex_target_state(self._handle, _ptr(coordinates), _ptr(commands), count))
+        return coordinates, commands
+
+    def _fh_target_errors(self):
+        layer, vertex = ctypes.c_float(), ctypes.c_float()
+        has_layer, has_vertex = ctypes.c_uint32(), ctypes.c_uint32()
+        self._call(self._lib.orc_target_errors(self._handle, ctypes.byref(layer), ctypes.byref(has_layer),
+                                               ctypes.byref(vertex), ctypes.byref(has_vertex)))
+        return float(layer.value), bool(has_layer.value), float(vertex.value), bool(has_vertex.value)
+
+    def _fh_compact(self, lower, upper, kinematics):
+        self._call(self._lib.orc_compact_cell(self._handle, _ptr(lower), _ptr(upper), kinematics))
+
+    def _fh_cell_bounds(self):
+        lower = np.empty(3, dtype=np.float32)
+        upper = np.empty(3, dtype=np.float32)
+        self._call(self._lib.orc_cell_bounds(self._handle, _ptr(lower), _ptr(upper)))
+        return lower, upper
+
+    def _fh_metrics(self, correction_fraction, stiffness):
+        out = np.empty(13, dtype=np.float32)
+        self._call(self._lib.orc_compaction_metrics(self._handle, ctypes.c_float(correction_fraction), _ptr(stiffness),
+                                                    _ptr(out)))
+        return out
+
+    def _fh_wall_reactions(self):
+        out = np.empty(3 * self.vertex_count, dtype=np.float32)
+        self._call(self._lib.orc_wall_reactions(self._handle, _ptr(out), out.size))
+        return out
+
+    def _fh_set_wall_reactions(self, xyz):
+        raise ValueError("the oracle does not restore wall reactions")
+
+    def _fh_set_fiber_curvatures(self, values):
+        self._call(self._lib.orc_set_fiber_max_curvatures(self._handle, _ptr(values), values.size))
 
     def close(self):
         if getattr(self, "_handle", None):

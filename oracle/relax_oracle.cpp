@@ -245,6 +245,26 @@ struct orc_world {
         wall_reactions;
     /* Curvature triplets that moved a vertex (a diagnostic count). */
     uint64_t projections = 0;
+    /* Staged activation (kernels.rs:164-221; world.rs:2139-2183): the
+     * segment_active / vertex_active masks, derived per fiber, and the
+     * active segment count (the cell list's slots). */
+    std::vector<uint8_t> fiber_on, segment_on, vertex_on;
+    std::vector<uint32_t> vertex_fiber;
+    uint32_t slots = 0;
+    uint64_t allocated_cells = 0;
+    float maximum_radius = 0.0f;
+    /* Formation layer target (world.rs:1723-1810) and vertex targets
+     * (world.rs:1811-1863). */
+    bool layer_on = false;
+    uint32_t layer_axis = 0, layer_first = 0, layer_last = 0;
+    float layer_stiffness = 0.0f, layer_max_translation = 0.0f;
+    std::vector<float> layer_targets;
+    std::vector<uint32_t> fiber_layers;
+    bool targets_on = false;
+    uint32_t target_axis = 0;
+    float target_stiffness = 0.0f, target_max_translation = 0.0f;
+    std::vector<uint32_t> target_vertices;
+    std::vector<float> target_coordinates, command_coordinates;
 };
 
 namespace {
@@ -299,6 +319,8 @@ int size_world(orc_world &w, const orc_cell_list_config &cl, float max_step) {
     uint64_t total = std::max<uint64_t>(w.S, 1);
     w.neighbor_block = (uint32_t)std::min<uint64_t>(cl.neighbor_capacity,
                                                     std::min<uint64_t>(w.neighbor_slots / total, 0xFFFFFFFFull));
+    w.allocated_cells = cell_count;
+    w.maximum_radius = maximum_radius;
     w.cell_counts.assign(cell_count, 0);
     w.cell_offsets.assign(cell_count, 0);
     w.cell_segments.assign(w.S, 0);
@@ -316,19 +338,23 @@ void build_cell_list(orc_world &w) {
     std::vector<uint32_t> cell_of(w.S);
 #pragma omp parallel for schedule(static)
     for (int64_t s = 0; s < (int64_t)w.S; ++s) {
+        if (!w.segment_on[s]) continue; /* inactive segments stay out of the cell list */
         uint32_t first = w.segment_vertices[2 * s], second = w.segment_vertices[2 * s + 1];
         const float *p = &w.positions[3 * first];
         const float *q = &w.positions[3 * second];
         cell_of[s] = proxy_cell(p[0], p[1], p[2], q[0], q[1], q[2], w.grid);
     }
-    for (uint32_t s = 0; s < w.S; ++s) w.cell_counts[cell_of[s]] += 1;
+    for (uint32_t s = 0; s < w.S; ++s)
+        if (w.segment_on[s]) w.cell_counts[cell_of[s]] += 1;
     uint32_t running = 0;
     for (size_t c = 0; c < w.cell_counts.size(); ++c) {
         w.cell_offsets[c] = running;
         running += w.cell_counts[c];
     }
+    w.slots = running;
     std::vector<uint32_t> cursor(w.cell_counts.size(), 0);
     for (uint32_t s = 0; s < w.S; ++s) {
+        if (!w.segment_on[s]) continue;
         uint32_t c = cell_of[s];
         w.cell_segments[w.cell_offsets[c] + cursor[c]++] = s;
     }
@@ -347,7 +373,7 @@ void build_neighbor_lists(orc_world &w) {
     {
         std::vector<uint32_t> found;
 #pragma omp for schedule(dynamic, 256)
-        for (int64_t slot = 0; slot < (int64_t)w.S; ++slot) {
+        for (int64_t slot = 0; slot < (int64_t)w.slots; ++slot) {
             uint32_t segment = w.cell_segments[slot];
             uint32_t first_vertex = w.segment_vertices[2 * segment];
             uint32_t second_vertex = w.segment_vertices[2 * segment + 1];
@@ -434,6 +460,7 @@ void flag_neighbor_list_displacement(orc_world &w) {
     uint32_t flag = 0;
 #pragma omp parallel for schedule(static) reduction(| : flag)
     for (int64_t v = 0; v < (int64_t)w.V; ++v) {
+        if (!w.vertex_on[v]) continue;
         float dx = w.positions[3 * v] - w.reference_positions[3 * v];
         float dy = w.positions[3 * v + 1] - w.reference_positions[3 * v + 1];
         float dz = w.positions[3 * v + 2] - w.reference_positions[3 * v + 2];
@@ -451,6 +478,7 @@ void find_segment_corrections(orc_world &w, float correction_fraction, uint32_t 
 #pragma omp parallel for schedule(dynamic, 256)
     for (int64_t si = 0; si < (int64_t)w.S; ++si) {
         const uint32_t segment = (uint32_t)si;
+        if (!w.segment_on[segment]) continue; /* active_segments only (contact.rs:268-272) */
         uint32_t first_vertex = w.segment_vertices[2 * segment];
         uint32_t second_vertex = w.segment_vertices[2 * segment + 1];
         float p1x = w.positions[3 * first_vertex], p1y = w.positions[3 * first_vertex + 1],
@@ -694,6 +722,7 @@ void measure_curvature_ratio(orc_world &w) {
 #pragma omp parallel for schedule(static)
     for (int64_t vi = 0; vi < (int64_t)w.V; ++vi) {
         uint32_t index = (uint32_t)vi;
+        if (!w.vertex_on[index]) continue; /* inactive vertices keep their last ratio */
         float maximum = w.max_curvature[index];
         float ratio = 0.0f;
         uint32_t previous_segment = w.vertex_segments[2 * index];
@@ -727,8 +756,10 @@ void measure_curvature_ratio(orc_world &w) {
 /* kernels.rs:95-162: atomic u32 max of non-negative f32 bits, then the gate. */
 void reduce_and_assess(orc_world &w, const orc_relax_config &config, uint32_t max_iterations) {
     uint32_t reduced[3] = {0, 0, 0};
-    for (uint32_t s = 0; s < w.S; ++s) reduced[0] = std::max(reduced[0], f32_bits(std::fmax(w.segment_max[s], 0.0f)));
+    for (uint32_t s = 0; s < w.S; ++s)
+        if (w.segment_on[s]) reduced[0] = std::max(reduced[0], f32_bits(std::fmax(w.segment_max[s], 0.0f)));
     for (uint32_t v = 0; v < w.V; ++v) {
+        if (!w.vertex_on[v]) continue;
         reduced[1] = std::max(reduced[1], f32_bits(std::fmax(w.vertex_step[v], 0.0f)));
         reduced[2] = std::max(reduced[2], f32_bits(std::fmax(w.curvature_ratio[v], 0.0f)));
     }
@@ -757,6 +788,7 @@ void internal_pass(orc_world &w, float stretch_stiffness, float bend_stiffness) 
     for (int64_t vi = 0; vi < (int64_t)w.V; ++vi) {
         uint32_t index = (uint32_t)vi;
         float *out = &w.internal[3 * (size_t)index];
+        if (!w.vertex_on[index]) continue;
         if (w.pinned[index]) {
             out[0] = out[1] = out[2] = 0.0f;
             continue;
@@ -809,7 +841,7 @@ void internal_pass(orc_world &w, float stretch_stiffness, float bend_stiffness) 
 #pragma omp parallel for schedule(static)
     for (int64_t vi = 0; vi < (int64_t)w.V; ++vi) {
         uint32_t index = (uint32_t)vi;
-        if (w.pinned[index]) continue;
+        if (!w.vertex_on[index] || w.pinned[index]) continue;
         for (int axis = 0; axis < 3; ++axis) {
             size_t coordinate = 3 * (size_t)index + axis;
             float radius = w.wall_extents[coordinate];
@@ -827,6 +859,7 @@ void apply_contact_corrections(orc_world &w, float max_step) {
 #pragma omp parallel for schedule(static)
     for (int64_t vi = 0; vi < (int64_t)w.V; ++vi) {
         uint32_t index = (uint32_t)vi;
+        if (!w.vertex_on[index]) continue;
         if (w.pinned[index]) {
             w.vertex_step[index] = 0.0f;
             continue;
@@ -937,7 +970,7 @@ void project_fiber_curvature(orc_world &w, uint32_t sweeps, float stiffness, flo
     for (int64_t fi = 0; fi < (int64_t)w.F; ++fi) {
         uint32_t start = w.fiber_vertex_spans[2 * fi];
         uint32_t count = w.fiber_vertex_spans[2 * fi + 1];
-        if (count < 3) continue;
+        if (count < 3 || !w.fiber_on[fi]) continue;
         for (uint32_t sweep = 0; sweep < sweeps; ++sweep) {
             for (uint32_t local = 2; local < count; ++local) {
                 uint32_t vertex = start + local;
@@ -1031,6 +1064,14 @@ int orc_world_create(const orc_packed *pk, const orc_cell_list_config *cl, float
         delete w;
         return 1;
     }
+    /* packed.rs:289-303: every segment and vertex starts active. */
+    w->fiber_on.assign(w->F, 1);
+    w->segment_on.assign(w->S, 1);
+    w->vertex_on.assign(w->V, 1);
+    w->vertex_fiber.assign(w->V, 0);
+    for (uint32_t f = 0; f < w->F; ++f)
+        for (uint32_t k = 0; k < w->fiber_vertex_spans[2 * f + 1]; ++k) w->vertex_fiber[w->fiber_vertex_spans[2 * f] + k] = f;
+    w->slots = w->S;
     w->metrics[0] = std::numeric_limits<float>::infinity();
     w->metrics[1] = 0.0f;
     w->metrics[2] = std::numeric_limits<float>::infinity();
@@ -1057,6 +1098,7 @@ void apply_rigid_contact_corrections(orc_world &w, float max_step) {
     const int64_t F = (int64_t)w.fiber_vertex_spans.size() / 2;
 #pragma omp parallel for schedule(static)
     for (int64_t f = 0; f < F; ++f) {
+        if (!w.fiber_on[f]) continue;
         const uint32_t s0 = w.fiber_segment_spans[2 * f], m = w.fiber_segment_spans[2 * f + 1];
         const uint32_t v0 = w.fiber_vertex_spans[2 * f], n = w.fiber_vertex_spans[2 * f + 1];
         float tx = 0.0f, ty = 0.0f, tz = 0.0f, deepest_squared = 0.0f;
@@ -1109,6 +1151,40 @@ void apply_rigid_contact_corrections(orc_world &w, float max_step) {
     }
 }
 
+/* apply_formation_layer_targets (kernels.rs:538-581): every active fiber
+ * whose layer the target range covers moves along the axis by its centre's
+ * capped, stiffness-scaled distance to the layer target. */
+static void apply_layer_targets(orc_world &w) {
+    if (!w.layer_on) return;
+    for (uint32_t f = 0; f < w.F; ++f) {
+        const uint32_t layer = w.fiber_layers[f];
+        if (layer == NONE || layer >= w.layer_targets.size() || layer < w.layer_first || layer > w.layer_last) continue;
+        const uint32_t start = w.fiber_vertex_spans[2 * f], count = w.fiber_vertex_spans[2 * f + 1];
+        if (count == 0 || !w.vertex_on[start]) continue;
+        float center = 0.0f;
+        for (uint32_t local = 0; local < count; ++local) center += w.positions[3 * (size_t)(start + local) + w.layer_axis];
+        center /= (float)count;
+        const float translation = clampf((w.layer_targets[layer] - center) * w.layer_stiffness,
+                                         -w.layer_max_translation, w.layer_max_translation);
+        for (uint32_t local = 0; local < count; ++local)
+            w.positions[3 * (size_t)(start + local) + w.layer_axis] += translation;
+    }
+}
+
+/* apply_vertex_targets (kernels.rs:604-634). */
+static void apply_vertex_targets(orc_world &w) {
+    if (!w.targets_on) return;
+    for (size_t k = 0; k < w.target_vertices.size(); ++k) {
+        const uint32_t vertex = w.target_vertices[k];
+        if (!w.vertex_on[vertex]) continue;
+        const float command = w.command_coordinates[k];
+        const float translation = clampf((w.target_coordinates[k] - command) * w.target_stiffness,
+                                         -w.target_max_translation, w.target_max_translation);
+        w.command_coordinates[k] = command + translation;
+        w.positions[3 * (size_t)vertex + w.target_axis] = command + translation;
+    }
+}
+
 int orc_run_batch(orc_world *w, const orc_relax_config *config, uint32_t iterations, orc_batch_status *status) {
     if (!w || !config || !status) return fail("null argument");
     if (iterations == 0) return fail("iterations must be positive");
@@ -1133,6 +1209,9 @@ int orc_run_batch(orc_world *w, const orc_relax_config *config, uint32_t iterati
                 project_fiber_curvature(*w, config->curvature_cleanup_sweeps, config->curvature_limit_stiffness,
                                         config->curvature_limit_safety_margin);
             }
+            /* world.rs:1420-1447: the manufacturing targets after the mechanics. */
+            apply_layer_targets(*w);
+            apply_vertex_targets(*w);
         }
         flag_neighbor_list_displacement(*w);
     }
@@ -1201,6 +1280,278 @@ int orc_debug_corrections(orc_world *w, const orc_relax_config *config, float *c
 int orc_debug_rebuild(orc_world *w) {
     w->neighbor_state[0] = 1;
     rebuild_neighbor_lists_if_requested(*w);
+    return 0;
+}
+
+/* ---- Formation hooks (world.rs:1723-2194; kernels.rs:164-221, 538-923). */
+
+/* activate_formation_step (world.rs:2139-2183) with the step comparison done
+ * by the caller: the masks follow the fiber flags, and the lists are
+ * rebuilt before the next contact pass. */
+int orc_set_active_fibers(orc_world *w, const uint8_t *active, uint64_t fiber_count, uint32_t *active_segments,
+                          uint32_t *active_vertices) {
+    if (!w || !active || !active_segments || !active_vertices) return fail("null argument");
+    if (fiber_count != w->F) return fail("active flags need one entry per fiber");
+    for (uint32_t f = 0; f < w->F; ++f) w->fiber_on[f] = active[f] ? 1 : 0;
+    uint32_t segments = 0, vertices = 0;
+    for (uint32_t s = 0; s < w->S; ++s) segments += (w->segment_on[s] = w->fiber_on[w->segment_fibers[s]]);
+    for (uint32_t v = 0; v < w->V; ++v) vertices += (w->vertex_on[v] = w->fiber_on[w->vertex_fiber[v]]);
+    w->neighbor_state[0] = 1;
+    *active_segments = segments;
+    *active_vertices = vertices;
+    return 0;
+}
+
+/* apply_layer_target_range (world.rs:1758-1804), clear_layer_targets
+ * (:1806-1810) when targets is NULL. */
+int orc_set_layer_targets(orc_world *w, uint32_t axis, const float *targets, uint32_t count,
+                          const uint32_t *fiber_layers, uint32_t first_layer, uint32_t last_layer, float stiffness,
+                          float max_translation, int apply_now) {
+    if (!w) return fail("null argument");
+    if (!targets) {
+        w->layer_on = false;
+        return 0;
+    }
+    if (axis >= 3 || count == 0 || !fiber_layers) return fail("bad layer target");
+    if (!(stiffness > 0.0f && stiffness <= 1.0f) || !(max_translation > 0.0f)) return fail("bad layer target gains");
+    w->layer_on = true;
+    w->layer_axis = axis;
+    w->layer_targets.assign(targets, targets + count);
+    w->fiber_layers.assign(fiber_layers, fiber_layers + w->F);
+    w->layer_first = first_layer;
+    w->layer_last = last_layer;
+    w->layer_stiffness = stiffness;
+    w->layer_max_translation = max_translation;
+    if (apply_now) apply_layer_targets(*w); /* the immediate launch ignores the gate */
+    return 0;
+}
+
+/* apply_vertex_displacement_targets (world.rs:1811-1859) with
+ * initialize_vertex_displacement_targets (kernels.rs:583-602);
+ * clear_vertex_targets (:1861-1863) when vertices is NULL. */
+int orc_set_vertex_targets(orc_world *w, uint32_t axis, const uint32_t *vertices, uint32_t count, float displacement,
+                           float stiffness, float max_translation) {
+    if (!w) return fail("null argument");
+    if (!vertices) {
+        w->targets_on = false;
+        w->target_vertices.clear();
+        return 0;
+    }
+    if (axis >= 3 || count == 0) return fail("bad vertex target");
+    if (!(std::isfinite(displacement) && displacement != 0.0f)) return fail("displacement must be finite and non-zero");
+    if (!(stiffness > 0.0f && stiffness <= 1.0f) || !(max_translation > 0.0f)) return fail("bad vertex target gains");
+    for (uint32_t k = 0; k < count; ++k)
+        if (vertices[k] >= w->V) return fail("vertex target index out of range");
+    w->targets_on = true;
+    w->target_axis = axis;
+    w->target_stiffness = stiffness;
+    w->target_max_translation = max_translation;
+    w->target_vertices.assign(vertices, vertices + count);
+    w->target_coordinates.resize(count);
+    w->command_coordinates.resize(count);
+    for (uint32_t k = 0; k < count; ++k) {
+        const float coordinate = w->positions[3 * (size_t)vertices[k] + axis];
+        w->target_coordinates[k] = coordinate + displacement;
+        w->command_coordinates[k] = coordinate;
+    }
+    return 0;
+}
+
+int orc_vertex_target_state(const orc_world *w, float *coordinates, float *command_coordinates, uint32_t count) {
+    if (!w || !coordinates || !command_coordinates) return fail("null argument");
+    if (!w->targets_on || count != w->target_vertices.size()) return fail("count differs from the installed targets");
+    std::memcpy(coordinates, w->target_coordinates.data(), count * sizeof(float));
+    std::memcpy(command_coordinates, w->command_coordinates.data(), count * sizeof(float));
+    return 0;
+}
+
+/* measure_layer_target_error / measure_vertex_target_error (kernels.rs:
+ * 636-711): serial maxima from zero. */
+int orc_target_errors(const orc_world *w, float *layer_error, uint32_t *has_layer, float *vertex_error,
+                      uint32_t *has_vertex) {
+    if (!w || !layer_error || !has_layer || !vertex_error || !has_vertex) return fail("null argument");
+    *has_layer = w->layer_on ? 1 : 0;
+    *has_vertex = w->targets_on ? 1 : 0;
+    float maximum = 0.0f;
+    if (w->layer_on)
+        for (uint32_t f = 0; f < w->F; ++f) {
+            const uint32_t layer = w->fiber_layers[f];
+            if (layer == NONE || layer >= w->layer_targets.size() || layer < w->layer_first || layer > w->layer_last)
+                continue;
+            const uint32_t start = w->fiber_vertex_spans[2 * f], count = w->fiber_vertex_spans[2 * f + 1];
+            if (count == 0 || !w->vertex_on[start]) continue;
+            float center = 0.0f;
+            for (uint32_t local = 0; local < count; ++local)
+                center += w->positions[3 * (size_t)(start + local) + w->layer_axis];
+            center /= (float)count;
+            const float error = std::fabs(w->layer_targets[layer] - center);
+            if (error > maximum) maximum = error;
+        }
+    *layer_error = maximum;
+    maximum = 0.0f;
+    if (w->targets_on)
+        for (size_t k = 0; k < w->target_vertices.size(); ++k) {
+            const uint32_t vertex = w->target_vertices[k];
+            if (!w->vertex_on[vertex]) continue;
+            const float error = std::fabs(w->target_coordinates[k] - w->positions[3 * (size_t)vertex + w->target_axis]);
+            if (error > maximum) maximum = error;
+        }
+    *vertex_error = maximum;
+    return 0;
+}
+
+/* compact_cell (world.rs:1931-2054) with compact_rigid_fiber_centers,
+ * compact_moving_walls and compact_affine_vertices (kernels.rs:712-818):
+ * kinematics 0, 1, 2. */
+int orc_compact_cell(orc_world *w, const float new_lower[3], const float new_upper[3], uint32_t kinematics) {
+    if (!w || !new_lower || !new_upper) return fail("null argument");
+    if (kinematics > 2) return fail("kinematics must be 0, 1 or 2");
+    uint32_t cells[3];
+    uint64_t C = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (!std::isfinite(new_lower[a]) || !std::isfinite(new_upper[a])) return fail("bounds must be finite");
+        if (!(new_upper[a] - new_lower[a] > 2.0f * w->maximum_radius)) return fail("cell narrower than two radii");
+        if (!(new_lower[a] >= w->grid.lower[a]) || !(new_upper[a] <= w->grid.upper[a]))
+            return fail("compaction cannot grow the cell");
+        cells[a] = f32_to_u32(std::fmax(std::floor((new_upper[a] - new_lower[a]) / w->cell_size), 1.0f));
+        C *= cells[a];
+    }
+    if (C > w->allocated_cells) return fail("the compacted grid needs more cells than allocated");
+    const float *ol = w->grid.lower, *ou = w->grid.upper;
+    if (kinematics == 0) {
+        for (uint32_t f = 0; f < w->F; ++f) {
+            const uint32_t start = w->fiber_vertex_spans[2 * f], count = w->fiber_vertex_spans[2 * f + 1];
+            if (count == 0 || !w->vertex_on[start]) continue;
+            float c[3] = {0.0f, 0.0f, 0.0f};
+            for (uint32_t local = 0; local < count; ++local)
+                for (int a = 0; a < 3; ++a) c[a] += w->positions[3 * (size_t)(start + local) + a];
+            float d[3];
+            for (int a = 0; a < 3; ++a) {
+                c[a] /= (float)count;
+                const float fraction = (c[a] - ol[a]) / (ou[a] - ol[a]);
+                d[a] = new_lower[a] + fraction * (new_upper[a] - new_lower[a]) - c[a];
+            }
+            for (uint32_t local = 0; local < count; ++local)
+                for (int a = 0; a < 3; ++a) {
+                    w->positions[3 * (size_t)(start + local) + a] += d[a];
+                    w->wall_reactions[3 * (size_t)(start + local) + a] = 0.0f;
+                }
+        }
+    } else {
+        for (uint32_t v = 0; v < w->V; ++v) {
+            if (!w->vertex_on[v]) continue;
+            for (int a = 0; a < 3; ++a) {
+                const size_t c = 3 * (size_t)v + a;
+                if (kinematics == 2) {
+                    const float fraction = (w->positions[c] - ol[a]) / (ou[a] - ol[a]);
+                    w->positions[c] = new_lower[a] + fraction * (new_upper[a] - new_lower[a]);
+                    w->wall_reactions[c] = 0.0f;
+                } else if (!w->grid.periodic[a]) {
+                    const float previous = w->positions[c];
+                    const float projected =
+                        clampf(previous, new_lower[a] + w->wall_extents[c], new_upper[a] - w->wall_extents[c]);
+                    w->positions[c] = projected;
+                    w->wall_reactions[c] = previous - projected;
+                } else {
+                    w->wall_reactions[c] = 0.0f;
+                }
+            }
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        w->grid.lower[a] = new_lower[a];
+        w->grid.upper[a] = new_upper[a];
+    }
+    w->grid.cx = cells[0];
+    w->grid.cy = cells[1];
+    w->grid.cz = cells[2];
+    w->cell_counts.assign(C, 0);
+    w->cell_offsets.assign(C, 0);
+    w->neighbor_state[0] = 1;
+    return 0;
+}
+
+int orc_cell_bounds(const orc_world *w, float lower[3], float upper[3]) {
+    if (!w || !lower || !upper) return fail("null argument");
+    for (int a = 0; a < 3; ++a) {
+        lower[a] = w->grid.lower[a];
+        upper[a] = w->grid.upper[a];
+    }
+    return 0;
+}
+
+/* measure_compaction_metrics (kernels.rs:820-923), serial f32 as the
+ * reference sums; curvature ratios from the last gate's measurement. */
+int orc_compaction_metrics(const orc_world *w, float correction_fraction, const float stiffness[3], float out[13]) {
+    if (!w || !stiffness || !out) return fail("null argument");
+    if (!(correction_fraction > 0.0f)) return fail("correction_fraction must be positive");
+    const float contact_stiffness = stiffness[0], stretch_stiffness = stiffness[1], bending_stiffness = stiffness[2];
+    float load_x = 0.0f, load_y = 0.0f, load_z = 0.0f, contact_energy = 0.0f, stretch_energy = 0.0f;
+    for (uint32_t segment = 0; segment < w->S; ++segment) {
+        if (!w->segment_on[segment]) continue;
+        const float *c = &w->corrections[6 * (size_t)segment];
+        load_x += std::fabs(c[0]) + std::fabs(c[3]);
+        load_y += std::fabs(c[1]) + std::fabs(c[4]);
+        load_z += std::fabs(c[2]) + std::fabs(c[5]);
+        const float penetration = w->segment_max[segment];
+        contact_energy += 0.5f * contact_stiffness * penetration * penetration;
+        const uint32_t first = w->segment_vertices[2 * segment], second = w->segment_vertices[2 * segment + 1];
+        const float dx = w->positions[3 * second] - w->positions[3 * first];
+        const float dy = w->positions[3 * second + 1] - w->positions[3 * first + 1];
+        const float dz = w->positions[3 * second + 2] - w->positions[3 * first + 2];
+        const float length = std::sqrt(dx * dx + dy * dy + dz * dz);
+        const float rest = w->rest_lengths[segment];
+        if (rest > 1.0e-7f) {
+            const float extension = length - rest;
+            stretch_energy += 0.5f * stretch_stiffness * extension * extension / rest;
+        }
+    }
+    float bending_energy = 0.0f;
+    for (uint32_t v = 0; v < w->V; ++v) {
+        const float excess = std::fmax(w->curvature_ratio[v] - 1.0f, 0.0f);
+        bending_energy += 0.5f * bending_stiffness * excess * excess;
+    }
+    const float lx = w->grid.upper[0] - w->grid.lower[0], ly = w->grid.upper[1] - w->grid.lower[1],
+                lz = w->grid.upper[2] - w->grid.lower[2];
+    float face[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t v = 0; v < w->V; ++v)
+        for (int a = 0; a < 3; ++a) {
+            const float r = w->wall_reactions[3 * (size_t)v + a];
+            face[2 * a] += std::fmax(-r, 0.0f);
+            face[2 * a + 1] += std::fmax(r, 0.0f);
+        }
+    const float inverse_projection = 1.0f / std::fmax(correction_fraction, 1.0e-7f);
+    const float px = w->grid.periodic[0] ? load_x : face[0] + face[1];
+    const float py = w->grid.periodic[1] ? load_y : face[2] + face[3];
+    const float pz = w->grid.periodic[2] ? load_z : face[4] + face[5];
+    out[0] = contact_stiffness * px * inverse_projection / (ly * lz);
+    out[1] = contact_stiffness * py * inverse_projection / (lx * lz);
+    out[2] = contact_stiffness * pz * inverse_projection / (lx * ly);
+    out[3] = contact_energy;
+    out[4] = stretch_energy;
+    out[5] = bending_energy;
+    out[6] = contact_energy + stretch_energy + bending_energy;
+    out[7] = contact_stiffness * face[0] * inverse_projection / (ly * lz);
+    out[8] = contact_stiffness * face[1] * inverse_projection / (ly * lz);
+    out[9] = contact_stiffness * face[2] * inverse_projection / (lx * lz);
+    out[10] = contact_stiffness * face[3] * inverse_projection / (lx * lz);
+    out[11] = contact_stiffness * face[4] * inverse_projection / (lx * ly);
+    out[12] = contact_stiffness * face[5] * inverse_projection / (lx * ly);
+    return 0;
+}
+
+int orc_wall_reactions(const orc_world *w, float *xyz, size_t len) {
+    if (!w || !xyz) return fail("null argument");
+    if (len != w->wall_reactions.size()) return fail("reaction buffer has the wrong length");
+    std::memcpy(xyz, w->wall_reactions.data(), len * sizeof(float));
+    return 0;
+}
+
+/* set_fiber_maximum_curvatures (world.rs:2185-2194). */
+int orc_set_fiber_max_curvatures(orc_world *w, const float *values, size_t count) {
+    if (!w || !values) return fail("null argument");
+    if (count != w->F) return fail("one curvature limit per fiber");
+    for (uint32_t v = 0; v < w->V; ++v) w->max_curvature[v] = values[w->vertex_fiber[v]];
     return 0;
 }
 

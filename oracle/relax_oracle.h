@@ -128,6 +128,26 @@ int orc_debug_corrections(orc_world *world, const orc_relax_config *config,
                           float *corrections, float *segment_max_penetration);
 /* Forces a neighbor-list rebuild from the current positions now. */
 int orc_debug_rebuild(orc_world *world);
+/* Formation hooks (world.rs:1723-2194; kernels.rs:164-221, 538-923); the
+ * same meanings as the tgl_world_* functions of include/tangle_cuda.h. */
+int orc_set_active_fibers(orc_world *world, const uint8_t *active, uint64_t fiber_count,
+                          uint32_t *active_segments, uint32_t *active_vertices);
+int orc_set_layer_targets(orc_world *world, uint32_t axis, const float *targets, uint32_t count,
+                          const uint32_t *fiber_layers, uint32_t first_layer, uint32_t last_layer,
+                          float stiffness, float max_translation, int apply_now);
+int orc_set_vertex_targets(orc_world *world, uint32_t axis, const uint32_t *vertices, uint32_t count,
+                           float displacement, float stiffness, float max_translation);
+int orc_vertex_target_state(const orc_world *world, float *coordinates, float *command_coordinates,
+                            uint32_t count);
+int orc_target_errors(const orc_world *world, float *layer_error, uint32_t *has_layer,
+                      float *vertex_error, uint32_t *has_vertex);
+int orc_compact_cell(orc_world *world, const float new_lower[3], const float new_upper[3],
+                     uint32_t kinematics);
+int orc_cell_bounds(const orc_world *world, float lower[3], float upper[3]);
+int orc_compaction_metrics(const orc_world *world, float correction_fraction, const float stiffness[3],
+                           float out[13]);
+int orc_wall_reactions(const orc_world *world, float *xyz, size_t len);
+int orc_set_fiber_max_curvatures(orc_world *world, const float *values, size_t count);
 /* The f32 arc cosine the curvature projection uses (see relax_oracle.cpp). */
 float orc_acos_f32(float x);
 const char *orc_last_error(void);

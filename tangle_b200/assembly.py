@@ -16,7 +16,11 @@ uploads; it follows the reference's non-adaptive packing
 * vertex_max_curvature is 1/min_bend_radius (f64 reciprocal, cast to f32) on
   interior vertices only, 0 (unrestricted) elsewhere (packed.rs:260-270,
   crates/tangle_core/src/admissibility.rs:10-12);
-* pin_fiber_ends pins the first and last vertex of every fiber.
+* pin_fiber_ends pins the first and last vertex of every fiber;
+* fiber_formation_steps / fiber_formation_layers carry each fiber's
+  formation step (0 by default) and layer (0xFFFFFFFF for none), and
+  fiber_active which fibers take part (all of them by default; packed.rs:
+  201-210, 289-303).
 """
 
 from __future__ import annotations
@@ -107,6 +111,8 @@ class Fiber:
     intrinsic: np.ndarray  # (n, 3) f64
     radius: float
     min_bend_radius: Optional[float] = None
+    formation_step: int = 0  # recipe step that inserts the fiber (assembly.rs formation_step)
+    formation_layer: Optional[int] = None  # manufacturing layer (assembly.rs formation_layer)
 
 
 @dataclass
@@ -133,6 +139,21 @@ class FiberAssembly:
     @property
     def fiber_count(self) -> int:
         return len(self.fibers)
+
+    def set_fiber_formation_step(self, fiber: int, step: int) -> None:
+        """FiberAssembly::set_fiber_formation_step: the recipe step whose
+        activation inserts the fiber."""
+        step = int(step)
+        if not 0 <= step < NONE:
+            raise ValueError("formation step must fit in 32 bits")
+        self.fibers[fiber].formation_step = step
+
+    def set_fiber_formation_layer(self, fiber: int, layer: Optional[int]) -> None:
+        """FiberAssembly::set_fiber_formation_layer: the manufacturing layer
+        that layer targets address (None for none)."""
+        if layer is not None and not 0 <= int(layer) < NONE:
+            raise ValueError("formation layer must fit in 32 bits")
+        self.fibers[fiber].formation_layer = None if layer is None else int(layer)
 
     def smallest_diameter(self) -> Optional[float]:
         if not self.fibers:
@@ -161,6 +182,18 @@ class PackedAssembly:
     cell_lower: np.ndarray  # f32 [3]
     cell_upper: np.ndarray  # f32 [3]
     cell_periodic: np.ndarray  # u32 [3]
+    fiber_formation_steps: Optional[np.ndarray] = None  # u32 [F]
+    fiber_formation_layers: Optional[np.ndarray] = None  # u32 [F], NONE = no layer
+    fiber_active: Optional[np.ndarray] = None  # u32 [F], 1 = takes part
+
+    def __post_init__(self):
+        F = self.fiber_vertex_spans.size // 2
+        if self.fiber_formation_steps is None:
+            self.fiber_formation_steps = np.zeros(F, dtype=np.uint32)
+        if self.fiber_formation_layers is None:
+            self.fiber_formation_layers = np.full(F, NONE, dtype=np.uint32)
+        if self.fiber_active is None:
+            self.fiber_active = np.ones(F, dtype=np.uint32)
 
     @property
     def vertex_count(self) -> int:
@@ -245,6 +278,9 @@ class PackedAssembly:
             cell_lower=lower.astype(np.float32),
             cell_upper=upper.astype(np.float32),
             cell_periodic=np.array([1 if p else 0 for p in cell.periodic], dtype=np.uint32),
+            fiber_formation_steps=np.array([f.formation_step for f in assembly.fibers], dtype=np.uint32),
+            fiber_formation_layers=np.array(
+                [NONE if f.formation_layer is None else f.formation_layer for f in assembly.fibers], dtype=np.uint32),
         )
 
     def unpack_positions(self, positions: np.ndarray, assembly: FiberAssembly) -> None:

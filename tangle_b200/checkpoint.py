@@ -5,9 +5,11 @@ crates/tangle_python/src/checkpoint.rs for the plain relaxation path:
 
 * `CheckpointSettings` has the reference's fields, defaults and validation
   (checkpoint.rs:30-105);
-* a checkpoint holds the packed assembly with the current positions and the
-  lifetime iteration count (`DeviceWorldCheckpoint`, world.rs:280-304), plus
-  the recipe's progress, and is written atomically (a temporary file renamed
+* a checkpoint holds the packed assembly with the current positions, cell,
+  active fibers and curvature limits, the lifetime iteration count, the wall
+  reactions and the installed layer and vertex targets
+  (`DeviceWorldCheckpoint`, world.rs:280-304), plus the recipe's progress,
+  and is written atomically (a temporary file renamed
   over the target, lib.rs:379-420) behind an 8-byte magic and a schema
   number that a load checks, with the case id (lib.rs:347-377);
 * saves happen when the iteration count crosses a multiple of
@@ -30,9 +32,10 @@ from typing import Optional
 import numpy as np
 
 from .assembly import PackedAssembly
+from .formation import LayerTargetCheckpoint, VertexTargetCheckpoint
 
 MAGIC = b"TANGLEB2"
-SCHEMA = 1
+SCHEMA = 2
 
 _PACKED_FIELDS = [f.name for f in dataclasses.fields(PackedAssembly)]
 
@@ -47,6 +50,9 @@ class DeviceWorldCheckpoint:
 
     packed: PackedAssembly
     total_iterations: int
+    wall_reactions: Optional[np.ndarray] = None  # f32 [3V]
+    layer_target: Optional[LayerTargetCheckpoint] = None
+    vertex_target: Optional[VertexTargetCheckpoint] = None
 
 
 @dataclass
@@ -111,6 +117,21 @@ def encode(checkpoint: RunCheckpoint) -> bytes:
     arrays["case_id"] = np.frombuffer(checkpoint.case_id.encode("utf-8"), dtype=np.uint8)
     arrays["counters"] = np.array([checkpoint.device.total_iterations, checkpoint.operation,
                                    checkpoint.operation_iterations, int(checkpoint.converged)], dtype=np.uint64)
+    device = checkpoint.device
+    if device.wall_reactions is not None:
+        arrays["wall_reactions"] = np.asarray(device.wall_reactions, dtype=np.float32)
+    if device.layer_target is not None:
+        t = device.layer_target
+        arrays["layer_coordinates"] = np.asarray(t.coordinates, dtype=np.float32)
+        arrays["layer_ints"] = np.array([t.axis, t.first_layer, t.last_layer], dtype=np.uint32)
+        arrays["layer_gains"] = np.array([t.stiffness, t.max_translation], dtype=np.float32)
+    if device.vertex_target is not None:
+        t = device.vertex_target
+        arrays["vertex_indices"] = np.asarray(t.indices, dtype=np.uint32)
+        arrays["vertex_coordinates"] = np.asarray(t.coordinates, dtype=np.float32)
+        arrays["vertex_commands"] = np.asarray(t.command_coordinates, dtype=np.float32)
+        arrays["vertex_axis"] = np.array([t.axis], dtype=np.uint32)
+        arrays["vertex_gains"] = np.array([t.stiffness, t.max_translation], dtype=np.float32)
     body = io.BytesIO()
     np.savez(body, **arrays)
     return MAGIC + SCHEMA.to_bytes(4, "little") + body.getvalue()
@@ -128,7 +149,21 @@ def decode(data: bytes, case_id: str) -> RunCheckpoint:
             raise CheckpointError(f"checkpoint case mismatch: expected {case_id!r}, found {found!r}")
         packed = PackedAssembly(**{name: archive[f"packed_{name}"].copy() for name in _PACKED_FIELDS})
         total, operation, op_iterations, converged = (int(x) for x in archive["counters"])
-    return RunCheckpoint(found, DeviceWorldCheckpoint(packed, total), operation, op_iterations, bool(converged))
+        device = DeviceWorldCheckpoint(packed, total)
+        if "wall_reactions" in archive:
+            device.wall_reactions = archive["wall_reactions"].copy()
+        if "layer_coordinates" in archive:
+            axis, first, last = (int(x) for x in archive["layer_ints"])
+            stiffness, max_translation = (float(x) for x in archive["layer_gains"])
+            device.layer_target = LayerTargetCheckpoint(archive["layer_coordinates"].copy(), axis, first, last,
+                                                        stiffness, max_translation)
+        if "vertex_indices" in archive:
+            stiffness, max_translation = (float(x) for x in archive["vertex_gains"])
+            device.vertex_target = VertexTargetCheckpoint(archive["vertex_indices"].copy(),
+                                                          archive["vertex_coordinates"].copy(),
+                                                          archive["vertex_commands"].copy(),
+                                                          int(archive["vertex_axis"][0]), stiffness, max_translation)
+    return RunCheckpoint(found, device, operation, op_iterations, bool(converged))
 
 
 def save(path: Path, checkpoint: RunCheckpoint) -> int:

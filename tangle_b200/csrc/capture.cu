@@ -16,6 +16,7 @@ __global__ void capture_kernel(WorldDev w, float max_gap, uint32_t capacity, uin
     const float length_epsilon = 1.0e-20f, parallel_relative_epsilon = 1.0e-6f;
     for (uint32_t segment = blockIdx.x * blockDim.x + threadIdx.x; segment < w.S;
          segment += gridDim.x * blockDim.x) {
+        if (!segment_on(w, segment)) continue;
         const uint32_t v0 = w.seg_v0[segment];
         const float4 P1 = w.pos[v0], Q1 = w.pos[v0 + 1];
         const float p1x = P1.x, p1y = P1.y, p1z = P1.z, q1x = Q1.x, q1y = Q1.y, q1z = Q1.z;

@@ -17,6 +17,7 @@
 // (contacts summed in ascending list order); only maxima, which are exact in
 // any order, use atomics (on u32 bits of non-negative floats).
 #include "kernels.cuh"
+#include "formation.cuh"
 #include "contact.cuh"
 
 #include <algorithm>
@@ -94,13 +95,13 @@ __device__ inline bool contact_moved(const WorldDev &w, uint32_t v, float x, flo
     return dx * dx + dy * dy + dz * dz > limit * limit;
 }
 
-// neighbor.rs:446-465, over every vertex (all are active in the plain path),
-// and the same check against the contact lists' snapshot.
+// neighbor.rs:446-465, over the active vertices, and the same check
+// against the contact lists' snapshot.
 template <bool A>
 __global__ void flag_displacement_kernel(WorldDev w) {
     uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     bool far = false, contact_far = false;
-    if (v < w.V) {
+    if (v < w.V && (A || vertex_on(w, v))) {
         const uint32_t spec = spec_of_vtx<A>(w, v);
         float md = 0.5f * skin_of<A>(w, spec);
         float4 p = w.pos[v], r = w.ref_pos[v];
@@ -123,26 +124,6 @@ __global__ void request_rebuild_kernel(WorldDev w) {
     if (threadIdx.x == 0) w.ctl->neighbor_state[0] = 1;
 }
 
-// kernels.rs:925-980 at one interior vertex of a fiber whose positions are
-// p(local index).
-template <typename Fetch>
-__device__ inline float curvature_ratio_at(Fetch p, int i, float maximum) {
-    float4 a0 = p(i - 1), c = p(i), b1 = p(i + 1);
-    float ax = c.x - a0.x, ay = c.y - a0.y, az = c.z - a0.z;
-    float bx = b1.x - c.x, by = b1.y - c.y, bz = b1.z - c.z;
-    float first_length = sqrtf(ax * ax + ay * ay + az * az);
-    float second_length = sqrtf(bx * bx + by * by + bz * bz);
-    float ratio = 0.0f;
-    if (first_length > 1.0e-7f && second_length > 1.0e-7f) {
-        float cosine = (ax * bx + ay * by + az * bz) / (first_length * second_length);
-        cosine = clampf(cosine, -1.0f, 1.0f);
-        float dual_length = 0.5f * (first_length + second_length);
-        float curvature = 2.0f * sqrtf(0.5f * (1.0f - cosine)) / dual_length;
-        ratio = curvature / maximum;
-    }
-    return ratio;
-}
-
 // Gate inputs for the first step of a batch: curvature ratio of the current
 // positions and the last applied step (kernels.rs:112-127).
 template <bool A>
@@ -151,7 +132,8 @@ __global__ void measure_start_kernel(WorldDev w) {
     const int lane = threadIdx.x & 31;
     const int warps = blockDim.x >> 5;
     uint32_t cmax = 0, smax = 0;
-    for (uint32_t f = blockIdx.x * warps + (threadIdx.x >> 5); f < w.F; f += gridDim.x * warps) {
+    for (uint32_t k = blockIdx.x * warps + (threadIdx.x >> 5); k < w.FA; k += gridDim.x * warps) {
+        const uint32_t f = w.fiber_order[k];
         const uint32_t spec = spec_of_fiber<A>(w, f);
         if (A && ctl_of<A>(w, spec)->control[0] == 0) continue;
         uint2 span = w.fiber_vspan[f];
@@ -201,13 +183,15 @@ __global__ void rb_clear_kernel(WorldDev w) {
     if (blockIdx.x == 0 && threadIdx.x == 0) w.ctl->cell_overflow = 0;
 }
 
-// count_cell_segments: each segment's midpoint cell, and its arrival ticket.
+// count_cell_segments: each segment's midpoint cell, and its arrival ticket;
+// the segments of inactive fibers stay out of the cell list.
 template <bool A>
 __global__ void rb_count_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < w.S; s += gridDim.x * blockDim.x) {
         const uint32_t spec = spec_of_seg<A>(w, s);
         if (A && !rebuilding<A>(w, spec)) continue;
+        if (!A && !segment_on(w, s)) continue;
         float4 a = w.geom[2 * (size_t)s], b = w.geom[2 * (size_t)s + 1];
         uint32_t cell = cell_base_of<A>(w, spec) + proxy_cell(a.x, a.y, a.z, b.x, b.y, b.z, grid_of<A>(w, spec));
         w.cell_of[s] = cell;
@@ -275,7 +259,8 @@ template <bool A>
 __global__ void rb_scatter_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < w.S; s += gridDim.x * blockDim.x)
-        if (!A || rebuilding<A>(w, spec_of_seg<A>(w, s))) w.cell_segments[w.cell_offsets[w.cell_of[s]] + w.ticket[s]] = s;
+        if (A ? rebuilding<A>(w, spec_of_seg<A>(w, s)) : segment_on(w, s))
+            w.cell_segments[w.cell_offsets[w.cell_of[s]] + w.ticket[s]] = s;
 }
 
 // rank_cell_segments (cell_list.rs:392-434): ascending segment order inside
@@ -323,7 +308,7 @@ __global__ void rb_sort_cells_kernel(WorldDev w) {
 template <bool A>
 __global__ void rb_gather_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
-    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.S; slot += gridDim.x * blockDim.x) {
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.NS; slot += gridDim.x * blockDim.x) {
         uint32_t s = w.cell_segments[slot];
         if (A && !rebuilding<A>(w, spec_of_seg<A>(w, s))) continue;
         float4 a = w.geom[2 * (size_t)s], b = w.geom[2 * (size_t)s + 1];
@@ -723,10 +708,10 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x)
             w.contact_ref[v] = w.pos[v];
     }
-    for (uint32_t base = (blockIdx.x * CONTACT_WARPS + warp) * 32u; base < w.S; base += warps_total * 32u) {
+    for (uint32_t base = (blockIdx.x * CONTACT_WARPS + warp) * 32u; base < w.NS; base += warps_total * 32u) {
         // Batches follow the cell list's slot order, so the 32 segments of a
         // batch are spatial neighbors and share most of their candidates.
-        const bool in_range = base + lane < w.S;
+        const bool in_range = base + lane < w.NS;
         const uint32_t segment = in_range ? w.cell_segments[base + lane] : 0u;
         const uint32_t my_spec = A && in_range ? spec_of_seg<A>(w, segment) : 0u;
         // Segments of an arena specimen whose gate has stopped it are skipped.
@@ -1016,29 +1001,51 @@ __device__ inline float wall_clamp(float moved, float extent, int axis, const Gr
     return g.periodic[axis] ? moved : clampf(moved, g.lower[axis] + extent, g.upper[axis] - extent);
 }
 
+// wall_clamp that adds moved - kept to the vertex's wall reaction
+// (kernels.rs:1440-1451, :1277-1305; R null = no reactions kept). The
+// reference adds the difference after every projection; a zero difference
+// leaves its running sum unchanged (the sum starts at +0 and a sum of
+// differences is never -0), so only a clamp that moves a coordinate is
+// written, by the one lane that owns the vertex at that point.
+__device__ inline float wall_clamp_r(float moved, float extent, int axis, const Grid &g, float4 *R, int i) {
+    const float kept = wall_clamp(moved, extent, axis, g);
+    if (R != nullptr && !(kept == moved)) {
+        float4 r = R[i];
+        const float d = moved - kept;
+        if (axis == 0)
+            r.x += d;
+        else if (axis == 1)
+            r.y += d;
+        else
+            r.z += d;
+        R[i] = r;
+    }
+    return kept;
+}
+
 __device__ inline void curvature_triplet_apply(float4 *P, const float4 *St, int prev, int center, int next,
-                                               const Triplet &t, const Grid &g) {
+                                               const Triplet &t, const Grid &g, float4 *R) {
     float4 pp = P[prev], pc = P[center], pn = P[next];
     float pe = St[prev].w, ce = St[center].w, ne = St[next].w;
     float mp, mc, mn;
     mp = pp.x - t.pw * t.scale * t.gux;
     mc = pc.x + t.cw * t.scale * t.cgx;
     mn = pn.x + t.nw * t.scale * t.gvx;
-    if (t.pw > 0.0f) pp.x = wall_clamp(mp, pe, 0, g);
-    if (t.cw > 0.0f) pc.x = wall_clamp(mc, ce, 0, g);
-    if (t.nw > 0.0f) pn.x = wall_clamp(mn, ne, 0, g);
+    if (t.pw > 0.0f) pp.x = wall_clamp_r(mp, pe, 0, g, R, prev);
+    if (t.cw > 0.0f) pc.x = wall_clamp_r(mc, ce, 0, g, R, center);
+    if (t.nw > 0.0f) pn.x = wall_clamp_r(mn, ne, 0, g, R, next);
     mp = pp.y - t.pw * t.scale * t.guy;
     mc = pc.y + t.cw * t.scale * t.cgy;
     mn = pn.y + t.nw * t.scale * t.gvy;
-    if (t.pw > 0.0f) pp.y = wall_clamp(mp, pe, 1, g);
-    if (t.cw > 0.0f) pc.y = wall_clamp(mc, ce, 1, g);
-    if (t.nw > 0.0f) pn.y = wall_clamp(mn, ne, 1, g);
+    if (t.pw > 0.0f) pp.y = wall_clamp_r(mp, pe, 1, g, R, prev);
+    if (t.cw > 0.0f) pc.y = wall_clamp_r(mc, ce, 1, g, R, center);
+    if (t.nw > 0.0f) pn.y = wall_clamp_r(mn, ne, 1, g, R, next);
     mp = pp.z - t.pw * t.scale * t.guz;
     mc = pc.z + t.cw * t.scale * t.cgz;
     mn = pn.z + t.nw * t.scale * t.gvz;
-    if (t.pw > 0.0f) pp.z = wall_clamp(mp, pe, 2, g);
-    if (t.cw > 0.0f) pc.z = wall_clamp(mc, ce, 2, g);
-    if (t.nw > 0.0f) pn.z = wall_clamp(mn, ne, 2, g);
+    if (t.pw > 0.0f) pp.z = wall_clamp_r(mp, pe, 2, g, R, prev);
+    if (t.cw > 0.0f) pc.z = wall_clamp_r(mc, ce, 2, g, R, center);
+    if (t.nw > 0.0f) pn.z = wall_clamp_r(mn, ne, 2, g, R, next);
     P[prev] = pp;
     P[center] = pc;
     P[next] = pn;
@@ -1060,17 +1067,20 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
     bool far = false;
     bool contact_far = false;
     const bool contact_lists = w.contact_skin > 0.0f;
-    for (uint32_t f = blockIdx.x * warps + warp; f < w.F; f += gridDim.x * warps) {
+    for (uint32_t k = blockIdx.x * warps + warp; k < w.FA; k += gridDim.x * warps) {
+        const uint32_t f = w.fiber_order[k];
         const uint2 span = w.fiber_vspan[f];
         const uint32_t v0 = span.x;
         const int n = (int)span.y;
         const uint32_t s0 = w.fiber_s0[f];
         const float radius = w.seg_static[s0].x;
+        float4 *const R = w.reaction != nullptr ? w.reaction + v0 : nullptr;
         for (int i = lane; i < n; i += 32) {
             float4 p = w.pos[v0 + i];
             p.w = w.pinned[v0 + i] ? 1.0f : 0.0f;
             P[i] = p;
             St[i] = w.vtx_static[v0 + i];
+            if (R) R[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // clear_wall_reactions (kernels.rs:13-24)
         }
         __syncwarp();
         // find/apply_internal_corrections x constraint_iterations (Jacobi).
@@ -1132,9 +1142,9 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
                 if (x.w != 0.0f) continue;
                 float4 c = T[i];
                 float e = St[i].w;
-                x.x = wall_clamp(x.x + c.x, e, 0, g);
-                x.y = wall_clamp(x.y + c.y, e, 1, g);
-                x.z = wall_clamp(x.z + c.z, e, 2, g);
+                x.x = wall_clamp_r(x.x + c.x, e, 0, g, R, i);
+                x.y = wall_clamp_r(x.y + c.y, e, 1, g, R, i);
+                x.z = wall_clamp_r(x.z + c.z, e, 2, g, R, i);
                 P[i] = x;
             }
             __syncwarp();
@@ -1165,9 +1175,9 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
                     cz *= scale;
                 }
                 float e = St[i].w;
-                x.x = wall_clamp(x.x + cx, e, 0, g);
-                x.y = wall_clamp(x.y + cy, e, 1, g);
-                x.z = wall_clamp(x.z + cz, e, 2, g);
+                x.x = wall_clamp_r(x.x + cx, e, 0, g, R, i);
+                x.y = wall_clamp_r(x.y + cy, e, 1, g, R, i);
+                x.z = wall_clamp_r(x.z + cz, e, 2, g, R, i);
                 P[i] = x;
                 step = sqrtf(cx * cx + cy * cy + cz * cz);
             }
@@ -1201,7 +1211,7 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
                     }
                     moved = true;
                     int j = __ffs(ballot) - 1;
-                    if (lane == j) curvature_triplet_apply(P, St, t, t + 1, t + 2, tr, g);
+                    if (lane == j) curvature_triplet_apply(P, St, t, t + 1, t + 2, tr, g, R);
                     __syncwarp();
                     t0 += j + 1;
                 }
@@ -1221,7 +1231,7 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
                     }
                     moved = true;
                     int j = __ffs(ballot) - 1;
-                    if (lane == j) curvature_triplet_apply(P, St, t, t + 1, t + 2, tr, g);
+                    if (lane == j) curvature_triplet_apply(P, St, t, t + 1, t + 2, tr, g, R);
                     __syncwarp();
                     t0 -= j + 1;
                 }
@@ -1229,6 +1239,7 @@ __global__ void __launch_bounds__(256) fiber_kernel(WorldDev w, StepParams sp) {
             }
         }
         __syncwarp();
+        formation_targets_staged(w, f, P, n, v0, lane);
         // Write back; displacement check; next gate's curvature ratios;
         // geometry records for the next contact pass.
         for (int i = lane; i < n; i += 32) {
@@ -1331,23 +1342,23 @@ __device__ inline bool lanes_test(const float4 *P, int t, float stiffness, float
     return tr.pw > 0.0f || tr.cw > 0.0f || tr.nw > 0.0f;
 }
 
-__device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float extent, const Grid &g) {
+__device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float extent, const Grid &g, float4 *R) {
     const float4 pp = P[t], pc = P[t + 1], pn = P[t + 2];
     float4 a = pp, b = pc, c = pn;
     if (tr.pw > 0.0f) {
-        a.x = wall_clamp(pp.x - tr.pw * tr.scale * tr.gux, extent, 0, g);
-        a.y = wall_clamp(pp.y - tr.pw * tr.scale * tr.guy, extent, 1, g);
-        a.z = wall_clamp(pp.z - tr.pw * tr.scale * tr.guz, extent, 2, g);
+        a.x = wall_clamp_r(pp.x - tr.pw * tr.scale * tr.gux, extent, 0, g, R, t);
+        a.y = wall_clamp_r(pp.y - tr.pw * tr.scale * tr.guy, extent, 1, g, R, t);
+        a.z = wall_clamp_r(pp.z - tr.pw * tr.scale * tr.guz, extent, 2, g, R, t);
     }
     if (tr.cw > 0.0f) {
-        b.x = wall_clamp(pc.x + tr.cw * tr.scale * tr.cgx, extent, 0, g);
-        b.y = wall_clamp(pc.y + tr.cw * tr.scale * tr.cgy, extent, 1, g);
-        b.z = wall_clamp(pc.z + tr.cw * tr.scale * tr.cgz, extent, 2, g);
+        b.x = wall_clamp_r(pc.x + tr.cw * tr.scale * tr.cgx, extent, 0, g, R, t + 1);
+        b.y = wall_clamp_r(pc.y + tr.cw * tr.scale * tr.cgy, extent, 1, g, R, t + 1);
+        b.z = wall_clamp_r(pc.z + tr.cw * tr.scale * tr.cgz, extent, 2, g, R, t + 1);
     }
     if (tr.nw > 0.0f) {
-        c.x = wall_clamp(pn.x + tr.nw * tr.scale * tr.gvx, extent, 0, g);
-        c.y = wall_clamp(pn.y + tr.nw * tr.scale * tr.gvy, extent, 1, g);
-        c.z = wall_clamp(pn.z + tr.nw * tr.scale * tr.gvz, extent, 2, g);
+        c.x = wall_clamp_r(pn.x + tr.nw * tr.scale * tr.gvx, extent, 0, g, R, t + 2);
+        c.y = wall_clamp_r(pn.y + tr.nw * tr.scale * tr.gvy, extent, 1, g, R, t + 2);
+        c.z = wall_clamp_r(pn.z + tr.nw * tr.scale * tr.gvz, extent, 2, g, R, t + 2);
     }
     P[t] = a;
     P[t + 1] = b;
@@ -1369,7 +1380,9 @@ __device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float ex
 // In an arena (A) each fiber takes its specimen's grid and skin, fibers of
 // stopped specimens are skipped, and the maxima and flags go to each
 // fiber's specimen.
-template <int LPF, bool A = false>
+// FM compiles in the formation work (wall reactions, layer and vertex
+// targets); without it the kernel carries none of it.
+template <int LPF, bool A = false, bool FM = false>
 __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepParams sp, int stride) {
     constexpr int FPW = 32 / LPF;  // fibers per warp
     if (w.ctl->control[0] == 0) return;
@@ -1381,9 +1394,9 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
     bool far = false;
     bool contact_far = false;
     const bool contact_lists = !A && w.contact_skin > 0.0f;
-    for (uint32_t batch = blockIdx.x; batch * FPW < w.F; batch += gridDim.x) {
+    for (uint32_t batch = blockIdx.x; batch * FPW < w.FA; batch += gridDim.x) {
         const uint32_t slot = batch * FPW + group;
-        uint32_t mine = slot < w.F ? w.fiber_order[slot] : TGL_NONE;
+        uint32_t mine = slot < w.FA ? w.fiber_order[slot] : TGL_NONE;
         if (A && mine != TGL_NONE && ctl_of<A>(w, spec_of_fiber<A>(w, mine))->control[0] == 0) mine = TGL_NONE;
         for (int j = 0; j < FPW; ++j) {
             const uint32_t f = __shfl_sync(FULL, mine, j * LPF);
@@ -1396,12 +1409,14 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             const uint32_t s0 = w.fiber_s0[f];
             const float extent = w.seg_static[s0].x;
             float4 *P = lanes_smem + (size_t)j * stride;
+            float4 *const R = FM && w.reaction != nullptr ? w.reaction + v0 : nullptr;
             for (int i = lane; i < n; i += 32) {
                 float4 p = w.pos[v0 + i];
                 const float limit = w.vtx_static[v0 + i].x;
                 p.w = w.pinned[v0 + i] ? -limit : limit;
                 if (w.pinned[v0 + i] && limit == 0.0f) p.w = -0.0f;
                 P[i] = p;
+                if (R) R[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // clear_wall_reactions (kernels.rs:13-24)
             }
             __syncwarp();
             // find/apply_internal_corrections x constraint_iterations (Jacobi).
@@ -1471,9 +1486,9 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                     if (i < n) {
                         float4 x = P[i];
                         if (!lanes_pinned(x)) {
-                            x.x = wall_clamp(x.x + cxs[k], extent, 0, g);
-                            x.y = wall_clamp(x.y + cys[k], extent, 1, g);
-                            x.z = wall_clamp(x.z + czs[k], extent, 2, g);
+                            x.x = wall_clamp_r(x.x + cxs[k], extent, 0, g, R, i);
+                            x.y = wall_clamp_r(x.y + cys[k], extent, 1, g, R, i);
+                            x.z = wall_clamp_r(x.z + czs[k], extent, 2, g, R, i);
                             P[i] = x;
                         }
                     }
@@ -1505,9 +1520,9 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                         cy *= scale;
                         cz *= scale;
                     }
-                    x.x = wall_clamp(x.x + cx, extent, 0, g);
-                    x.y = wall_clamp(x.y + cy, extent, 1, g);
-                    x.z = wall_clamp(x.z + cz, extent, 2, g);
+                    x.x = wall_clamp_r(x.x + cx, extent, 0, g, R, i);
+                    x.y = wall_clamp_r(x.y + cy, extent, 1, g, R, i);
+                    x.z = wall_clamp_r(x.z + cz, extent, 2, g, R, i);
                     P[i] = x;
                     step = sqrtf(cx * cx + cy * cy + cz * cz);
                 }
@@ -1533,6 +1548,8 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             const Grid &g = grid_of<A>(w, mine != TGL_NONE ? spec_of_fiber<A>(w, mine) : 0u);
             const int last = mine != TGL_NONE ? (int)w.fiber_vspan[mine].y - 3 : -1;
             const float extent = mine != TGL_NONE ? w.seg_static[w.fiber_s0[mine]].x : 0.0f;
+            float4 *const R =
+                FM && mine != TGL_NONE && w.reaction != nullptr ? w.reaction + w.fiber_vspan[mine].x : nullptr;
             float4 *P = lanes_smem + (size_t)group * stride;
             bool done = mine == TGL_NONE || sp.curvature_cleanup_sweeps == 0;
             bool forward = true, moved = false;
@@ -1548,7 +1565,7 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                 if (!done) {
                     if (bits) {
                         const int first = __ffs(bits) - 1;
-                        if (gl == first) lanes_apply(P, t, tr, extent, g);
+                        if (gl == first) lanes_apply(P, t, tr, extent, g, R);
                         moved = true;
                         t0 = forward ? t0 + first + 1 : t0 - first - 1;
                     } else {
@@ -1585,7 +1602,8 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             const int n = (int)span.y;
             const uint32_t s0 = w.fiber_s0[f];
             const float radius = w.seg_static[s0].x;
-            const float4 *P = lanes_smem + (size_t)j * stride;
+            float4 *P = lanes_smem + (size_t)j * stride;
+            if (FM) formation_targets_staged(w, f, P, n, v0, lane);
             for (int i = lane; i < n; i += 32) {
                 const float4 x = P[i];
                 w.pos[v0 + i] = make_float4(x.x, x.y, x.z, 0.0f);
@@ -1652,7 +1670,8 @@ __global__ void __launch_bounds__(256) rigid_kernel(WorldDev w, StepParams sp) {
     const bool contact_lists = !A && w.contact_skin > 0.0f;
     uint32_t smax = 0, cmax = 0;
     bool far = false, contact_far = false;
-    for (uint32_t f = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); f < w.F; f += warps) {
+    for (uint32_t k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); k < w.FA; k += warps) {
+        const uint32_t f = w.fiber_order[k];
         const uint32_t spec = spec_of_fiber<A>(w, f);
         if (A && ctl_of<A>(w, spec)->control[0] == 0) continue;
         const Grid &g = grid_of<A>(w, spec);
@@ -1715,6 +1734,10 @@ __global__ void __launch_bounds__(256) rigid_kernel(WorldDev w, StepParams sp) {
         for (int a = 0; a < 3; ++a)
             if (!g.periodic[a]) t[a] = t[a] < lo[a] ? lo[a] : (t[a] > hi[a] ? hi[a] : t[a]);
         const float applied = sqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        // The wall's share of the translation, spread over the vertices
+        // (the reactions were cleared at the step's start).
+        float4 *const R = !A && w.reaction != nullptr ? w.reaction + v0 : nullptr;
+        const float4 reaction = make_float4((tx - t[0]) / (float)n, (ty - t[1]) / (float)n, (tz - t[2]) / (float)n, 0.0f);
         for (uint32_t local = lane; local < n; local += 32) {
             float4 x = w.pos[v0 + local];
             x.x += t[0];
@@ -1722,8 +1745,10 @@ __global__ void __launch_bounds__(256) rigid_kernel(WorldDev w, StepParams sp) {
             x.z += t[2];
             w.pos[v0 + local] = x;
             w.vertex_step[v0 + local] = applied;
+            if (R) R[local] = reaction;
         }
         __syncwarp();
+        if (!A) formation_targets_staged(w, f, w.pos + v0, (int)n, v0, lane);
         smax = max(smax, __float_as_uint(fmaxf(applied, 0.0f)));
         const float md = 0.5f * skin_of<A>(w, spec);
         const float radius = w.seg_static[s0].x;
@@ -1839,14 +1864,14 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
         for (int a = 0; a < 3; ++a) edge = std::max(edge, w.grid.length[a]);
         lp.line_eps = 4.0e-6f * edge;
     }
-    lp.contact_blocks = grid_for((w.S + 31) / 32, CONTACT_WARPS, lp.num_sms * 3);
+    lp.contact_blocks = grid_for((w.NS + 31) / 32, CONTACT_WARPS, lp.num_sms * 3);
     // Update kernel: as many warps per block as fit 96 KB of staged fibers.
     size_t per_warp = (size_t)3 * w.max_fiber * sizeof(float4);
     int warps = 8;
     while (warps > 1 && per_warp * warps > 96 * 1024) warps >>= 1;
     lp.fiber_warps = warps;
     lp.fiber_smem = per_warp * warps;
-    lp.fiber_blocks = grid_for(w.F, warps, 1 << 20);
+    lp.fiber_blocks = grid_for(w.FA, warps, 1 << 20);
     // Lane-per-fiber update for fibers of at most 32 * LANES_KMAX vertices:
     // 32 fibers per warp, an odd float4 stride per fiber so that the lanes'
     // same-index accesses spread over the banks.
@@ -1857,7 +1882,7 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     lp.lanes_stride = (int)(w.max_fiber | 1u);
     lp.lanes_smem = (size_t)fpw * lp.lanes_stride * sizeof(float4);
     lp.fiber_lanes = w.max_fiber <= 32u * LANES_KMAX && lp.lanes_smem <= 200 * 1024;
-    lp.lanes_blocks = (int)((w.F + fpw - 1) / fpw);
+    lp.lanes_blocks = (int)((w.FA + fpw - 1) / fpw);
     lp.contact_lists = w.contact_skin > 0.0f;
     lp.build_ch = 3072;
     lp.build_smem = (size_t)lp.build_ch * (sizeof(float4) + sizeof(uint32_t));
@@ -1877,14 +1902,21 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     cudaFuncSetAttribute(fiber_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(lp.fiber_smem, 1));
     if (lp.fiber_lanes) {
         const int smem = (int)lp.lanes_smem;
-        cudaFuncSetAttribute(fiber_lanes_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(fiber_lanes_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(fiber_lanes_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(fiber_lanes_kernel<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(fiber_lanes_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(fiber_lanes_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(fiber_lanes_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(fiber_lanes_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        const auto allow = [smem](auto kernel) {
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        };
+        allow(fiber_lanes_kernel<2, false, false>);
+        allow(fiber_lanes_kernel<4, false, false>);
+        allow(fiber_lanes_kernel<8, false, false>);
+        allow(fiber_lanes_kernel<32, false, false>);
+        allow(fiber_lanes_kernel<2, true, false>);
+        allow(fiber_lanes_kernel<4, true, false>);
+        allow(fiber_lanes_kernel<8, true, false>);
+        allow(fiber_lanes_kernel<32, true, false>);
+        allow(fiber_lanes_kernel<2, false, true>);
+        allow(fiber_lanes_kernel<4, false, true>);
+        allow(fiber_lanes_kernel<8, false, true>);
+        allow(fiber_lanes_kernel<32, false, true>);
     }
     cudaFuncSetAttribute(rb_build_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.build_smem);
     cudaFuncSetAttribute(rb_build_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.build_smem);
@@ -1976,13 +2008,15 @@ int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp
     return 1;
 }
 
-template <bool A>
+template <bool A, bool FM>
 static void enqueue_lanes(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st) {
     switch (lp.lanes_per_fiber) {
-        case 2: fiber_lanes_kernel<2, A><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
-        case 8: fiber_lanes_kernel<8, A><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
-        case 32: fiber_lanes_kernel<32, A><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
-        default: fiber_lanes_kernel<4, A><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+        case 2: fiber_lanes_kernel<2, A, FM><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+        case 8: fiber_lanes_kernel<8, A, FM><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+        case 32:
+            fiber_lanes_kernel<32, A, FM><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride);
+            break;
+        default: fiber_lanes_kernel<4, A, FM><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
     }
 }
 
@@ -1997,9 +2031,11 @@ int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParam
     }
     if (lp.fiber_lanes) {
         if (lp.arena)
-            enqueue_lanes<true>(w, lp, sp, st);
+            enqueue_lanes<true, false>(w, lp, sp, st);
+        else if (w.reaction != nullptr || w.layer_target != nullptr || w.vertex_target != nullptr)
+            enqueue_lanes<false, true>(w, lp, sp, st);
         else
-            enqueue_lanes<false>(w, lp, sp, st);
+            enqueue_lanes<false, false>(w, lp, sp, st);
     } else {
         fiber_kernel<<<lp.fiber_blocks, lp.fiber_warps * 32, lp.fiber_smem, st>>>(w, sp);
     }
@@ -2010,6 +2046,11 @@ int launch_positions_from_stage(const WorldDev &w, cudaStream_t st) {
     positions_from_stage_kernel<<<grid_for(w.V, 256, 1 << 16), 256, 0, st>>>(w);
     refresh_geometry_kernel<<<grid_for(w.S, 256, 1 << 16), 256, 0, st>>>(w);
     return 2;
+}
+
+int launch_refresh_geometry(const WorldDev &w, cudaStream_t st) {
+    refresh_geometry_kernel<<<grid_for(w.S, 256, 1 << 16), 256, 0, st>>>(w);
+    return 1;
 }
 
 int launch_positions_to_stage(const WorldDev &w, cudaStream_t st) {

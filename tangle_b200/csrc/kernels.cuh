@@ -78,7 +78,92 @@ struct WorldDev {
     const uint32_t *fiber_spec; // [F]
     const uint32_t *vtx_spec;  // [V]
     const uint32_t *cell_spec; // [C]
+    // Staged activation (activate_formation_step, kernels.rs:164-221): the
+    // cell list holds the NS segments of active fibers, the update kernels
+    // run the first FA entries of fiber_order (the active fibers), and
+    // fiber_on flags each fiber (nullptr: all active, NS = S, FA = F).
+    uint32_t NS, FA;
+    const uint32_t *fiber_on;  // [F]
+    // Wall reactions of the last update step (kernels.rs:1421-1453 and the
+    // curvature cleanup): xyz per vertex, w unused; nullptr when no axis has
+    // walls (every reaction is then zero).
+    float4 *reaction;          // [V]
+    // Formation layer target (kernels.rs:538-581), applied at the end of
+    // every update step while layer_target is set.
+    const uint32_t *fiber_layer; // [F] layer of each fiber, TGL_NONE = none
+    const float *layer_target;   // [layer_count] target centre coordinates
+    uint32_t layer_count, layer_first, layer_last, layer_axis;
+    float layer_stiffness, layer_max_translation;
+    // Vertex displacement targets (kernels.rs:583-634), applied after the
+    // layer target: target index of each vertex (-1 = none).
+    const int32_t *vertex_target; // [V]
+    const float *target_coord;    // [targets] absolute target coordinates
+    float *command_coord;         // [targets] commanded coordinates so far
+    uint32_t target_axis;
+    float target_stiffness, target_max_translation;
 };
+
+// Is segment s on a fiber that takes part (staged activation)?
+__device__ inline bool segment_on(const WorldDev &w, uint32_t s) {
+    return w.fiber_on == nullptr || w.fiber_on[__float_as_uint(w.seg_static[s].w)] != 0u;
+}
+
+// Is vertex v on an active fiber (through either of its segments)?
+__device__ inline bool vertex_on(const WorldDev &w, uint32_t v) {
+    if (w.fiber_on == nullptr) return true;
+    const int4 l = w.links[v];
+    return segment_on(w, (uint32_t)(l.z >= 0 ? l.z : l.w));
+}
+
+// kernels.rs:925-980 at one interior vertex of a fiber whose positions are
+// p(local index).
+template <typename Fetch>
+__device__ inline float curvature_ratio_at(Fetch p, int i, float maximum) {
+    float4 a0 = p(i - 1), c = p(i), b1 = p(i + 1);
+    float ax = c.x - a0.x, ay = c.y - a0.y, az = c.z - a0.z;
+    float bx = b1.x - c.x, by = b1.y - c.y, bz = b1.z - c.z;
+    float first_length = sqrtf(ax * ax + ay * ay + az * az);
+    float second_length = sqrtf(bx * bx + by * by + bz * bz);
+    float ratio = 0.0f;
+    if (first_length > 1.0e-7f && second_length > 1.0e-7f) {
+        float cosine = (ax * bx + ay * by + az * bz) / (first_length * second_length);
+        cosine = clampf(cosine, -1.0f, 1.0f);
+        float dual_length = 0.5f * (first_length + second_length);
+        float curvature = 2.0f * sqrtf(0.5f * (1.0f - cosine)) / dual_length;
+        ratio = curvature / maximum;
+    }
+    return ratio;
+}
+
+// Formation launchers (formation.cu).
+// apply_formation_layer_targets once, outside a batch (world.rs:1758-1800).
+void launch_layer_targets_now(const WorldDev &w, cudaStream_t st);
+// initialize_vertex_displacement_targets (kernels.rs:583-602) into target
+// and command.
+void launch_init_vertex_targets(const WorldDev &w, const uint32_t *vertices, uint32_t count, float displacement,
+                                float *target, float *command, cudaStream_t st);
+// measure_layer_target_error / measure_vertex_target_error (kernels.rs:
+// 636-711) as u32 bits of the non-negative maxima: bits2[0] layer, bits2[1]
+// vertex (fibers[k]: the fiber of target k's vertex).
+void launch_target_errors(const WorldDev &w, const uint32_t *vertices, const uint32_t *fibers, uint32_t count,
+                          unsigned int *bits2, cudaStream_t st);
+// compact_rigid_fiber_centers (kinematics 0), compact_moving_walls (1),
+// compact_affine_vertices (2) (kernels.rs:712-818), from the box in w.grid.
+void launch_compaction(const WorldDev &w, const float new_lower[3], const float new_upper[3], uint32_t kinematics,
+                       cudaStream_t st);
+// measure_compaction_metrics (kernels.rs:820-923) into out13 (device),
+// through METRIC_BLOCKS * 12 doubles of partial sums.
+constexpr int METRIC_BLOCKS = 296;
+void launch_compaction_metrics(const WorldDev &w, float correction_fraction, float contact_stiffness,
+                               float stretch_stiffness, float bending_stiffness, double *partials, float *out13,
+                               cudaStream_t st);
+// set_fiber_maximum_curvatures (world.rs:2185-2194): every vertex of fiber f
+// takes values[f] (device array of F).
+void launch_set_fiber_curvatures(const WorldDev &w, float4 *vtx_static, const float *values, cudaStream_t st);
+// Zeroes the wall reactions of inactive fibers' vertices.
+void launch_clear_inactive_reactions(const WorldDev &w, cudaStream_t st);
+// Segment geometry records from the positions.
+int launch_refresh_geometry(const WorldDev &w, cudaStream_t st);
 
 struct StepParams {
     float penetration_tolerance;

@@ -148,7 +148,7 @@ __global__ void graph_count_kernel(WorldDev w, GraphBuffers g, float cutoff) {
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); a < w.S; a += warps) {
-        const uint32_t count = w.nbr_count[a];
+        const uint32_t count = segment_on(w, a) ? w.nbr_count[a] : 0u;
         uint32_t kept = 0;
         if (count <= w.block) {
             for (uint32_t i0 = 0; i0 < count; i0 += 32) {
@@ -244,7 +244,7 @@ __global__ void graph_fill_kernel(WorldDev w, GraphBuffers g, float cutoff) {
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); a < w.S; a += warps) {
-        const uint32_t count = w.nbr_count[a];
+        const uint32_t count = segment_on(w, a) ? w.nbr_count[a] : 0u;
         if (count > w.block) continue;
         const int64_t base = (int64_t)g.offsets[a] + g.in_count[a];
         uint32_t rank = 0;
@@ -411,7 +411,7 @@ __global__ void residual_kernel(WorldDev w, unsigned int *out2, float *block_sum
     unsigned int pen = 0, ratio = 0;
     float sum = 0.0f;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < w.S; s += gridDim.x * blockDim.x) {
-        const float p = fmaxf(w.corr[2 * (size_t)s].w, 0.0f);
+        const float p = segment_on(w, s) ? fmaxf(w.corr[2 * (size_t)s].w, 0.0f) : 0.0f;
         pen = max(pen, __float_as_uint(p));
         sum += p / (2.0f * w.seg_static[s].x);
     }

@@ -119,6 +119,28 @@ struct tgl_world {
     const GraphEntry *last = nullptr;  // graph of the last batch
     uint64_t last_batch_iterations = 0;
     WarmGraph warm;
+    // Formation state (single worlds): the host's copy of the fiber layout,
+    // the active flags, and the device buffers of the targets, the
+    // compaction metrics and the target errors.
+    std::vector<uint2> h_vspan;
+    std::vector<uint32_t> h_s0;
+    std::vector<uint32_t> h_active;
+    uint32_t *fiber_order_d = nullptr;
+    uint32_t *fiber_on_d = nullptr;
+    float4 *vtx_static_d = nullptr;
+    uint32_t *fiber_layer_d = nullptr;
+    float *layer_target_d = nullptr;
+    uint32_t layer_capacity = 0;
+    int32_t *vertex_target_d = nullptr;
+    uint32_t *target_vertices_d = nullptr, *target_fibers_d = nullptr;
+    float *target_coord_d = nullptr, *command_coord_d = nullptr;
+    uint32_t target_capacity = 0, target_count = 0;
+    std::vector<uint32_t> h_target_vertices;
+    unsigned int *error_bits_d = nullptr;
+    double *metric_partials_d = nullptr;
+    float *metric_out_d = nullptr;
+    uint64_t allocated_cells = 0;
+    float maximum_radius = 0.0f, maximum_length = 0.0f;
 
     ~tgl_world() {
         for (auto &kv : graphs) destroy_entry(kv.second);
@@ -609,6 +631,11 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
     d.S = S;
     d.F = F;
     d.C = (uint32_t)C;
+    d.NS = S;  // every fiber starts active
+    d.FA = F;
+    w->allocated_cells = C;
+    w->maximum_radius = h0.maximum_radius;
+    w->maximum_length = h0.maximum_length;
     d.block = block;
     d.max_fiber = max_fiber;
     d.skin = skin;
@@ -666,6 +693,20 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
     d.fiber_s0 = fiber_s0_d;
     d.fiber_order = fiber_order_d;
     d.vtx_static = vtx_static_d;
+    w->fiber_order_d = fiber_order_d;
+    w->vtx_static_d = vtx_static_d;
+    if (!arena) {
+        w->h_vspan = fiber_vspan;
+        w->h_s0 = fiber_s0;
+        w->h_active.assign(F, 1u);
+        // Wall reactions are kept when some axis has walls (on periodic
+        // axes every reaction is zero).
+        if (!grid.periodic[0] || !grid.periodic[1] || !grid.periodic[2]) {
+            if ((rc = w->alloc(&d.reaction, V))) return fail(rc);
+            if (cudaMemset(d.reaction, 0, V * sizeof(float4)) != cudaSuccess)
+                return fail(set_error(TGL_ERR_CUDA, "device initialisation failed"));
+        }
+    }
     d.pinned = pinned_d;
     d.rest = rest_d;
     d.P = count;
@@ -1175,6 +1216,371 @@ int tgl_debug_corrections(tgl_world *w, const tgl_relax_config *config, float *c
     cudaFree(corr6);
     cudaFree(pen);
     if (e != cudaSuccess) return set_error(TGL_ERR_CUDA, cudaGetErrorString(e));
+    TGL_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- formation hooks
+
+namespace {
+
+// A change to the world's by-value kernel parameters (counts, targets,
+// grid) retires every captured batch graph.
+void invalidate_graphs(tgl_world *w) {
+    for (auto &kv : w->graphs) destroy_entry(kv.second);
+    w->graphs.clear();
+    w->last = nullptr;
+    w->warm.counted = false;
+}
+
+int formation_world(tgl_world *w) {
+    if (!w) return set_error(TGL_ERR_INVALID, "null argument");
+    if (w->arena) return set_error(TGL_ERR_UNSUPPORTED, "formation hooks take a single world, not an arena");
+    return 0;
+}
+
+// Grows a device buffer to hold `count` elements (the old one stays in the
+// world's allocation list until the world is destroyed).
+template <typename T>
+int reserve(tgl_world *w, T **buffer, uint32_t &capacity, uint32_t count) {
+    if (*buffer && capacity >= count) return 0;
+    if (int rc = w->alloc(buffer, std::max<size_t>(count, 1))) return rc;
+    capacity = count;
+    return 0;
+}
+
+// The fiber of vertex v (binary search over the fiber spans).
+uint32_t fiber_of_vertex(const tgl_world *w, uint32_t v) {
+    size_t lo = 0, hi = w->h_vspan.size();
+    while (hi - lo > 1) {
+        const size_t mid = (lo + hi) / 2;
+        if (w->h_vspan[mid].x <= v)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return (uint32_t)lo;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tgl_world_set_active_fibers(tgl_world *w, const uint8_t *active, uint64_t fiber_count, uint32_t *active_segments,
+                                uint32_t *active_vertices) {
+    if (int rc = formation_world(w)) return rc;
+    if (!active || !active_segments || !active_vertices) return set_error(TGL_ERR_INVALID, "null argument");
+    WorldDev &d = w->dev;
+    if (fiber_count != d.F) return set_error(TGL_ERR_INVALID, "active flags need one entry per fiber");
+    uint64_t segments = 0, vertices = 0;
+    std::vector<uint32_t> order;
+    order.reserve(d.F);
+    for (uint32_t f = 0; f < d.F; ++f) {
+        w->h_active[f] = active[f] ? 1u : 0u;
+        if (!active[f]) continue;
+        order.push_back(f);
+        segments += w->h_vspan[f].y - 1;
+        vertices += w->h_vspan[f].y;
+    }
+    // Active fibers by descending vertex count, as at creation.
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return w->h_vspan[a].y > w->h_vspan[b].y; });
+    if (!order.empty())
+        TGL_CUDA(cudaMemcpyAsync(w->fiber_order_d, order.data(), order.size() * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, w->stream));
+    const bool all = order.size() == d.F;
+    if (!all) {
+        if (!w->fiber_on_d && w->alloc(&w->fiber_on_d, d.F)) return TGL_ERR_MEMORY;
+        TGL_CUDA(cudaMemcpyAsync(w->fiber_on_d, w->h_active.data(), d.F * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                 w->stream));
+    }
+    d.fiber_on = all ? nullptr : w->fiber_on_d;
+    d.FA = (uint32_t)order.size();
+    d.NS = (uint32_t)segments;
+    plan_launches(d, w->lp);
+    launch_clear_inactive_reactions(d, w->stream);
+    // world.rs:2179-2181: newly active fibers are missing from the lists.
+    w->launches += launch_request_rebuild(d, w->lp, w->stream);
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    TGL_CUDA(cudaGetLastError());
+    invalidate_graphs(w);
+    *active_segments = (uint32_t)segments;
+    *active_vertices = (uint32_t)vertices;
+    return 0;
+}
+
+int tgl_world_set_layer_targets(tgl_world *w, const tgl_layer_targets *t) {
+    if (int rc = formation_world(w)) return rc;
+    WorldDev &d = w->dev;
+    invalidate_graphs(w);
+    if (!t) {  // world.rs:1806-1810
+        d.layer_target = nullptr;
+        return 0;
+    }
+    // world.rs:1774-1777 and :1750.
+    if (t->axis >= 3) return set_error(TGL_ERR_INVALID, "layer axis must be 0, 1 or 2");
+    if (t->count == 0 || !t->targets || !t->fiber_layers) return set_error(TGL_ERR_INVALID, "layer targets are empty");
+    if (!(t->stiffness > 0.0f && t->stiffness <= 1.0f)) return set_error(TGL_ERR_INVALID, "stiffness must be in (0, 1]");
+    if (!(t->max_translation > 0.0f)) return set_error(TGL_ERR_INVALID, "max_translation must be positive");
+    if (t->first_layer > t->last_layer) return set_error(TGL_ERR_INVALID, "first_layer exceeds last_layer");
+    uint32_t fiber_capacity = w->fiber_layer_d ? d.F : 0;
+    if (int rc = reserve(w, &w->fiber_layer_d, fiber_capacity, d.F)) return rc;
+    if (int rc = reserve(w, &w->layer_target_d, w->layer_capacity, t->count)) return rc;
+    TGL_CUDA(cudaMemcpyAsync(w->fiber_layer_d, t->fiber_layers, d.F * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             w->stream));
+    TGL_CUDA(cudaMemcpyAsync(w->layer_target_d, t->targets, t->count * sizeof(float), cudaMemcpyHostToDevice,
+                             w->stream));
+    d.fiber_layer = w->fiber_layer_d;
+    d.layer_target = w->layer_target_d;
+    d.layer_count = t->count;
+    d.layer_first = t->first_layer;
+    d.layer_last = t->last_layer;
+    d.layer_axis = t->axis;
+    d.layer_stiffness = t->stiffness;
+    d.layer_max_translation = t->max_translation;
+    if (t->apply_now) {  // the first correction at once (world.rs:1778-1799)
+        launch_layer_targets_now(d, w->stream);
+        w->launches += 1 + launch_refresh_geometry(d, w->stream);
+    }
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    TGL_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int tgl_world_set_vertex_targets(tgl_world *w, const tgl_vertex_targets *t) {
+    if (int rc = formation_world(w)) return rc;
+    WorldDev &d = w->dev;
+    invalidate_graphs(w);
+    if (!t) {  // world.rs:1861-1863
+        d.vertex_target = nullptr;
+        w->target_count = 0;
+        w->h_target_vertices.clear();
+        return 0;
+    }
+    // world.rs:1819-1828.
+    if (t->axis >= 3) return set_error(TGL_ERR_INVALID, "target axis must be 0, 1 or 2");
+    if (t->count == 0 || !t->vertices) return set_error(TGL_ERR_INVALID, "vertex targets are empty");
+    if (!(t->stiffness > 0.0f && t->stiffness <= 1.0f)) return set_error(TGL_ERR_INVALID, "stiffness must be in (0, 1]");
+    if (!(t->max_translation > 0.0f)) return set_error(TGL_ERR_INVALID, "max_translation must be positive");
+    const bool restoring = t->coordinates != nullptr;
+    if (restoring != (t->command_coordinates != nullptr))
+        return set_error(TGL_ERR_INVALID, "coordinates and command_coordinates come together");
+    if (!restoring && !(std::isfinite(t->displacement) && t->displacement != 0.0f))
+        return set_error(TGL_ERR_INVALID, "displacement must be finite and non-zero");
+    std::vector<int32_t> map(d.V, -1);
+    std::vector<uint32_t> fibers(t->count);
+    for (uint32_t k = 0; k < t->count; ++k) {
+        const uint32_t v = t->vertices[k];
+        if (v >= d.V) return set_error(TGL_ERR_INVALID, "vertex target index out of range");
+        if (map[v] >= 0) return set_error(TGL_ERR_INVALID, "vertex target indices must be distinct");
+        map[v] = (int32_t)k;
+        fibers[k] = fiber_of_vertex(w, v);
+    }
+    uint32_t vertex_capacity = w->vertex_target_d ? d.V : 0;
+    if (int rc = reserve(w, &w->vertex_target_d, vertex_capacity, d.V)) return rc;
+    uint32_t cap = w->target_capacity;
+    if (int rc = reserve(w, &w->target_vertices_d, cap, t->count)) return rc;
+    cap = w->target_capacity;
+    if (int rc = reserve(w, &w->target_fibers_d, cap, t->count)) return rc;
+    cap = w->target_capacity;
+    if (int rc = reserve(w, &w->target_coord_d, cap, t->count)) return rc;
+    cap = w->target_capacity;
+    if (int rc = reserve(w, &w->command_coord_d, cap, t->count)) return rc;
+    w->target_capacity = std::max(w->target_capacity, t->count);
+    TGL_CUDA(cudaMemcpyAsync(w->vertex_target_d, map.data(), d.V * sizeof(int32_t), cudaMemcpyHostToDevice, w->stream));
+    TGL_CUDA(cudaMemcpyAsync(w->target_vertices_d, t->vertices, t->count * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             w->stream));
+    TGL_CUDA(cudaMemcpyAsync(w->target_fibers_d, fibers.data(), t->count * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             w->stream));
+    d.target_axis = t->axis;
+    d.target_stiffness = t->stiffness;
+    d.target_max_translation = t->max_translation;
+    d.target_coord = w->target_coord_d;
+    d.command_coord = w->command_coord_d;
+    d.vertex_target = w->vertex_target_d;
+    if (restoring) {
+        TGL_CUDA(cudaMemcpyAsync(w->target_coord_d, t->coordinates, t->count * sizeof(float), cudaMemcpyHostToDevice,
+                                 w->stream));
+        TGL_CUDA(cudaMemcpyAsync(w->command_coord_d, t->command_coordinates, t->count * sizeof(float),
+                                 cudaMemcpyHostToDevice, w->stream));
+    } else {
+        launch_init_vertex_targets(d, w->target_vertices_d, t->count, t->displacement, w->target_coord_d,
+                                   w->command_coord_d, w->stream);
+        w->launches += 1;
+    }
+    w->target_count = t->count;
+    w->h_target_vertices.assign(t->vertices, t->vertices + t->count);
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    TGL_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int tgl_world_vertex_target_state(tgl_world *w, float *coordinates, float *command_coordinates, uint32_t count) {
+    if (int rc = formation_world(w)) return rc;
+    if (!coordinates || !command_coordinates) return set_error(TGL_ERR_INVALID, "null argument");
+    if (!w->dev.vertex_target) return set_error(TGL_ERR_INVALID, "no vertex targets are installed");
+    if (count != w->target_count) return set_error(TGL_ERR_INVALID, "count differs from the installed target count");
+    TGL_CUDA(cudaMemcpyAsync(coordinates, w->target_coord_d, count * sizeof(float), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaMemcpyAsync(command_coordinates, w->command_coord_d, count * sizeof(float), cudaMemcpyDeviceToHost,
+                             w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    return 0;
+}
+
+int tgl_world_target_errors(tgl_world *w, float *layer_error, uint32_t *has_layer, float *vertex_error,
+                            uint32_t *has_vertex) {
+    if (int rc = formation_world(w)) return rc;
+    if (!layer_error || !has_layer || !vertex_error || !has_vertex) return set_error(TGL_ERR_INVALID, "null argument");
+    const WorldDev &d = w->dev;
+    *has_layer = d.layer_target ? 1u : 0u;
+    *has_vertex = d.vertex_target ? 1u : 0u;
+    *layer_error = 0.0f;
+    *vertex_error = 0.0f;
+    if (!d.layer_target && !d.vertex_target) return 0;
+    if (!w->error_bits_d && w->alloc(&w->error_bits_d, 2)) return TGL_ERR_MEMORY;
+    launch_target_errors(d, w->target_vertices_d, w->target_fibers_d, w->target_count, w->error_bits_d, w->stream);
+    w->launches += (d.layer_target ? 1 : 0) + (d.vertex_target ? 1 : 0);
+    unsigned int bits[2] = {0, 0};
+    TGL_CUDA(cudaMemcpyAsync(bits, w->error_bits_d, sizeof(bits), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    TGL_CUDA(cudaGetLastError());
+    std::memcpy(layer_error, &bits[0], 4);
+    std::memcpy(vertex_error, &bits[1], 4);
+    return 0;
+}
+
+int tgl_world_compact_cell(tgl_world *w, const float new_lower[3], const float new_upper[3], uint32_t kinematics) {
+    if (int rc = formation_world(w)) return rc;
+    if (!new_lower || !new_upper) return set_error(TGL_ERR_INVALID, "null argument");
+    if (kinematics > 2) return set_error(TGL_ERR_INVALID, "kinematics must be 0 (rigid centres), 1 (walls) or 2 (affine)");
+    WorldDev &d = w->dev;
+    // world.rs:1937-1950.
+    uint32_t cells[3];
+    uint64_t C = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (!std::isfinite(new_lower[a]) || !std::isfinite(new_upper[a]))
+            return set_error(TGL_ERR_INVALID, "the new cell bounds must be finite");
+        if (!(new_upper[a] - new_lower[a] > 2.0f * w->maximum_radius))
+            return set_error(TGL_ERR_INVALID, "the new cell must be wider than two largest radii on every axis");
+        if (!(new_lower[a] >= d.grid.lower[a]) || !(new_upper[a] <= d.grid.upper[a]))
+            return set_error(TGL_ERR_INVALID, "compaction cannot grow the cell");
+        cells[a] = f32_to_u32_host(std::fmax(std::floor((new_upper[a] - new_lower[a]) / w->cell_size), 1.0f));
+        C *= cells[a];
+    }
+    if (C > w->allocated_cells) return set_error(TGL_ERR_INVALID, "the compacted grid needs more cells than allocated");
+    launch_compaction(d, new_lower, new_upper, kinematics, w->stream);
+    w->launches += 1;
+    // world.rs:2035-2053: the resident cell and the grid follow; the cell
+    // size stays.
+    for (int a = 0; a < 3; ++a) {
+        const float extent = new_upper[a] - new_lower[a];
+        d.grid.lower[a] = new_lower[a];
+        d.grid.upper[a] = new_upper[a];
+        d.grid.cells[a] = cells[a];
+        d.grid.length[a] = extent;
+        d.grid.width[a] = extent / (float)cells[a];
+        d.grid.inv_length[a] = 1.0f / extent;
+    }
+    d.C = (uint32_t)C;
+    // The contact lists' single-image bound follows the new box edges.
+    if (d.contact_skin > 0.0f) {
+        d.contact_half_limit = INFINITY;
+        for (int a = 0; a < 3; ++a)
+            if (d.grid.periodic[a])
+                d.contact_half_limit =
+                    std::fmin(d.contact_half_limit,
+                              0.999f * 0.5f * (0.5f * d.grid.length[a] - 2.0f * w->maximum_radius - d.contact_skin));
+    }
+    plan_launches(d, w->lp);
+    w->launches += launch_refresh_geometry(d, w->stream);
+    w->launches += launch_request_rebuild(d, w->lp, w->stream);  // world.rs:2052
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    TGL_CUDA(cudaGetLastError());
+    invalidate_graphs(w);
+    return 0;
+}
+
+int tgl_world_cell_bounds(tgl_world *w, float lower[3], float upper[3]) {
+    if (!w || !lower || !upper) return set_error(TGL_ERR_INVALID, "null argument");
+    for (int a = 0; a < 3; ++a) {
+        lower[a] = w->dev.grid.lower[a];
+        upper[a] = w->dev.grid.upper[a];
+    }
+    return 0;
+}
+
+int tgl_world_compaction_metrics(tgl_world *w, float correction_fraction, const float stiffness[3], float out[13]) {
+    if (int rc = formation_world(w)) return rc;
+    if (!stiffness || !out) return set_error(TGL_ERR_INVALID, "null argument");
+    // world.rs:2061-2064.
+    if (!(correction_fraction > 0.0f)) return set_error(TGL_ERR_INVALID, "correction_fraction must be positive");
+    for (int k = 0; k < 3; ++k)
+        if (!(stiffness[k] >= 0.0f)) return set_error(TGL_ERR_INVALID, "energy stiffnesses must be non-negative");
+    if (!w->metric_partials_d && w->alloc(&w->metric_partials_d, (size_t)METRIC_BLOCKS * 12)) return TGL_ERR_MEMORY;
+    if (!w->metric_out_d && w->alloc(&w->metric_out_d, 13)) return TGL_ERR_MEMORY;
+    launch_compaction_metrics(w->dev, correction_fraction, stiffness[0], stiffness[1], stiffness[2],
+                              w->metric_partials_d, w->metric_out_d, w->stream);
+    w->launches += 2;
+    TGL_CUDA(cudaMemcpyAsync(out, w->metric_out_d, 13 * sizeof(float), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    TGL_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int tgl_world_wall_reactions(tgl_world *w, float *xyz, size_t len) {
+    if (int rc = formation_world(w)) return rc;
+    if (!xyz) return set_error(TGL_ERR_INVALID, "null argument");
+    const WorldDev &d = w->dev;
+    if (len != 3 * (size_t)d.V) return set_error(TGL_ERR_INVALID, "reaction buffer has the wrong length");
+    if (!d.reaction) {  // no walls: every reaction is zero
+        std::memset(xyz, 0, len * sizeof(float));
+        return 0;
+    }
+    std::vector<float4> r(d.V);
+    TGL_CUDA(cudaMemcpyAsync(r.data(), d.reaction, d.V * sizeof(float4), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    for (uint32_t v = 0; v < d.V; ++v) {
+        xyz[3 * (size_t)v] = r[v].x;
+        xyz[3 * (size_t)v + 1] = r[v].y;
+        xyz[3 * (size_t)v + 2] = r[v].z;
+    }
+    return 0;
+}
+
+int tgl_world_set_wall_reactions(tgl_world *w, const float *xyz, size_t len) {
+    if (int rc = formation_world(w)) return rc;
+    if (!xyz) return set_error(TGL_ERR_INVALID, "null argument");
+    const WorldDev &d = w->dev;
+    if (len != 3 * (size_t)d.V) return set_error(TGL_ERR_INVALID, "reaction buffer has the wrong length");
+    if (!d.reaction) return 0;  // no walls: reactions stay zero
+    std::vector<float4> r(d.V);
+    for (uint32_t v = 0; v < d.V; ++v)
+        r[v] = make_float4(xyz[3 * (size_t)v], xyz[3 * (size_t)v + 1], xyz[3 * (size_t)v + 2], 0.0f);
+    TGL_CUDA(cudaMemcpyAsync(d.reaction, r.data(), d.V * sizeof(float4), cudaMemcpyHostToDevice, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    return 0;
+}
+
+int tgl_world_set_fiber_max_curvatures(tgl_world *w, const float *values, size_t count) {
+    if (int rc = formation_world(w)) return rc;
+    if (!values) return set_error(TGL_ERR_INVALID, "null argument");
+    const WorldDev &d = w->dev;
+    if (count != d.F) return set_error(TGL_ERR_INVALID, "one curvature limit per fiber");  // world.rs:2186
+    for (size_t f = 0; f < count; ++f)
+        if (!(values[f] >= 0.0f) || !std::isfinite(values[f]))
+            return set_error(TGL_ERR_INVALID, "curvature limits must be finite and non-negative");
+    float *values_d = nullptr;
+    if (cudaMalloc(&values_d, count * sizeof(float)) != cudaSuccess) return set_error(TGL_ERR_MEMORY, "cudaMalloc failed");
+    cudaError_t e = cudaMemcpyAsync(values_d, values, count * sizeof(float), cudaMemcpyHostToDevice, w->stream);
+    if (e == cudaSuccess) {
+        launch_set_fiber_curvatures(d, w->vtx_static_d, values_d, w->stream);
+        w->launches += 1;
+        e = cudaStreamSynchronize(w->stream);
+    }
+    cudaFree(values_d);
+    if (e != cudaSuccess) return set_error(TGL_ERR_CUDA, std::string("curvature limits: ") + cudaGetErrorString(e));
     TGL_CUDA(cudaGetLastError());
     return 0;
 }

@@ -19,6 +19,7 @@ from typing import List, Optional
 
 import numpy as np
 
+from .formation import FormationHooks
 from .settings import BatchStatus, CellListConfig, RelaxationConfig
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -39,9 +40,45 @@ EXPORTS = (
     "tgl_gemm_bf16", "tgl_warmstart_graph_count", "tgl_warmstart_graph_fill", "tgl_world_displace",
     "tgl_world_residual", "tgl_mp_edge_inputs", "tgl_mp_node_inputs", "tgl_mp_node_inputs_backward",
     "tgl_mp_edge_inputs_backward", "tgl_column_sums_scratch", "tgl_column_sums", "tgl_adam_step", "tgl_mse",
-    "tgl_convert_bf16",
+    "tgl_convert_bf16", "tgl_world_set_active_fibers", "tgl_world_set_layer_targets", "tgl_world_set_vertex_targets",
+    "tgl_world_vertex_target_state", "tgl_world_target_errors", "tgl_world_compact_cell", "tgl_world_cell_bounds",
+    "tgl_world_compaction_metrics", "tgl_world_wall_reactions", "tgl_world_set_wall_reactions",
+    "tgl_world_set_fiber_max_curvatures",
     "tgl_last_error",
 )
+
+
+class LayerTargets(ctypes.Structure):
+    """tgl_layer_targets."""
+
+    _fields_ = [
+        ("axis", ctypes.c_uint32),
+        ("count", ctypes.c_uint32),
+        ("targets", ctypes.c_void_p),
+        ("fiber_layers", ctypes.c_void_p),
+        ("first_layer", ctypes.c_uint32),
+        ("last_layer", ctypes.c_uint32),
+        ("stiffness", ctypes.c_float),
+        ("max_translation", ctypes.c_float),
+        ("apply_now", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+class VertexTargets(ctypes.Structure):
+    """tgl_vertex_targets."""
+
+    _fields_ = [
+        ("axis", ctypes.c_uint32),
+        ("count", ctypes.c_uint32),
+        ("vertices", ctypes.c_void_p),
+        ("displacement", ctypes.c_float),
+        ("stiffness", ctypes.c_float),
+        ("max_translation", ctypes.c_float),
+        ("reserved", ctypes.c_uint32),
+        ("coordinates", ctypes.c_void_p),
+        ("command_coordinates", ctypes.c_void_p),
+    ]
 
 
 class Packed(ctypes.Structure):
@@ -200,6 +237,24 @@ def load_library():
     lib.tgl_last_kernel_times.restype = ctypes.c_int
     lib.tgl_world_stream.argtypes = [P]
     lib.tgl_world_stream.restype = ctypes.c_void_p
+    lib.tgl_world_set_active_fibers.argtypes = [P, P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32),
+                                                ctypes.POINTER(ctypes.c_uint32)]
+    lib.tgl_world_set_layer_targets.argtypes = [P, ctypes.POINTER(LayerTargets)]
+    lib.tgl_world_set_vertex_targets.argtypes = [P, ctypes.POINTER(VertexTargets)]
+    lib.tgl_world_vertex_target_state.argtypes = [P, P, P, ctypes.c_uint32]
+    lib.tgl_world_target_errors.argtypes = [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32),
+                                            ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32)]
+    lib.tgl_world_compact_cell.argtypes = [P, P, P, ctypes.c_uint32]
+    lib.tgl_world_cell_bounds.argtypes = [P, P, P]
+    lib.tgl_world_compaction_metrics.argtypes = [P, ctypes.c_float, P, P]
+    lib.tgl_world_wall_reactions.argtypes = [P, P, ctypes.c_size_t]
+    lib.tgl_world_set_wall_reactions.argtypes = [P, P, ctypes.c_size_t]
+    lib.tgl_world_set_fiber_max_curvatures.argtypes = [P, P, ctypes.c_size_t]
+    for name in ("tgl_world_set_active_fibers", "tgl_world_set_layer_targets", "tgl_world_set_vertex_targets",
+                 "tgl_world_vertex_target_state", "tgl_world_target_errors", "tgl_world_compact_cell",
+                 "tgl_world_cell_bounds", "tgl_world_compaction_metrics", "tgl_world_wall_reactions",
+                 "tgl_world_set_wall_reactions", "tgl_world_set_fiber_max_curvatures"):
+        getattr(lib, name).restype = ctypes.c_int
     lib.tgl_last_error.argtypes = []
     lib.tgl_last_error.restype = ctypes.c_char_p
     _lib = lib
@@ -279,7 +334,7 @@ class ContactCapture:
     overflow: bool
 
 
-class DeviceWorld:
+class DeviceWorld(FormationHooks):
     """Resident relaxation world on the current CUDA device."""
 
     def __init__(self, packed, cell_list: Optional[CellListConfig] = None, max_step: float = 0.006,
@@ -303,6 +358,8 @@ class DeviceWorld:
         self._packed = packed
         self.vertex_count = packed.vertex_count
         self.segment_count = packed.segment_count
+        if not np.all(np.asarray(packed.fiber_active)):
+            self.set_active_fibers(np.asarray(packed.fiber_active))
 
     @classmethod
     def upload(cls, config: RelaxationConfig, packed) -> "DeviceWorld":
@@ -367,14 +424,20 @@ class DeviceWorld:
 
     @classmethod
     def restore(cls, config: RelaxationConfig, checkpoint) -> "DeviceWorld":
-        """DeviceWorld::restore(config, checkpoint) (plugin.rs:358-391): a
-        world uploaded from the checkpoint's packed assembly whose lifetime
-        iteration count continues from the checkpoint's."""
-        return cls(checkpoint.packed, config.cell_list, config.max_step, checkpoint.total_iterations)
+        """DeviceWorld::restore(config, checkpoint) (plugin.rs:358-391;
+        world.rs:693-756): a world uploaded from the checkpoint's packed
+        assembly (positions, cell, active fibers, curvature limits) whose
+        lifetime iteration count continues from the checkpoint's, with its
+        wall reactions and formation targets re-installed."""
+        world = cls(checkpoint.packed, config.cell_list, config.max_step, checkpoint.total_iterations)
+        world._restore_formation(checkpoint)
+        return world
 
     def checkpoint(self):
-        """DeviceWorld::checkpoint() (plugin.rs:393-404): the packed assembly
-        with the current positions, and the lifetime iteration count."""
+        """DeviceWorld::checkpoint() (plugin.rs:393-404; world.rs:758-823):
+        the packed assembly with the current positions, cell, active fibers
+        and curvature limits, the lifetime iteration count, the wall
+        reactions and the installed formation targets."""
         import dataclasses
 
         from .checkpoint import DeviceWorldCheckpoint
@@ -382,7 +445,75 @@ class DeviceWorld:
         xyz = np.empty(3 * self.vertex_count, dtype=np.float32)
         total = ctypes.c_uint64()
         self._check(self._lib.tgl_world_checkpoint(self._handle, _ptr(xyz), xyz.size, ctypes.byref(total)))
-        return DeviceWorldCheckpoint(dataclasses.replace(self._packed, positions=xyz), int(total.value))
+        lower, upper = self._fh_cell_bounds()
+        packed = dataclasses.replace(self._packed, positions=xyz, cell_lower=lower, cell_upper=upper,
+                                     fiber_active=self.fiber_active, vertex_max_curvature=self.vertex_max_curvature)
+        return DeviceWorldCheckpoint(packed, int(total.value), self.wall_reactions(), self.layer_target_checkpoint(),
+                                     self.vertex_target_checkpoint())
+
+    # ---- formation hooks (tangle_b200.formation.FormationHooks)
+
+    def _fh_set_active(self, flags):
+        segments, vertices = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self._lib.tgl_world_set_active_fibers(self._handle, _ptr(flags), flags.size,
+                                                          ctypes.byref(segments), ctypes.byref(vertices)))
+        return int(segments.value), int(vertices.value)
+
+    def _fh_set_layer_targets(self, axis, targets, layers, first, last, stiffness, max_translation, apply_now):
+        if targets is None:
+            self._check(self._lib.tgl_world_set_layer_targets(self._handle, None))
+            return
+        t = LayerTargets(axis, targets.size, targets.ctypes.data, layers.ctypes.data, first, last, stiffness,
+                         max_translation, 1 if apply_now else 0, 0)
+        self._check(self._lib.tgl_world_set_layer_targets(self._handle, ctypes.byref(t)))
+
+    def _fh_set_vertex_targets(self, axis, indices, displacement, stiffness, max_translation, coordinates, commands):
+        if indices is None:
+            self._check(self._lib.tgl_world_set_vertex_targets(self._handle, None))
+            return
+        t = VertexTargets(axis, indices.size, indices.ctypes.data, displacement, stiffness, max_translation, 0,
+                          None if coordinates is None else coordinates.ctypes.data,
+                          None if commands is None else commands.ctypes.data)
+        self._check(self._lib.tgl_world_set_vertex_targets(self._handle, ctypes.byref(t)))
+
+    def _fh_vertex_target_state(self, count):
+        coordinates = np.empty(count, dtype=np.float32)
+        commands = np.empty(count, dtype=np.float32)
+        self._check(self._lib.tgl_world_vertex_target_state(self._handle, _ptr(coordinates), _ptr(commands), count))
+        return coordinates, commands
+
+    def _fh_target_errors(self):
+        layer, vertex = ctypes.c_float(), ctypes.c_float()
+        has_layer, has_vertex = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self._lib.tgl_world_target_errors(self._handle, ctypes.byref(layer), ctypes.byref(has_layer),
+                                                      ctypes.byref(vertex), ctypes.byref(has_vertex)))
+        return float(layer.value), bool(has_layer.value), float(vertex.value), bool(has_vertex.value)
+
+    def _fh_compact(self, lower, upper, kinematics):
+        self._check(self._lib.tgl_world_compact_cell(self._handle, _ptr(lower), _ptr(upper), kinematics))
+
+    def _fh_cell_bounds(self):
+        lower = np.empty(3, dtype=np.float32)
+        upper = np.empty(3, dtype=np.float32)
+        self._check(self._lib.tgl_world_cell_bounds(self._handle, _ptr(lower), _ptr(upper)))
+        return lower, upper
+
+    def _fh_metrics(self, correction_fraction, stiffness):
+        out = np.empty(13, dtype=np.float32)
+        self._check(self._lib.tgl_world_compaction_metrics(self._handle, ctypes.c_float(correction_fraction),
+                                                           _ptr(stiffness), _ptr(out)))
+        return out
+
+    def _fh_wall_reactions(self):
+        out = np.empty(3 * self.vertex_count, dtype=np.float32)
+        self._check(self._lib.tgl_world_wall_reactions(self._handle, _ptr(out), out.size))
+        return out
+
+    def _fh_set_wall_reactions(self, xyz):
+        self._check(self._lib.tgl_world_set_wall_reactions(self._handle, _ptr(xyz), xyz.size))
+
+    def _fh_set_fiber_curvatures(self, values):
+        self._check(self._lib.tgl_world_set_fiber_max_curvatures(self._handle, _ptr(values), values.size))
 
     def packed(self):
         """DeviceWorld::packed() (plugin.rs:619-636): the uploaded host assembly."""

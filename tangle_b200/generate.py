@@ -10,8 +10,8 @@
   (population.rs:657-693), in that order. Python defaults follow
   crates/tangle_python/src/generators.rs:395-450 (length 16-24 diameters,
   curvature amplitude 0-0.8 diameters, 8 segments, seed 1).
-* `mid_size_specimen`, `cpu_runnable_specimen`, `batched_specimens` -- the
-  benchmark workloads: synthetic stand-ins with the shapes, sizes and value
+* `mid_size_specimen`, `cpu_runnable_specimen`, `batched_specimens`,
+  `ply_stack_specimen` -- the benchmark workloads: synthetic stand-ins with the shapes, sizes and value
   distributions of the configurations they are named after (no dataset is
   involved; every input is generated here from a seed).
 """
@@ -313,3 +313,84 @@ def batched_specimens(count: int = 512, seed: int = 1, max_fibers: int = 5000) -
             assembly.add_fiber(points, points, radius=0.5 * d, min_bend_radius=5.0 * d)
         out.append(assembly)
     return out
+
+
+def _normal_deviate(random: SplitMix64) -> float:
+    """Box-Muller from two unit draws (the first moved off zero)."""
+    u1 = max(random.unit(), 1.0e-300)
+    u2 = random.unit()
+    return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+
+
+def ply_stack_specimen(plies: int = 20, side: float = 2.0e-3, thickness: float = 0.1e-3, seed: int = 1,
+                       volume_fraction: float = 0.15, fiber_length: float = 1.0e-3, segment_over_d: float = 0.8,
+                       tilt_degrees: float = 3.0, rest_curvature_fraction: float = 0.5) -> FiberAssembly:
+    """A stack of planar plies, each side x side x thickness, periodic in x
+    and y with walls in z (the cell is plies x thickness high). Ply k holds 7
+    and 19 um fibers split 50:50 by fiber volume at `volume_fraction` of the
+    ply, directions uniform in the xy plane with a tilt out of it drawn from
+    N(0, tilt_degrees), centres uniform in the ply; each fiber's rest (and
+    initial) shape is a circular arc whose curvature is uniform in [0,
+    rest_curvature_fraction] x its limit 1/(5 d), bent in a random plane
+    through its axis. Segments are `segment_over_d` diameters long. Fiber f of
+    ply k carries formation step k and formation layer k, so a recipe
+    deposits the plies in sequence. The defaults give 20 plies of about
+    146,000 segments (2.9 M segments in all)."""
+    cell = Cell([side, side, plies * thickness], "xy")
+    assembly = FiberAssembly(cell)
+    random = SplitMix64(seed)
+    ply_volume = side * side * thickness
+    for k in range(plies):
+        for diameter in (19.0e-6, 7.0e-6):
+            radius = 0.5 * diameter
+            count = max(int(round(0.5 * volume_fraction * ply_volume / (math.pi * radius * radius * fiber_length))), 1)
+            segments = max(int(round(fiber_length / (segment_over_d * diameter))), 2)
+            limit = 1.0 / (5.0 * diameter)
+            s = (np.arange(segments + 1, dtype=np.float64) / segments - 0.5) * fiber_length
+            for _ in range(count):
+                azimuth = 2.0 * math.pi * random.unit()
+                tilt = math.radians(tilt_degrees) * _normal_deviate(random)
+                direction = np.array([math.cos(tilt) * math.cos(azimuth), math.cos(tilt) * math.sin(azimuth),
+                                      math.sin(tilt)])
+                ta = np.array(perpendicular(direction.tolist()))
+                tb = np.cross(direction, ta)
+                turn = 2.0 * math.pi * random.unit()
+                normal = math.cos(turn) * ta + math.sin(turn) * tb
+                curvature = rest_curvature_fraction * limit * random.unit()
+                center = np.array([side * random.unit(), side * random.unit(),
+                                   (k + 0.5 + 0.8 * (random.unit() - 0.5)) * thickness])
+                if curvature > 0.0:
+                    angle = s * curvature
+                    along = np.sin(angle) / curvature
+                    offset = (1.0 - np.cos(angle)) / curvature
+                else:
+                    along, offset = s, np.zeros_like(s)
+                points = center[None, :] + along[:, None] * direction[None, :] + offset[:, None] * normal[None, :]
+                index = assembly.add_fiber(points, points, radius=radius, min_bend_radius=5.0 * diameter)
+                assembly.set_fiber_formation_step(index, k)
+                assembly.set_fiber_formation_layer(index, k)
+    return assembly
+
+
+def layer_centers(assembly: FiberAssembly, axis: int) -> List[float]:
+    """The layer targets of a layered assembly along `axis`
+    (crates/tangle_generate/src/layered.rs:178-213): per formation layer
+    0..max, the f64 mean of its fibers' mean vertex coordinates (serial sums),
+    cast to f32. Every layer up to the largest must hold a fiber."""
+    layers = [f.formation_layer for f in assembly.fibers if f.formation_layer is not None]
+    if not layers:
+        raise ValueError("layered formation requires formation-layer labels")
+    sums = [0.0] * (max(layers) + 1)
+    counts = [0] * len(sums)
+    for fiber in assembly.fibers:
+        if fiber.formation_layer is None:
+            continue
+        values = fiber.placed[:, axis].tolist()
+        total = 0.0
+        for value in values:
+            total += value
+        sums[fiber.formation_layer] += total / len(values)
+        counts[fiber.formation_layer] += 1
+    if min(counts) == 0:
+        raise ValueError("formation layers must be contiguous and populated")
+    return [float(np.float32(total / count)) for total, count in zip(sums, counts)]
