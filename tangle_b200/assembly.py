@@ -113,6 +113,7 @@ class Fiber:
     min_bend_radius: Optional[float] = None
     formation_step: int = 0  # recipe step that inserts the fiber (assembly.rs formation_step)
     formation_layer: Optional[int] = None  # manufacturing layer (assembly.rs formation_layer)
+    material: Optional[str] = None  # material name (assembly.rs materials table)
 
 
 @dataclass
@@ -122,7 +123,8 @@ class FiberAssembly:
     cell: Cell
     fibers: List[Fiber] = field(default_factory=list)
 
-    def add_fiber(self, placed, intrinsic=None, *, radius: float, min_bend_radius: Optional[float] = None) -> int:
+    def add_fiber(self, placed, intrinsic=None, *, radius: float, min_bend_radius: Optional[float] = None,
+                  material: Optional[str] = None, formation_layer: Optional[int] = None) -> int:
         placed = np.asarray(placed, dtype=np.float64).reshape(-1, 3)
         intrinsic = placed.copy() if intrinsic is None else np.asarray(intrinsic, dtype=np.float64).reshape(-1, 3)
         if placed.shape[0] < 2:
@@ -133,7 +135,9 @@ class FiberAssembly:
             raise ValueError("fiber coordinates must be finite")
         if not (math.isfinite(radius) and radius > 0.0):
             raise ValueError("fiber radius must be positive and finite")
-        self.fibers.append(Fiber(placed, intrinsic, float(radius), min_bend_radius))
+        self.fibers.append(Fiber(placed, intrinsic, float(radius), min_bend_radius, 0, None, material))
+        if formation_layer is not None:
+            self.set_fiber_formation_layer(len(self.fibers) - 1, formation_layer)
         return len(self.fibers) - 1
 
     @property

@@ -181,7 +181,8 @@ def generate_fiber_population(cell: Cell, population: FiberPopulation) -> FiberA
         if placed_fiber is None:
             raise RuntimeError(f"could not place fiber {fiber_index} inside the cell")
         intrinsic, placed, radius = placed_fiber
-        assembly.add_fiber(placed, intrinsic, radius=radius, min_bend_radius=min_bend)
+        assembly.add_fiber(placed, intrinsic, radius=radius, min_bend_radius=min_bend,
+                           material=population.material.name)
     return assembly
 
 
@@ -366,7 +367,8 @@ def ply_stack_specimen(plies: int = 20, side: float = 2.0e-3, thickness: float =
                 else:
                     along, offset = s, np.zeros_like(s)
                 points = center[None, :] + along[:, None] * direction[None, :] + offset[:, None] * normal[None, :]
-                index = assembly.add_fiber(points, points, radius=radius, min_bend_radius=5.0 * diameter)
+                index = assembly.add_fiber(points, points, radius=radius, min_bend_radius=5.0 * diameter,
+                                           material=f"fiber_{round(diameter * 1e6)}um")
                 assembly.set_fiber_formation_step(index, k)
                 assembly.set_fiber_formation_layer(index, k)
     return assembly
@@ -394,3 +396,19 @@ def layer_centers(assembly: FiberAssembly, axis: int) -> List[float]:
     if min(counts) == 0:
         raise ValueError("formation layers must be contiguous and populated")
     return [float(np.float32(total / count)) for total, count in zip(sums, counts)]
+
+
+def ply_collections(stack: FiberAssembly) -> List[FiberAssembly]:
+    """The plies of a layered assembly as separate collections, in the
+    stack's cell: collection k holds layer k's fibers in order (with their
+    shapes, materials and layer labels), as a recipe inserts them one ply at
+    a time."""
+    layers = [f.formation_layer for f in stack.fibers if f.formation_layer is not None]
+    out = [FiberAssembly(stack.cell) for _ in range(max(layers) + 1 if layers else 0)]
+    for fiber in stack.fibers:
+        if fiber.formation_layer is None:
+            continue
+        out[fiber.formation_layer].add_fiber(fiber.placed, fiber.intrinsic, radius=fiber.radius,
+                                             min_bend_radius=fiber.min_bend_radius, material=fiber.material,
+                                             formation_layer=fiber.formation_layer)
+    return out

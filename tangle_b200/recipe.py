@@ -1,33 +1,44 @@
-"""`Recipe` / `RunResult`: the reference's Python entry point to relaxation.
+"""`Recipe` / `RunResult`: the reference's Python entry point to relaxation
+and formation.
 
-Mirrors crates/tangle_python/python/tangle/_tangle.pyi:915-1014 for the
-relaxation operations, and the run loop of
-crates/tangle_python/src/recipe.rs:618-723 with the batch controller of
-crates/tangle_relax/src/device/plugin.rs:1041-1181 and the operation
-controllers of crates/tangle_generate/src/recipe.rs:1311-1380:
+Mirrors crates/tangle_python/python/tangle/_tangle.pyi:898-1014 and
+crates/tangle_python/src/recipe.rs:240-560 for the recording side, and the
+run loop of crates/tangle_python/src/recipe.rs:618-723 with the batch
+controller of crates/tangle_relax/src/device/plugin.rs:1041-1181 and the
+formation operations of crates/tangle_generate/src/recipe.rs:859-1600:
 
+* every `insert` is a formation step: the whole recipe's fibers are uploaded
+  once and the step's fibers join the resident world when the step is
+  reached (activate_formation_step, no re-upload);
 * unset length settings are sized from the smallest fiber diameter;
 * a recipe that only inserts fibers relaxes them until converged;
 * each batch runs at most `iterations_per_batch` iterations and at most the
-  run-wide `max_iterations` remaining; `relax_for` forces full batches;
-* a `relax_until_converged` step that exhausts its budget raises
-  `RecipeError`.
+  run-wide `max_iterations` remaining; `relax_for` and `settle_targets`
+  force full batches;
+* layer operations hold layer targets on the stack axis (`scale_layer_spacing`,
+  `place_layer_above`) until `release_layer_placement` or the end of the
+  recipe; `fit_cell_to_active_fibers` moves the walls onto the active
+  fibers; `set_min_bend_radius` changes a material's curvature limit;
+* a step that exhausts its budget raises `RecipeError`.
 """
 
 from __future__ import annotations
 
 import copy
 from dataclasses import dataclass
-from typing import List, Optional, Union
+from typing import List, Optional, Sequence, Union
 
 import numpy as np
 
 from . import checkpoint as ckpt
-from .assembly import Cell, FiberAssembly, PackedAssembly
+from .assembly import Cell, FiberAssembly, Material, PackedAssembly
 from .checkpoint import CheckpointReport, CheckpointSettings
 from .device import DeviceWorld
-from .generate import FiberPopulation, generate_fiber_population
+from .formation import CompactionKinematics
+from .generate import FiberPopulation, generate_fiber_population, layer_centers
 from .settings import BatchStatus, RelaxationSettings
+
+DEFAULT_STACK_AXIS = 2
 
 
 class RecipeError(RuntimeError):
@@ -42,9 +53,35 @@ class RecipeError(RuntimeError):
 
 
 @dataclass
+class FiberSelection:
+    """The fibers one `insert` added (recipe.rs PyFiberSelection): their
+    indices in the recipe's assembly and their formation step."""
+
+    name: str
+    fibers: List[int]
+    formation_step: int
+
+
+class HeldTargets:
+    """Returned by operations that hold fibers on targets (_tangle.pyi:898-913):
+    as a context manager it records the matching release when the block ends."""
+
+    def __init__(self, recipe: "Recipe", release):
+        self._recipe = recipe
+        self._release = release
+
+    def __enter__(self) -> "Recipe":
+        return self._recipe
+
+    def __exit__(self, exc_type=None, exc=None, traceback=None) -> bool:
+        self._release()
+        return False
+
+
+@dataclass
 class _Insert:
-    assembly: FiberAssembly
-    count: int = 0  # fibers this step adds
+    step: int
+    count: int
 
 
 @dataclass
@@ -57,11 +94,50 @@ class _RelaxFor:
     iterations: int
 
 
+@dataclass
+class _SettleTargets:
+    tolerance: float
+    maximum_iterations: int
+
+
+@dataclass
+class _SetMinBendRadius:
+    material: str
+    minimum_bend_radius: float
+
+
+@dataclass
+class _ScaleLayerSpacing:
+    factor: float
+    stiffness: float
+    max_translation: float
+
+
+@dataclass
+class _PlaceLayerAbove:
+    layer: int
+    gap: float
+    stiffness: float
+    max_translation: float
+
+
+@dataclass
+class _ReleaseLayerPlacement:
+    pass
+
+
+@dataclass
+class _FitCell:
+    axes: List[bool]
+    padding: float
+
+
 class RunResult:
     """The relaxed fibers and run statistics (_tangle.pyi:1003-1014)."""
 
     def __init__(self, assembly: FiberAssembly, status: BatchStatus, uploaded_bytes: int, downloaded_bytes: int,
-                 cell_size: float, cell_count: int, rebuilds: int, report: Optional[CheckpointReport] = None):
+                 cell_size: float, cell_count: int, rebuilds: int, report: Optional[CheckpointReport] = None,
+                 events: Optional[List[str]] = None):
         self.assembly = assembly
         self._status = status
         self.uploaded_bytes = uploaded_bytes
@@ -69,6 +145,7 @@ class RunResult:
         self.cell_size = cell_size
         self.cell_count = cell_count
         self.neighbor_list_rebuilds = rebuilds
+        self.events = list(events or [])
         report = report or CheckpointReport()
         self.resumed = report.resumed
         self.resumed_iteration = report.resumed_iteration
@@ -98,45 +175,173 @@ def _upload_bytes(packed: PackedAssembly) -> int:
     return int(sum(a.nbytes for a in arrays)) + 6 * 4 + 3 * 4
 
 
+def infer_stack_axis(periodic: Sequence[bool]) -> int:
+    """collection.rs:104-112: z unless it is periodic, else the last walled axis."""
+    if not periodic[DEFAULT_STACK_AXIS]:
+        return DEFAULT_STACK_AXIS
+    for axis in (2, 1, 0):
+        if not periodic[axis]:
+            return axis
+    return DEFAULT_STACK_AXIS
+
+
+def _positive(value: float, name: str) -> float:
+    value = float(value)
+    if not (np.isfinite(value) and value > 0.0):
+        raise ValueError(f"{name} must be positive and finite")
+    return value
+
+
+def _unit_fraction(value: float, name: str) -> float:
+    value = float(value)
+    if not (0.0 < value <= 1.0):
+        raise ValueError(f"{name} must be in (0, 1]")
+    return value
+
+
+def active_capsule_bounds(packed: PackedAssembly, positions: np.ndarray, fiber_active: np.ndarray,
+                          padding: float):
+    """compaction_control.rs:446-474: the box around every active segment's
+    capsule (its endpoints grown by its radius plus `padding`), in f32."""
+    active = np.asarray(fiber_active, dtype=bool)[np.asarray(packed.segment_fibers)]
+    if not np.any(active):
+        raise ValueError("cannot fit a cell without active fiber segments")
+    xyz = np.asarray(positions, dtype=np.float32).reshape(-1, 3)
+    ends = np.asarray(packed.segment_vertices).reshape(-1, 2)[active]
+    grow = (np.asarray(packed.segment_radii, dtype=np.float32)[active] + np.float32(padding))[:, None]
+    lower = np.minimum((xyz[ends[:, 0]] - grow).min(axis=0), (xyz[ends[:, 1]] - grow).min(axis=0))
+    upper = np.maximum((xyz[ends[:, 0]] + grow).max(axis=0), (xyz[ends[:, 1]] + grow).max(axis=0))
+    return lower.astype(np.float32), upper.astype(np.float32)
+
+
 class Recipe:
     """An ordered list of steps on one cell; nothing runs until `run`."""
 
-    def __init__(self, cell: Union[Cell, FiberAssembly]):
+    def __init__(self, cell: Union[Cell, FiberAssembly], *, stack_axis: Optional[int] = None):
         if isinstance(cell, FiberAssembly):
             self._assembly = copy.deepcopy(cell)
         elif isinstance(cell, Cell):
             self._assembly = FiberAssembly(cell)
         else:
             raise TypeError("Recipe needs a Cell or a FiberAssembly")
+        if stack_axis is None:
+            stack_axis = infer_stack_axis(self._assembly.cell.periodic)
+        if stack_axis not in (0, 1, 2):
+            raise ValueError("stack_axis must be 0, 1 or 2")
+        self._stack_axis = int(stack_axis)
         self._operations: list = []
         self._descriptions: List[str] = []
+        self._next_step = 0
 
     @property
     def cell(self) -> Cell:
         return self._assembly.cell
 
-    def insert(self, collection) -> None:
+    @property
+    def stack_axis(self) -> int:
+        return self._stack_axis
+
+    def _push(self, operation, description: str) -> None:
+        self._operations.append(operation)
+        self._descriptions.append(description)
+
+    def insert(self, collection, *, name: Optional[str] = None, translation: Sequence[float] = (0.0, 0.0, 0.0),
+               rotation: Optional[Sequence[Sequence[float]]] = None) -> FiberSelection:
+        """recipe.rs:249-296: the collection's fibers, rotated then
+        translated, become the next formation step."""
         if isinstance(collection, FiberPopulation):
             collection = generate_fiber_population(self._assembly.cell, collection)
         if not isinstance(collection, FiberAssembly):
             raise TypeError("insert takes a FiberAssembly (a generated collection) or a FiberPopulation")
+        if not collection.fibers:
+            raise ValueError("cannot insert an empty fiber collection")
+        rotation = np.eye(3) if rotation is None else np.asarray(rotation, dtype=np.float64)
+        translation = np.asarray(translation, dtype=np.float64)
+        if rotation.shape != (3, 3) or translation.shape != (3,):
+            raise ValueError("rotation must be 3x3 and translation three values")
+        step = self._next_step
+        self._next_step += 1
+        indices = []
         for fiber in collection.fibers:
-            self._assembly.add_fiber(fiber.placed, fiber.intrinsic, radius=fiber.radius,
-                                     min_bend_radius=fiber.min_bend_radius)
-        self._operations.append(_Insert(collection, collection.fiber_count))
-        self._descriptions.append(f"insert {collection.fiber_count} fibers")
+            index = self._assembly.add_fiber(fiber.placed @ rotation.T + translation,
+                                             fiber.intrinsic @ rotation.T + translation, radius=fiber.radius,
+                                             min_bend_radius=fiber.min_bend_radius, material=fiber.material,
+                                             formation_layer=fiber.formation_layer)
+            self._assembly.set_fiber_formation_step(index, step)
+            indices.append(index)
+        name = name or "collection"
+        self._push(_Insert(step, len(indices)),
+                   f"insert {name!r} ({len(indices)} fibers) as formation step {step}")
+        return FiberSelection(name, indices, step)
 
     def relax_until_converged(self, *, max_iterations: int = 2000) -> None:
         if max_iterations <= 0:
             raise ValueError("max_iterations must be positive")
-        self._operations.append(_RelaxUntilConverged(int(max_iterations)))
-        self._descriptions.append("relax until converged")
+        self._push(_RelaxUntilConverged(int(max_iterations)), "relax until converged")
 
     def relax_for(self, iterations: int) -> None:
         if iterations <= 0:
             raise ValueError("iterations must be positive")
-        self._operations.append(_RelaxFor(int(iterations)))
-        self._descriptions.append(f"relax for {iterations} iterations")
+        self._push(_RelaxFor(int(iterations)), f"relax for {iterations} iterations")
+
+    def settle_targets(self, *, tolerance: float, max_iterations: int) -> None:
+        """recipe.rs:328-342: relax in full batches until every held target
+        is within `tolerance`."""
+        tolerance = float(tolerance)
+        if not (np.isfinite(tolerance) and tolerance >= 0.0):
+            raise ValueError("tolerance must be non-negative and finite")
+        if max_iterations <= 0:
+            raise ValueError("max_iterations must be positive")
+        self._push(_SettleTargets(tolerance, int(max_iterations)), f"settle held targets to tolerance {tolerance}")
+
+    def set_min_bend_radius(self, material: Union[Material, str], min_bend_radius: float) -> None:
+        """recipe.rs:366-394: every fiber of `material` takes this bend limit."""
+        name = material.name if isinstance(material, Material) else material
+        if not isinstance(name, str):
+            raise TypeError("material must be a Material or a material name")
+        if not name.strip():
+            raise ValueError("material name must not be empty")
+        radius = _positive(min_bend_radius, "min_bend_radius")
+        self._push(_SetMinBendRadius(name, radius), f"set {name!r} minimum bend radius to {radius:.3e}")
+
+    def scale_layer_spacing(self, factor: float, *, stiffness: float = 0.25,
+                            max_translation: float = 1.0e-5) -> HeldTargets:
+        """recipe.rs:396-415 (MoveLayers): every layer's target moves to the
+        cell centre plus `factor` times its initial offset."""
+        self._push(_ScaleLayerSpacing(_positive(factor, "factor"), _unit_fraction(stiffness, "stiffness"),
+                                      _positive(max_translation, "max_translation")),
+                   f"scale layer spacing by {factor}")
+        return HeldTargets(self, self.release_layer_placement)
+
+    def place_layer_above(self, layer: int, *, gap: float, stiffness: float = 0.25,
+                          max_translation: float = 1.0e-5) -> HeldTargets:
+        """recipe.rs:419-443 (PlaceLayerAbove): layer `layer` is held `gap`
+        above layer `layer - 1`'s target."""
+        if int(layer) <= 0:
+            raise ValueError("layer must be greater than zero")
+        self._push(_PlaceLayerAbove(int(layer), _positive(gap, "gap"), _unit_fraction(stiffness, "stiffness"),
+                                    _positive(max_translation, "max_translation")),
+                   f"place layer {layer} above layer {int(layer) - 1}")
+        return HeldTargets(self, self.release_layer_placement)
+
+    def release_layer_placement(self) -> None:
+        self._push(_ReleaseLayerPlacement(), "release layer placement")
+
+    def fit_cell_to_active_fibers(self, *, axes: Optional[Sequence[bool]] = None, padding: float = 0.0) -> None:
+        """recipe.rs:515-545 (FitCellToActiveFibers): the walls of the chosen
+        axes (the stack axis by default) move onto the active fibers."""
+        if axes is None:
+            axes = [axis == self._stack_axis for axis in range(3)]
+        axes = [bool(a) for a in axes]
+        if len(axes) != 3 or not any(axes):
+            raise ValueError("at least one cell-fit axis must be selected")
+        padding = float(padding)
+        if not (np.isfinite(padding) and padding >= 0.0):
+            raise ValueError("padding must be non-negative and finite")
+        for axis in range(3):
+            if axes[axis] and self._assembly.cell.periodic[axis]:
+                raise ValueError(f"cannot fit periodic cell axis {axis} to active fibers")
+        self._push(_FitCell(axes, padding), f"fit cell to active fibers with {padding:.3e} padding")
 
     def operations(self) -> List[str]:
         return list(self._descriptions)
@@ -145,7 +350,7 @@ class Recipe:
         return self._assembly.centerlines()
 
     def run(self, settings: Optional[RelaxationSettings] = None, *,
-            checkpoint: Optional[CheckpointSettings] = None) -> RunResult:
+            checkpoint: Optional[CheckpointSettings] = None, world_factory=None) -> RunResult:
         """Simulates every recorded step and returns the relaxed fibers.
 
         With `checkpoint`, the run saves a restart file whenever the lifetime
@@ -153,6 +358,8 @@ class Recipe:
         it ends; with `checkpoint.resume` it first restores the world and the
         recipe's progress from `resume_path` (or `path`), or only the world
         when `fresh_formation_on_resume` (tangle_checkpoint lib.rs:214-345).
+        `world_factory(packed, cell_list, max_step)` replaces the CUDA world
+        (tests drive the oracle through it).
         """
         if not self._assembly.fibers:
             raise ValueError("recipe contains no fibers")
@@ -169,55 +376,26 @@ class Recipe:
             operations.append(_RelaxUntilConverged(config.max_iterations))
             descriptions.append("relax until converged")
         assembly = copy.deepcopy(self._assembly)
-        # Staged activation (kernels.rs:164-221): the fibers of an insert step
-        # take part from that step on. The world holds the fibers active so
-        # far; when a relaxation step follows new inserts, it is re-created
-        # from the relaxed positions plus the new fibers (the lifetime
-        # iteration count carries over). Lists only need to be supersets of
-        # the contacts, so this moves nothing differently from masking.
-        active_after, active = [], 0
-        for op in operations:
-            if isinstance(op, _Insert):
-                active += op.count
-            active_after.append(active)
+        axis = self._stack_axis
         status = BatchStatus(max_penetration=float("inf"), max_curvature_ratio=float("inf"))
         report = CheckpointReport()
+        events: List[str] = []
         first_operation, first_completed = 0, 0
-        world, world_fibers, packed, uploaded = None, 0, None, 0
-
-        def first_fibers(k: int) -> FiberAssembly:
-            sub = FiberAssembly(assembly.cell)
-            for fiber in assembly.fibers[:k]:
-                sub.add_fiber(fiber.placed, fiber.intrinsic, radius=fiber.radius,
-                              min_bend_radius=fiber.min_bend_radius)
-            return sub
-
-        def activate(k: int) -> None:
-            nonlocal world, world_fibers, packed, uploaded
-            if world is not None:
-                if k == world_fibers:
-                    return
-                packed.unpack_positions(world.download_positions(), assembly)
-                world.close()
-            packed = PackedAssembly.from_assembly(first_fibers(k), config.pin_fiber_ends)
-            world = DeviceWorld(packed, config.cell_list, config.max_step,
-                                status.total_iterations if status.total_iterations else None)
-            uploaded += _upload_bytes(packed)
-            world_fibers = k
-
+        packed = PackedAssembly.from_assembly(assembly, config.pin_fiber_ends)
+        uploaded = _upload_bytes(packed)
+        factory = world_factory or (lambda p, cl, step: DeviceWorld(p, cl, step))
+        world = None
         if checkpoint is not None and checkpoint.resume:
             source = checkpoint.resume_path or checkpoint.path
             saved = ckpt.load(source, checkpoint.resume_case_id or checkpoint.case_id)
-            k = saved.device.packed.fiber_count
-            expected = PackedAssembly.from_assembly(first_fibers(k), config.pin_fiber_ends) if k <= len(
-                assembly.fibers) else None
-            if expected is None or saved.device.packed.vertex_count != expected.vertex_count or \
-                    saved.device.packed.segment_count != expected.segment_count:
+            sp = saved.device.packed
+            if (sp.fiber_count, sp.vertex_count, sp.segment_count) != (packed.fiber_count, packed.vertex_count,
+                                                                       packed.segment_count):
                 raise ckpt.CheckpointError("checkpoint assembly does not match the recipe's fibers")
+            if world_factory is not None:
+                raise ValueError("a resumed run restores the CUDA world")
             world = DeviceWorld.restore(config, saved.device)
-            packed = saved.device.packed
-            world_fibers = k
-            uploaded += _upload_bytes(packed)
+            packed = sp
             status = BatchStatus(total_iterations=saved.device.total_iterations, max_penetration=float("inf"),
                                  max_curvature_ratio=float("inf"))
             if not checkpoint.fresh_formation_on_resume:
@@ -226,7 +404,11 @@ class Recipe:
             report.resumed = True
             report.resumed_iteration = saved.device.total_iterations
             report.last_saved_iteration = saved.device.total_iterations
+        else:
+            world = factory(packed, config.cell_list, config.max_step)
         downloaded = 0
+        initial_targets: List[float] = []
+        current_targets: List[float] = []
 
         def save(index: int, completed: int, terminal: bool) -> None:
             nonlocal downloaded
@@ -246,48 +428,132 @@ class Recipe:
             report.last_saved_iteration = iteration
             report.last_saved_bytes = size
 
+        def relax(index: int, budget: int, force: bool, done) -> None:
+            """Batches until done() or the budget is spent (then RecipeError
+            unless the step is a fixed interval)."""
+            nonlocal status, downloaded
+            started = status.total_iterations - (first_completed if index == first_operation else 0)
+            while True:
+                completed = status.total_iterations - started
+                if done():
+                    return
+                if completed >= budget:
+                    if force and not isinstance(operations[index], _SettleTargets):
+                        return
+                    raise RecipeError(index, descriptions[index], status.total_iterations, failure(budget))
+                remaining = config.max_iterations - status.total_iterations
+                if remaining <= 0:
+                    raise RecipeError(index, descriptions[index], status.total_iterations,
+                                      "run-wide max_iterations exhausted")
+                batch = min(remaining, config.iterations_per_batch, budget - completed)
+                batch_config = copy.copy(config)
+                batch_config.force_full_iterations = config.force_full_iterations or force
+                status = world.run_batch(batch_config, batch)
+                downloaded += 11 * 4 + 3 * 4
+                if status.cell_list_overflow:
+                    save(index, status.total_iterations - started, True)
+                    raise RecipeError(index, descriptions[index], status.total_iterations, "cell list overflow")
+                save(index, status.total_iterations - started, False)
+
+        def failure(budget: int) -> str:
+            op = operations[current]
+            if isinstance(op, _SettleTargets):
+                error = world.formation_target_error()
+                worst = max(v for v in (error.layer, error.vertex) if v is not None)
+                return (f"formation targets remained at residual {worst:.3e} after {budget} iterations "
+                        f"(tolerance {op.tolerance:.3e})")
+            return (f"failed to converge in {budget} iterations: penetration {status.max_penetration:.3e}, "
+                    f"curvature ratio {status.max_curvature_ratio:.6f}")
+
+        def ensure_layer_targets() -> None:
+            if not initial_targets:
+                initial_targets.extend(layer_centers(assembly, axis))
+                current_targets.extend(initial_targets)
+
+        current = 0
         try:
             for index, op in enumerate(operations):
-                if isinstance(op, _Insert) or index < first_operation:
+                current = index
+                if index < first_operation:
                     continue
-                activate(active_after[index])
-                started = status.total_iterations - (first_completed if index == first_operation else 0)
-                force = isinstance(op, _RelaxFor)
-                budget = op.iterations if force else op.maximum_iterations
-                while True:
-                    completed = status.total_iterations - started
-                    if not force and status.converged:
-                        break
-                    if completed >= budget:
-                        if force:
-                            break
-                        raise RecipeError(index, descriptions[index], status.total_iterations,
-                                          f"failed to converge in {budget} iterations: penetration "
-                                          f"{status.max_penetration:.3e}, curvature ratio "
-                                          f"{status.max_curvature_ratio:.6f}")
-                    remaining = config.max_iterations - status.total_iterations
-                    if remaining <= 0:
-                        raise RecipeError(index, descriptions[index], status.total_iterations,
-                                          "run-wide max_iterations exhausted")
-                    batch = min(remaining, config.iterations_per_batch, budget - completed)
-                    batch_config = copy.copy(config)
-                    batch_config.force_full_iterations = config.force_full_iterations or force
-                    status = world.run_batch(batch_config, batch)
-                    downloaded += 11 * 4 + 3 * 4
-                    if status.cell_list_overflow:
-                        save(index, status.total_iterations - started, True)
-                        raise RecipeError(index, descriptions[index], status.total_iterations, "cell list overflow")
-                    save(index, status.total_iterations - started, False)
-                if force:
+                if isinstance(op, _Insert):
+                    # recipe.rs:925-946: the step's fibers join the resident world.
+                    world.activate_formation_step(op.step)
                     status.converged = False
-            if world is None:  # nothing to relax: the fibers stay where they were placed
-                activate(active_after[-1])
+                elif isinstance(op, (_RelaxUntilConverged, _RelaxFor)):
+                    force = isinstance(op, _RelaxFor)
+                    budget = op.iterations if force else op.maximum_iterations
+                    relax(index, budget, force, lambda: not force and status.converged)
+                    if force:
+                        status.converged = False
+                elif isinstance(op, _SettleTargets):
+                    def settled(op=op):
+                        error = world.formation_target_error()
+                        values = [v for v in (error.layer, error.vertex) if v is not None]
+                        return not values or max(values) <= op.tolerance
+                    relax(index, op.maximum_iterations, True, settled)
+                    status.converged = False
+                elif isinstance(op, _SetMinBendRadius):
+                    # recipe.rs:947-1007.
+                    matching = [i for i, f in enumerate(assembly.fibers) if f.material == op.material]
+                    if not matching:
+                        known = sorted({f.material for f in assembly.fibers if f.material is not None})
+                        raise RecipeError(index, descriptions[index], status.total_iterations,
+                                          f"unknown material {op.material!r}; known materials: {known}")
+                    for i in matching:
+                        assembly.fibers[i].min_bend_radius = op.minimum_bend_radius
+                    limits = np.array([0.0 if f.min_bend_radius is None else np.float32(1.0 / f.min_bend_radius)
+                                       for f in assembly.fibers], dtype=np.float32)
+                    world.set_fiber_maximum_curvatures(limits)
+                    status.converged = False
+                elif isinstance(op, _ScaleLayerSpacing):
+                    # recipe.rs:1008-1046 (MoveLayers).
+                    ensure_layer_targets()
+                    lower = np.float64(assembly.cell.origin[axis])
+                    center = np.float32(lower + 0.5 * assembly.cell.lengths[axis])
+                    current_targets[:] = [float(center + (np.float32(t) - center) * np.float32(op.factor))
+                                          for t in initial_targets]
+                    world.apply_layer_targets(axis, current_targets, op.stiffness, op.max_translation)
+                    status.converged = False
+                elif isinstance(op, _PlaceLayerAbove):
+                    # recipe.rs:1047-1085.
+                    ensure_layer_targets()
+                    if op.layer >= len(current_targets):
+                        raise RecipeError(index, descriptions[index], status.total_iterations,
+                                          f"cannot place layer {op.layer}: only {len(current_targets)} layers exist")
+                    current_targets[op.layer] = float(np.float32(current_targets[op.layer - 1]) + np.float32(op.gap))
+                    world.apply_single_layer_target(axis, current_targets, op.layer, op.stiffness,
+                                                    op.max_translation)
+                    status.converged = False
+                elif isinstance(op, _ReleaseLayerPlacement):
+                    world.clear_layer_targets()
+                    status.converged = False
+                elif isinstance(op, _FitCell):
+                    # recipe.rs:1205-1255: walls onto the active capsules.
+                    positions = world.download_positions()
+                    downloaded += positions.nbytes
+                    old_lower, old_upper = world.cell_bounds()
+                    fiber_lower, fiber_upper = active_capsule_bounds(packed, positions, world.fiber_active,
+                                                                     op.padding)
+                    new_lower = [max(float(fiber_lower[a]), old_lower[a]) if op.axes[a] else old_lower[a]
+                                 for a in range(3)]
+                    new_upper = [min(float(fiber_upper[a]), old_upper[a]) if op.axes[a] else old_upper[a]
+                                 for a in range(3)]
+                    world.compact_cell(new_lower, new_upper, CompactionKinematics.MOVING_WALLS)
+                    lower, upper = world.cell_bounds()
+                    assembly.cell = Cell([u - l for l, u in zip(lower, upper)], assembly.cell.periodic, lower)
+                    status.converged = False
+                events.append(descriptions[index])
+            # recipe.rs:905-921: the recipe ends with its targets released.
+            world.clear_layer_targets()
+            world.clear_vertex_targets()
             save(len(operations), 0, True)
             positions = world.download_positions()
             downloaded += positions.nbytes
-            packed.unpack_positions(positions, assembly)
+            world.unpack_positions(positions, assembly)
             return RunResult(assembly, status, uploaded, downloaded, world.cell_size, world.cell_count,
-                             world.neighbor_list_rebuilds(), report)
+                             world.neighbor_list_rebuilds(), report, events)
         finally:
-            if world is not None:
-                world.close()
+            close = getattr(world, "close", None)
+            if close is not None:
+                close()
