@@ -55,7 +55,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
-    ap.add_argument("--workload", choices=["mid_size", "cpu_runnable", "batched"], default="mid_size")
+    ap.add_argument("--workload", choices=["mid_size", "cpu_runnable", "batched", "ply_stack"], default="mid_size")
+    ap.add_argument("--plies", type=int, default=20, help="plies of the ply_stack workload")
+    ap.add_argument("--ply-budget", type=int, default=1024, help="iteration cap per ply of the ply_stack workload")
+    ap.add_argument("--ply-side", type=float, default=2.0e-3, help="ply edge of the ply_stack workload (m)")
     ap.add_argument("--specimens", type=int, default=512, help="specimens of the batched workload")
     ap.add_argument("--iterations", type=int, default=128, help="relaxation iterations per step")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the mid-size cell (tests only)")
@@ -291,6 +294,105 @@ def arena_time_to_admissible(packs, config, limit):
             "iterations_cap": limit, "seconds_p50": pct(done, 50), "seconds_p90": pct(done, 90),
             "seconds_max": max(done) if done else None, "iterations_p50": pct(its, 50),
             "iterations_p90": pct(its, 90), "iterations_max": max(its) if its else None, "method": "plain PBD"}
+
+
+PLY_MILESTONES = (0.2, 0.1, 0.05)
+
+
+def ply_stack_deposition(assembly, packed, config, d_min, plies, budget, net):
+    """The 20-ply formation sequence on one resident world: for each ply,
+    activate its formation step (the ply was generated in place, one ply
+    thickness above the previous), optionally apply the learned warm start,
+    and relax until the gate holds or `budget` iterations. Returns the whole
+    job's wall time (host-driven, inputs resident), per-ply records and the
+    node-iterations done."""
+    import torch
+
+    from tangle_b200.device import DeviceWorld
+
+    world = DeviceWorld(packed, config.cell_list, config.max_step)
+    records = []
+    node_iterations = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(plies):
+        tk = time.perf_counter()
+        _, vertices = world.activate_formation_step(k)
+        accepted = None
+        if net is not None:
+            from tangle_b200.warmstart import warm_start
+
+            accepted = warm_start(world, net, config).accepted
+        start = None
+        status = None
+        reached = {}
+        while True:
+            status = world.run_batch(config, min(config.iterations_per_batch, budget))
+            if start is None:
+                start = status.total_iterations - status.batch_iterations
+            done = status.total_iterations - start
+            for m in PLY_MILESTONES:
+                if m not in reached and status.max_penetration <= m * d_min:
+                    reached[m] = {"iterations": done, "seconds": time.perf_counter() - tk}
+            if status.converged or done >= budget:
+                break
+        node_iterations += vertices * done
+        records.append({"ply": k, "active_vertices": vertices, "iterations": done, "converged": status.converged,
+                        "seconds": time.perf_counter() - tk,
+                        "max_penetration_over_d": status.max_penetration / d_min,
+                        "max_curvature_ratio": status.max_curvature_ratio, "warm_start_accepted": accepted,
+                        "milestones_over_d": {str(m): reached.get(m) for m in PLY_MILESTONES}})
+    torch.cuda.synchronize()
+    seconds = time.perf_counter() - t0
+    world.close()
+    return seconds, node_iterations, records
+
+
+def run_ply_stack(args):
+    """The 20-ply stack (2 x 2 x 0.1 mm plies, periodic x/y, z walls, 7/19
+    um at 15 % per ply, rest curvature up to half the limit, ~2.9 M
+    segments), deposited ply by ply on one world, with plain PBD and with the
+    learned warm start per ply: whole-job seconds (lower is better) and the
+    node-iterations per second of the relaxation."""
+    import torch
+
+    from tangle_b200.assembly import PackedAssembly
+    from tangle_b200.build import build
+    from tangle_b200.generate import ply_stack_specimen
+    from tangle_b200.settings import RelaxationSettings
+
+    build()
+    torch.cuda.set_device(0)
+    assembly = ply_stack_specimen(plies=args.plies, side=args.ply_side)
+    packed = PackedAssembly.from_assembly(assembly)
+    d_min = assembly.smallest_diameter()
+    settings = RelaxationSettings(penetration_tolerance=1.0e-3 * d_min, neighbor_capacity=args.capacity,
+                                  max_list_bytes=8 << 30, iterations_per_batch=64, max_iterations=1 << 30)
+    config = settings.to_config(d_min)
+    runs = {}
+    net = load_warmstart_net()
+    for label, use_net in (("plain", None), ("warm_start", net)):
+        if label == "warm_start" and net is None:
+            continue
+        seconds, node_iterations, records = ply_stack_deposition(assembly, packed, config, d_min, args.plies,
+                                                                 args.ply_budget, use_net)
+        runs[label] = {"seconds": seconds, "node_iterations": node_iterations,
+                       "node_iter_per_s": node_iterations / seconds if seconds > 0 else None,
+                       "iterations": sum(r["iterations"] for r in records),
+                       "plies_converged": sum(1 for r in records if r["converged"]), "plies": records}
+    plain = runs["plain"]
+    line = {"metric": "s to deposit and relax a 20-ply stack ply by ply (gate: overlap < 1e-3 d per ply)",
+            "value": plain["seconds"], "unit": "s", "n_gpus": 1, "higher_is_better": False, "dtype": "f32",
+            "data": "synthetic", "impl": "cuda",
+            "config": {"workload": (f"ply_stack: {args.plies} plies {args.ply_side * 1e3:g} x {args.ply_side * 1e3:g}"
+                                    " x 0.1 mm, periodic xy, z walls, 7/19 um 50:50 by volume at 15 % per ply, "
+                                    "xy directions with N(0, 3 deg) tilt, rest curvature up to 0.5 x limit 1/(5d), "
+                                    "segment 0.8 d, 1 mm fibers"),
+                       "nodes": packed.vertex_count, "segments": packed.segment_count,
+                       "fibers": packed.fiber_count, "ply_iteration_cap": args.ply_budget},
+            "runs": runs}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def load_warmstart_net():
@@ -568,6 +670,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ply_stack":
+        return run_ply_stack(args)
     return run_cuda(args)
 
 

@@ -372,7 +372,7 @@ __global__ void node_features_kernel(WorldDev w, GraphBuffers g, MpGraph graph) 
 __global__ void displace_kernel(WorldDev w, const float *dx, int64_t ld, float scale, int in_diameters,
                                 float max_step) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x) {
-        if (w.pinned[v]) continue;
+        if (w.pinned[v] || !vertex_on(w, v)) continue;  // frozen (inactive) fibers stay put
         const float k0 = in_diameters ? scale * 2.0f * w.vtx_static[v].w : scale;
         float mx = k0 * dx[v * ld], my = k0 * dx[v * ld + 1], mz = k0 * dx[v * ld + 2];
         const float m = sqrtf(mx * mx + my * my + mz * mz);

@@ -331,9 +331,10 @@ def ply_stack_specimen(plies: int = 20, side: float = 2.0e-3, thickness: float =
     and 19 um fibers split 50:50 by fiber volume at `volume_fraction` of the
     ply, directions uniform in the xy plane with a tilt out of it drawn from
     N(0, tilt_degrees), centres uniform in the ply; each fiber's rest (and
-    initial) shape is a circular arc whose curvature is uniform in [0,
-    rest_curvature_fraction] x its limit 1/(5 d), bent in a random plane
-    through its axis. Segments are `segment_over_d` diameters long. Fiber f of
+    initial) shape is a waviness of wavelength 20 d in a random plane through
+    its axis whose peak curvature is uniform in [0, rest_curvature_fraction] x
+    its limit 1/(5 d); a fiber whose tilt reaches past a wall moves along z
+    until it lies inside. Segments are `segment_over_d` diameters long. Fiber f of
     ply k carries formation step k and formation layer k, so a recipe
     deposits the plies in sequence. The defaults give 20 plies of about
     146,000 segments (2.9 M segments in all)."""
@@ -350,23 +351,35 @@ def ply_stack_specimen(plies: int = 20, side: float = 2.0e-3, thickness: float =
             s = (np.arange(segments + 1, dtype=np.float64) / segments - 0.5) * fiber_length
             for _ in range(count):
                 azimuth = 2.0 * math.pi * random.unit()
-                tilt = math.radians(tilt_degrees) * _normal_deviate(random)
-                direction = np.array([math.cos(tilt) * math.cos(azimuth), math.cos(tilt) * math.sin(azimuth),
-                                      math.sin(tilt)])
-                ta = np.array(perpendicular(direction.tolist()))
-                tb = np.cross(direction, ta)
                 turn = 2.0 * math.pi * random.unit()
-                normal = math.cos(turn) * ta + math.sin(turn) * tb
-                curvature = rest_curvature_fraction * limit * random.unit()
+                peak = rest_curvature_fraction * limit * random.unit()
+                phase = 2.0 * math.pi * random.unit()
                 center = np.array([side * random.unit(), side * random.unit(),
                                    (k + 0.5 + 0.8 * (random.unit() - 0.5)) * thickness])
-                if curvature > 0.0:
-                    angle = s * curvature
-                    along = np.sin(angle) / curvature
-                    offset = (1.0 - np.cos(angle)) / curvature
-                else:
-                    along, offset = s, np.zeros_like(s)
-                points = center[None, :] + along[:, None] * direction[None, :] + offset[:, None] * normal[None, :]
+                # Waviness of wavelength 20 d whose peak curvature
+                # amplitude * (2 pi / wavelength)^2 is `peak`.
+                wavelength = 20.0 * diameter
+                amplitude = peak * (wavelength / (2.0 * math.pi)) ** 2
+                along = s
+                offset = amplitude * np.sin(2.0 * math.pi * s / wavelength + phase)
+                # The tilt is redrawn until the fiber fits between the walls
+                # (flat after 64 draws), and the centre moves along z until
+                # the whole fiber lies inside, as population.rs:657-693
+                # contains a centre.
+                for attempt in range(65):
+                    tilt = math.radians(tilt_degrees) * _normal_deviate(random) if attempt < 64 else 0.0
+                    direction = np.array([math.cos(tilt) * math.cos(azimuth), math.cos(tilt) * math.sin(azimuth),
+                                          math.sin(tilt)])
+                    ta = np.array(perpendicular(direction.tolist()))
+                    tb = np.cross(direction, ta)
+                    normal = math.cos(turn) * ta + math.sin(turn) * tb
+                    shape = along[:, None] * direction[None, :] + offset[:, None] * normal[None, :]
+                    low = radius - shape[:, 2].min()
+                    high = plies * thickness - radius - shape[:, 2].max()
+                    if low <= high:
+                        break
+                center[2] = min(max(center[2], low), high)
+                points = center[None, :] + shape
                 index = assembly.add_fiber(points, points, radius=radius, min_bend_radius=5.0 * diameter,
                                            material=f"fiber_{round(diameter * 1e6)}um")
                 assembly.set_fiber_formation_step(index, k)

@@ -241,7 +241,10 @@ def test_ply_stack_layout():
     assert 140_000 < p.segment_count / 2 < 155_000
     assert p.fiber_vertex_spans.reshape(-1, 2)[:, 1].max() <= 256
     centers = layer_centers(a, 2)
-    assert len(centers) == 2 and abs(centers[0] - 0.05e-3) < 0.01e-3 and abs(centers[1] - 0.15e-3) < 0.01e-3
+    assert len(centers) == 2 and 0.0 < centers[0] < centers[1] < 0.2e-3
+    z = np.concatenate([f.placed[:, 2] for f in a.fibers])
+    r = np.concatenate([np.full(len(f.placed), f.radius) for f in a.fibers])
+    assert np.all(z - r >= -1e-12) and np.all(z + r <= 0.2e-3 + 1e-12)  # every fiber inside the walls
 
 
 # --------------------------------------------------------------------- parity
