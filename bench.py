@@ -83,6 +83,23 @@ def dist_env():
     return rank, world, local
 
 
+def replica_throughput(seconds: float, work: float, world_size: int, device: str = "cuda"):
+    """Whole-job throughput of independent replicas (no data-path
+    collective): every rank's work summed, over the slowest rank's time (max
+    over ranks), reduced through the process group (NCCL on the GPUs, gloo in
+    the CPU tests). Returns (value, seconds, work)."""
+    if world_size > 1:
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+        w = torch.tensor([float(work)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(w, op=dist.ReduceOp.SUM)
+        seconds, work = float(t.item()), float(w.item())
+    return work / seconds, seconds, work
+
+
 def workload(args, rank):
     """(assembly or list of assemblies for the arena, config, name, smallest diameter)."""
     from tangle_b200.generate import batched_specimens, cpu_runnable_specimen, mid_size_specimen
@@ -563,17 +580,9 @@ def run_cuda(args):
     refreshes = contact_info["refreshes"] - refreshes0
     elapsed_ms = start.elapsed_time(end)
     barrier()
-    local_t = torch.tensor([elapsed_ms, float(nodes * iterations_done)], dtype=torch.float64, device="cuda")
-    if world_size > 1:
-        t_max = local_t[:1].clone()
-        torch.distributed.all_reduce(t_max, op=torch.distributed.ReduceOp.MAX)
-        work = local_t[1:].clone()
-        torch.distributed.all_reduce(work, op=torch.distributed.ReduceOp.SUM)
-        elapsed_ms = float(t_max.item())
-        total_work = float(work.item())
-    else:
-        total_work = float(local_t[1].item())
-    value = total_work / (elapsed_ms / 1000.0)
+    value, elapsed_s, total_work = replica_throughput(elapsed_ms / 1000.0, float(nodes * iterations_done),
+                                                     world_size)
+    elapsed_ms = elapsed_s * 1000.0
     clock_summary = clocks.summary()
 
     # Roofline of the contact pass: the passes' algorithmic bytes (listed and
@@ -607,17 +616,8 @@ def run_cuda(args):
             st = world.run_batch(fixed, args.iterations)
             world.download_positions(host_np)
             done += st.batch_iterations
-        e2e_s = time.perf_counter() - t0
-        e2e_t = torch.tensor([e2e_s, float(nodes * done)], dtype=torch.float64, device="cuda")
-        if world_size > 1:
-            tm = e2e_t[:1].clone()
-            torch.distributed.all_reduce(tm, op=torch.distributed.ReduceOp.MAX)
-            wk = e2e_t[1:].clone()
-            torch.distributed.all_reduce(wk, op=torch.distributed.ReduceOp.SUM)
-            e2e_s, e2e_work = float(tm.item()), float(wk.item())
-        else:
-            e2e_work = float(e2e_t[1].item())
-        e2e = {"value": e2e_work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 12 * nodes,
+        e2e_value, _, _ = replica_throughput(time.perf_counter() - t0, float(nodes * done), world_size)
+        e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 12 * nodes,
                "d2h_bytes_per_step": 12 * nodes + 64}
     world.close()
 
