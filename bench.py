@@ -14,9 +14,11 @@ Printed JSON line (rank 0):
 * e2e -- the same metric through the public API with host buffers: every
   step uploads positions from pinned host memory, runs the batch and
   downloads the positions;
-* roofline -- the contact pass (the dominant kernel): algorithmic bytes
-  sum_s (60 + 4 K_s) per launch over its CUDA-event duration inside the timed
-  region, against the measured HBM copy bandwidth;
+* roofline -- the fiber update (the largest kernel): algorithmic bytes per
+  launch (`update_bytes`) over its CUDA-event duration inside the timed
+  region, against the measured HBM copy bandwidth, with the DRAM traffic of
+  the committed ncu capture; roofline_contact -- the same for the contact
+  pass: sum_s (60 + 4 K_s) bytes per launch;
 * cpu_baseline -- the CPU oracle on the same specimen, all host threads,
   a bounded sample of iterations;
 * time_to_admissible -- seconds from the initial specimen to max overlap
@@ -26,7 +28,8 @@ Printed JSON line (rank 0):
 
 `--impl reference` times the reference algorithm's CPU restatement (the
 oracle; the reference is Rust and cannot be built here) on the same
-workload, rank 0 only.
+workload, rank 0 only. `--workload ply_stack` deposits the 20-ply stack ply
+by ply (its own JSON line: whole-job seconds, plain and warm-started).
 Multi-GPU: one independent replica specimen per rank (replicas only; the
 relaxation of one specimen runs on one GPU).
 """
@@ -238,6 +241,27 @@ def ncu_traffic(refresh_share: float, lists_on: bool):
         return None
 
 
+def update_bytes(nodes: int, segments: int, contact_lists: bool) -> float:
+    """Algorithmic bytes of one fiber-update launch: per vertex the position
+    read and written (16 + 16), its static record (16), pinned flag (4),
+    list snapshot (16) and step (4), plus the contact-list snapshot (16) when
+    contact lists are on; per segment its rest length (4), two correction
+    records (32) and two geometry records written (32)."""
+    return float(nodes) * (72.0 + (16.0 if contact_lists else 0.0)) + float(segments) * 68.0
+
+
+def update_traffic(nodes: int):
+    """Per-launch DRAM bytes of the fiber update from the committed ncu
+    summary, scaled to `nodes` (traffic grows with the nodes)."""
+    path = os.path.join(ROOT, "profiles", "update_traffic.json")
+    try:
+        with open(path) as fh:
+            data = json.load(fh)
+        return float(data["dram_bytes_per_launch"]) * nodes / float(data["nodes"])
+    except (OSError, KeyError, ValueError, ZeroDivisionError):
+        return None
+
+
 MILESTONES = (0.1, 0.05, 0.03, 0.02, 0.01, 0.001)  # max overlap / d
 
 
@@ -319,10 +343,11 @@ PLY_MILESTONES = (0.2, 0.1, 0.05)
 def ply_stack_deposition(assembly, packed, config, d_min, plies, budget, net):
     """The 20-ply formation sequence on one resident world: for each ply,
     activate its formation step (the ply was generated in place, one ply
-    thickness above the previous), optionally apply the learned warm start,
-    and relax until the gate holds or `budget` iterations. Returns the whole
-    job's wall time (host-driven, inputs resident), per-ply records and the
-    node-iterations done."""
+    thickness above the previous), optionally apply the learned warm start to
+    the new ply's fibers, and relax until the gate holds or `budget`
+    iterations. Returns the whole job's wall time (host-driven, inputs
+    resident), per-ply records and the node-iterations done."""
+    import numpy as np
     import torch
 
     from tangle_b200.device import DeviceWorld
@@ -339,7 +364,8 @@ def ply_stack_deposition(assembly, packed, config, d_min, plies, budget, net):
         if net is not None:
             from tangle_b200.warmstart import warm_start
 
-            accepted = warm_start(world, net, config).accepted
+            new_ply = np.nonzero(np.asarray(packed.fiber_formation_steps) == k)[0]
+            accepted = warm_start(world, net, config, fibers=new_ply).accepted
         start = None
         status = None
         reached = {}
@@ -387,7 +413,13 @@ def run_ply_stack(args):
                                   max_list_bytes=8 << 30, iterations_per_batch=64, max_iterations=1 << 30)
     config = settings.to_config(d_min)
     runs = {}
-    net = load_warmstart_net()
+    ply_net = os.path.join(ROOT, "tangle_b200", "warmstart_ply_net.npz")
+    if os.path.exists(ply_net):
+        from tangle_b200.warmstart import WarmStartNet
+
+        net = WarmStartNet.load(ply_net)
+    else:
+        net = load_warmstart_net()
     for label, use_net in (("plain", None), ("warm_start", net)):
         if label == "warm_start" and net is None:
             continue
@@ -550,6 +582,7 @@ def run_cuda(args):
     contact_ms = 0.0
     contact_passes = 0
     update_ms = 0.0
+    updates = 0
     rebuild_ms = 0.0
     iterations_done = 0
     rebuilds0 = world.neighbor_list_rebuilds()
@@ -567,6 +600,7 @@ def run_cuda(args):
             contact_ms += kt["contact_ms"]
             contact_passes += kt["contact_passes"]
             update_ms += kt["update_ms"]
+            updates += kt["updates"]
             rebuild_ms += kt["rebuild_ms"]
         with torch.cuda.stream(stream):
             end.record(stream)
@@ -595,12 +629,24 @@ def run_cuda(args):
     algorithmic = refresh_share * refresh_bytes + (1.0 - refresh_share) * listed_bytes
     peak, peak_kind = measured_peak()
     achieved = algorithmic / avg_contact_s / 1.0e9 if avg_contact_s > 0 else 0.0
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": ncu_traffic(refresh_share, contact_info["block"] > 0), "peak_source": f"{peak_kind} hbm_gbs",
-                "kernel": "contact_kernel (find_segment_corrections)",
-                "algorithmic_bytes_per_launch": algorithmic, "avg_launch_ms": avg_contact_s * 1000.0,
-                "contact_passes": contact_passes, "refresh_passes": refreshes,
-                "contact_skin_m": contact_info["skin"]}
+    roofline_contact = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": ncu_traffic(refresh_share, contact_info["block"] > 0),
+                        "peak_source": f"{peak_kind} hbm_gbs", "kernel": "contact_kernel (find_segment_corrections)",
+                        "algorithmic_bytes_per_launch": algorithmic, "avg_launch_ms": avg_contact_s * 1000.0,
+                        "contact_passes": contact_passes, "refresh_passes": refreshes,
+                        "contact_skin_m": contact_info["skin"]}
+    # Roofline of the fiber update, the largest kernel (42 % of the launch
+    # time): its algorithmic bytes per launch over its mean duration.
+    segments = world.segment_count
+    avg_update_s = (update_ms / max(updates, 1)) / 1000.0
+    update_algorithmic = update_bytes(nodes, segments, contact_info["block"] > 0)
+    update_achieved = update_algorithmic / avg_update_s / 1.0e9 if avg_update_s > 0 else 0.0
+    roofline = {"bound": "hbm", "achieved": update_achieved, "peak": peak, "unit": "GB/s",
+                "frac": update_achieved / peak, "traffic": update_traffic(nodes),
+                "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel": "fiber_lanes_kernel (internal, contact and curvature corrections)",
+                "algorithmic_bytes_per_launch": update_algorithmic, "avg_launch_ms": avg_update_s * 1000.0,
+                "launches": updates}
 
     # End to end through the public API with pinned host buffers: the timed
     # steps again, from the same start state, each step uploading the
@@ -654,6 +700,7 @@ def run_cuda(args):
             "neighbor_list_rebuilds": int(rebuilds),
             "kernel_ms": {"contact": contact_ms, "update": update_ms, "rebuild_and_gated": rebuild_ms},
             "roofline": roofline,
+            "roofline_contact": roofline_contact,
             "clocks": clock_summary,
             "e2e": e2e,
             "time_to_admissible": tta,

@@ -493,12 +493,13 @@ class WarmStartReport:
 
 
 def warm_start(world: DeviceWorld, net: WarmStartNet, config: RelaxationConfig, scale: float = 1.0,
-               max_step_diameters: float = 2.0) -> WarmStartReport:
+               max_step_diameters: float = 2.0, fibers=None) -> WarmStartReport:
     """Applies the network's proposal to the world's positions; reverts it
     unless it lowers the overlap residual (the sum over segments of their
     deepest penetration / d). Curvature is left to the plain iterations that
     always follow: their gate includes it, and the proposal's small kinks are
-    removed within their first sweeps."""
+    removed within their first sweeps. With `fibers` (indices), only those
+    fibers' vertices move (a newly deposited ply on a relaxed stack)."""
     import torch
 
     t0 = time.perf_counter()
@@ -506,6 +507,12 @@ def warm_start(world: DeviceWorld, net: WarmStartNet, config: RelaxationConfig, 
     saved = world.download_positions()
     graph = ContactGraph.from_world(world, graph_cutoff(world))
     y = net.forward(graph)
+    if fibers is not None:
+        spans = np.asarray(world.packed().fiber_vertex_spans, dtype=np.int64).reshape(-1, 2)
+        keep = np.zeros(world.vertex_count, dtype=np.float32)
+        for f in np.asarray(fibers, dtype=np.int64):
+            keep[spans[f, 0]: spans[f, 0] + spans[f, 1]] = 1.0
+        y = y * torch.from_numpy(keep).to(y.device)[:, None]
     d_max = float(graph.diameters().max().item()) if graph.V else 0.0
     _check(_lib().tgl_world_displace(world._handle, _p(y), OUTPUT, ctypes.c_float(scale), 1,
                                      ctypes.c_float(max_step_diameters * d_max)))
@@ -529,6 +536,14 @@ def training_specimen(index: int, seed_base: int = 1000):
     return mid_size_specimen(scale=(2000.0 / 20000.0) ** (1.0 / 3.0), seed=seed_base + index)
 
 
+def ply_training_specimen(index: int, seed_base: int = 1000):
+    """Two plies of the 20-ply stack's kind on a 1 mm square: the first is
+    relaxed before the second is activated on top of it."""
+    from .generate import ply_stack_specimen
+
+    return ply_stack_specimen(plies=2, side=1.0e-3, seed=seed_base + index)
+
+
 def relaxation_config(assembly, neighbor_capacity: int = 256) -> RelaxationConfig:
     from .settings import RelaxationSettings
 
@@ -537,16 +552,23 @@ def relaxation_config(assembly, neighbor_capacity: int = 256) -> RelaxationConfi
                               max_list_bytes=8 << 30).to_config(d)
 
 
-def generate_samples(count: int, iterations: int = 64, seed_base: int = 1000, progress=None) -> List[Sample]:
+def generate_samples(count: int, iterations: int = 64, seed_base: int = 1000, progress=None,
+                     geometry: str = "mid_size") -> List[Sample]:
     """Training samples from the plain relaxer's own trajectories: each
-    specimen's graph at its start and its displacement after `iterations`."""
+    specimen's graph at its start and its displacement after `iterations`.
+    With geometry "ply": the first ply relaxed 256 iterations alone, then
+    the second activated, and the sample taken from there."""
     from .assembly import PackedAssembly
 
     samples = []
     for i in range(count):
-        assembly = training_specimen(i, seed_base)
+        assembly = (ply_training_specimen if geometry == "ply" else training_specimen)(i, seed_base)
         config = relaxation_config(assembly)
         world = DeviceWorld(PackedAssembly.from_assembly(assembly), config.cell_list, config.max_step)
+        if geometry == "ply":
+            world.activate_formation_step(0)
+            world.run_batch(RelaxationConfig(**{**config.__dict__, "force_full_iterations": True}), 256)
+            world.activate_formation_step(1)
         samples.append(make_sample(world, config, iterations))
         world.close()
         if progress:
@@ -632,6 +654,8 @@ def _main(argv=None) -> int:
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--gain-specimens", type=int, default=8)
     ap.add_argument("--load", default=None, help="evaluate a saved network on held-out specimens; no training")
+    ap.add_argument("--geometry", choices=["mid_size", "ply"], default="mid_size",
+                    help="training specimens: mid-size-like cubes, or a ply deposited on a relaxed ply")
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
     if args.load:
@@ -641,7 +665,7 @@ def _main(argv=None) -> int:
     if not args.out:
         ap.error("--out is required when training")
     t0 = time.perf_counter()
-    samples = generate_samples(args.specimens + args.held_out, args.iterations)
+    samples = generate_samples(args.specimens + args.held_out, args.iterations, geometry=args.geometry)
     train_set, test_set = samples[: args.specimens], samples[args.specimens:]
     t1 = time.perf_counter()
     net = WarmStartNet(seed=args.seed)
@@ -651,7 +675,8 @@ def _main(argv=None) -> int:
     t2 = time.perf_counter()
     after = evaluate(net, test_set)
     net.save(args.out)
-    gain = measure_gain(net, args.gain_specimens, args.iterations) if args.gain_specimens else None
+    gain = (measure_gain(net, args.gain_specimens, args.iterations)
+            if args.gain_specimens and args.geometry == "mid_size" else None)
     print(json.dumps({"specimens": args.specimens, "held_out": args.held_out, "iterations": args.iterations,
                       "epochs": args.epochs, "parameters": net.parameter_count, "data_seconds": t1 - t0,
                       "train_seconds": t2 - t1, "held_out_before": before, "held_out_after": after,
