@@ -1241,16 +1241,6 @@ int formation_world(tgl_world *w) {
     return 0;
 }
 
-// Grows a device buffer to hold `count` elements (the old one stays in the
-// world's allocation list until the world is destroyed).
-template <typename T>
-int reserve(tgl_world *w, T **buffer, uint32_t &capacity, uint32_t count) {
-    if (*buffer && capacity >= count) return 0;
-    if (int rc = w->alloc(buffer, std::max<size_t>(count, 1))) return rc;
-    capacity = count;
-    return 0;
-}
-
 // The fiber of vertex v (binary search over the fiber spans).
 uint32_t fiber_of_vertex(const tgl_world *w, uint32_t v) {
     size_t lo = 0, hi = w->h_vspan.size();
@@ -1325,9 +1315,11 @@ int tgl_world_set_layer_targets(tgl_world *w, const tgl_layer_targets *t) {
     if (!(t->stiffness > 0.0f && t->stiffness <= 1.0f)) return set_error(TGL_ERR_INVALID, "stiffness must be in (0, 1]");
     if (!(t->max_translation > 0.0f)) return set_error(TGL_ERR_INVALID, "max_translation must be positive");
     if (t->first_layer > t->last_layer) return set_error(TGL_ERR_INVALID, "first_layer exceeds last_layer");
-    uint32_t fiber_capacity = w->fiber_layer_d ? d.F : 0;
-    if (int rc = reserve(w, &w->fiber_layer_d, fiber_capacity, d.F)) return rc;
-    if (int rc = reserve(w, &w->layer_target_d, w->layer_capacity, t->count)) return rc;
+    if (!w->fiber_layer_d && w->alloc(&w->fiber_layer_d, d.F)) return TGL_ERR_MEMORY;
+    if (t->count > w->layer_capacity) {
+        if (w->alloc(&w->layer_target_d, t->count)) return TGL_ERR_MEMORY;
+        w->layer_capacity = t->count;
+    }
     TGL_CUDA(cudaMemcpyAsync(w->fiber_layer_d, t->fiber_layers, d.F * sizeof(uint32_t), cudaMemcpyHostToDevice,
                              w->stream));
     TGL_CUDA(cudaMemcpyAsync(w->layer_target_d, t->targets, t->count * sizeof(float), cudaMemcpyHostToDevice,
@@ -1378,17 +1370,13 @@ int tgl_world_set_vertex_targets(tgl_world *w, const tgl_vertex_targets *t) {
         map[v] = (int32_t)k;
         fibers[k] = fiber_of_vertex(w, v);
     }
-    uint32_t vertex_capacity = w->vertex_target_d ? d.V : 0;
-    if (int rc = reserve(w, &w->vertex_target_d, vertex_capacity, d.V)) return rc;
-    uint32_t cap = w->target_capacity;
-    if (int rc = reserve(w, &w->target_vertices_d, cap, t->count)) return rc;
-    cap = w->target_capacity;
-    if (int rc = reserve(w, &w->target_fibers_d, cap, t->count)) return rc;
-    cap = w->target_capacity;
-    if (int rc = reserve(w, &w->target_coord_d, cap, t->count)) return rc;
-    cap = w->target_capacity;
-    if (int rc = reserve(w, &w->command_coord_d, cap, t->count)) return rc;
-    w->target_capacity = std::max(w->target_capacity, t->count);
+    if (!w->vertex_target_d && w->alloc(&w->vertex_target_d, d.V)) return TGL_ERR_MEMORY;
+    if (t->count > w->target_capacity) {  // the four per-target buffers grow together
+        if (w->alloc(&w->target_vertices_d, t->count) || w->alloc(&w->target_fibers_d, t->count) ||
+            w->alloc(&w->target_coord_d, t->count) || w->alloc(&w->command_coord_d, t->count))
+            return TGL_ERR_MEMORY;
+        w->target_capacity = t->count;
+    }
     TGL_CUDA(cudaMemcpyAsync(w->vertex_target_d, map.data(), d.V * sizeof(int32_t), cudaMemcpyHostToDevice, w->stream));
     TGL_CUDA(cudaMemcpyAsync(w->target_vertices_d, t->vertices, t->count * sizeof(uint32_t), cudaMemcpyHostToDevice,
                              w->stream));
