@@ -17,8 +17,10 @@ formation operations of crates/tangle_generate/src/recipe.rs:859-1600:
   force full batches;
 * layer operations hold layer targets on the stack axis (`scale_layer_spacing`,
   `place_layer_above`) until `release_layer_placement` or the end of the
-  recipe; `fit_cell_to_active_fibers` moves the walls onto the active
-  fibers; `set_min_bend_radius` changes a material's curvature limit;
+  recipe; `needle_layer` pulls chosen fibers of a layer through the stack
+  with vertex displacement targets until `release_needles`;
+  `fit_cell_to_active_fibers` moves the walls onto the active fibers;
+  `set_min_bend_radius` changes a material's curvature limit;
 * a step that exhausts its budget raises `RecipeError`.
 """
 
@@ -36,6 +38,8 @@ from .checkpoint import CheckpointReport, CheckpointSettings
 from .device import DeviceWorld
 from .formation import CompactionKinematics
 from .generate import FiberPopulation, generate_fiber_population, layer_centers
+from .needling import (CircularFootprint, NeedlingConfig, RandomFiberFraction, random_footprint_center,
+                       selected_needling_vertices)
 from .settings import BatchStatus, RelaxationSettings
 
 DEFAULT_STACK_AXIS = 2
@@ -130,6 +134,16 @@ class _ReleaseLayerPlacement:
 class _FitCell:
     axes: List[bool]
     padding: float
+
+
+@dataclass
+class _NeedleLayer:
+    config: NeedlingConfig
+
+
+@dataclass
+class _ReleaseNeedles:
+    pass
 
 
 class RunResult:
@@ -326,6 +340,38 @@ class Recipe:
 
     def release_layer_placement(self) -> None:
         self._push(_ReleaseLayerPlacement(), "release layer placement")
+
+    def needle_layer(self, layer: int, *, footprint, depth: float, min_fiber_diameter: Optional[float] = None,
+                     stiffness: float = 0.25, max_translation: float = 1.0e-5,
+                     max_translation_over_diameter: float = 0.25) -> HeldTargets:
+        """recipe.rs:455-503 (NeedleLayer): fibers of `layer` chosen by the
+        footprint are each pulled at one internal vertex `depth` toward the
+        negative stack axis, held until `release_needles`."""
+        depth = _positive(depth, "depth")
+        if min_fiber_diameter is not None:
+            min_fiber_diameter = _positive(min_fiber_diameter, "min_fiber_diameter")
+        stiffness = _unit_fraction(stiffness, "stiffness")
+        max_translation = _positive(max_translation, "max_translation")
+        ratio = _positive(max_translation_over_diameter, "max_translation_over_diameter")
+        layer = int(layer)
+        if isinstance(footprint, RandomFiberFraction):
+            how = f"a random {footprint.fraction} of its fibers"
+        elif isinstance(footprint, CircularFootprint):
+            if footprint.center is None:  # recipe.rs:761-776: a reproducible centre per layer
+                plane = [a for a in range(3) if a != self._stack_axis]
+                cell = self._assembly.cell
+                center = random_footprint_center(footprint.seed, layer, [cell.origin[a] for a in plane],
+                                                 [cell.lengths[a] for a in plane])
+                footprint = CircularFootprint(center, diameter=footprint.diameter)
+            how = f"a {footprint.diameter:.3e} circle at [{footprint.center[0]:.3e}, {footprint.center[1]:.3e}]"
+        else:
+            raise TypeError("footprint must be a CircularFootprint or RandomFiberFraction")
+        config = NeedlingConfig(layer, footprint, depth, stiffness, max_translation, ratio, min_fiber_diameter)
+        self._push(_NeedleLayer(config), f"needle layer {layer} through {how}")
+        return HeldTargets(self, self.release_needles)
+
+    def release_needles(self) -> None:
+        self._push(_ReleaseNeedles(), "release needles")
 
     def fit_cell_to_active_fibers(self, *, axes: Optional[Sequence[bool]] = None, padding: float = 0.0) -> None:
         """recipe.rs:515-545 (FitCellToActiveFibers): the walls of the chosen
@@ -527,6 +573,32 @@ class Recipe:
                     status.converged = False
                 elif isinstance(op, _ReleaseLayerPlacement):
                     world.clear_layer_targets()
+                    status.converged = False
+                elif isinstance(op, _NeedleLayer):
+                    # recipe.rs:1086-1180.
+                    cfg = op.config
+                    active = np.asarray(world.fiber_active, dtype=bool)
+                    steps = np.asarray(packed.fiber_formation_steps)
+                    active_step = int(steps[active].max()) if np.any(active) else None
+                    if active_step is None or active_step < cfg.layer:
+                        raise RecipeError(index, descriptions[index], status.total_iterations,
+                                          f"cannot needle layer {cfg.layer}: it has not been inserted yet")
+                    positions = world.download_positions()
+                    downloaded += positions.nbytes
+                    vertices = selected_needling_vertices(assembly, packed, positions, active, active_step, axis, cfg)
+                    world.clear_vertex_targets()
+                    if vertices:
+                        spans = np.asarray(packed.fiber_vertex_spans).reshape(-1, 2)
+                        fibers = np.searchsorted(spans[:, 0], np.asarray(vertices), side="right") - 1
+                        smallest = min(2.0 * assembly.fibers[int(f)].radius for f in fibers)
+                        limit = np.float32(smallest) * np.float32(cfg.max_translation_over_diameter)
+                        world.apply_vertex_displacement_targets(axis, vertices, -cfg.depth, cfg.stiffness,
+                                                                float(min(np.float32(cfg.max_translation), limit)))
+                    events_detail = f" ({len(vertices)} vertices)"
+                    descriptions[index] = descriptions[index] + events_detail
+                    status.converged = False
+                elif isinstance(op, _ReleaseNeedles):
+                    world.clear_vertex_targets()
                     status.converged = False
                 elif isinstance(op, _FitCell):
                     # recipe.rs:1205-1255: walls onto the active capsules.
