@@ -344,6 +344,16 @@ __device__ inline bool build_pair(const WorldDev &w, const Grid &grid, float ski
     return other != segment && !near_along_fiber;
 }
 
+// Order-preserving int key of an f32, for shared-memory atomic min / max.
+__device__ inline int float_key(float x) {
+    const int b = __float_as_int(x);
+    return b >= 0 ? b : b ^ 0x7fffffff;
+}
+__device__ inline float key_float(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff); }
+
+// Distance along one axis from 0 to the interval [lo, hi].
+__device__ inline float interval_gap(float lo, float hi) { return fmaxf(0.0f, fmaxf(lo, -hi)); }
+
 // build_segment_neighbor_lists (neighbor.rs:155-364). One block per home cell.
 // The 27 stencil cells' bounding spheres are staged in shared memory; each
 // warp takes one home segment and tests 32 candidates at a time with a
@@ -356,12 +366,28 @@ __device__ inline bool build_pair(const WorldDev &w, const Grid &grid, float ski
 // unwrapped, so a segment's cell says nothing about its image.) Survivors
 // queue up and get the exact test 32 at a time; hits append in scan order
 // and are sorted later.
+//
+// Stencil-cell culling (with the sphere test on). While staging, the block
+// bounds each stencil cell's staged spheres, radii scaled by 1.0003, by a box
+// in that cell's own frame: centre minus the cell's lower corner, wrapped
+// into the nearest image on periodic axes, so the frame is right whichever
+// image the unwrapped coordinates sit in. A home warp then skips every cell
+// whose box is farther from its own sphere centre (in the home cell's frame,
+// shifted by the stencil offset, nearest of the three images on periodic
+// axes) than (home radius + skin) * 1.0002 + the sphere test's margin + a
+// rounding margin. The distance to a box of balls is at most the distance to
+// any of the balls, so no candidate of a skipped cell can pass the sphere
+// test: the lists are the same, the scan is shorter. A non-finite sphere
+// makes its cell's box unbounded (never skipped).
 template <bool A>
 __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int prefilter_world, float sphere_eps_world) {
     if (w.ctl->neighbor_state[0] == 0) return;
     extern __shared__ float4 build_smem[];
     uint32_t *slot_of = reinterpret_cast<uint32_t *>(build_smem + ch);
     __shared__ uint32_t st_count[27], st_off[27], st_prefix[28];
+    __shared__ float st_face[27][3];      // lower corner of each stencil cell
+    __shared__ int box_lo[27][3], box_hi[27][3];  // float_key of the staged spheres' box, cell frame
+    __shared__ uint32_t box_mag[27];      // largest |x| + |y| + |z| of a staged centre (f32 bits)
     __shared__ uint32_t queue[8][64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int warps = blockDim.x >> 5;
@@ -380,7 +406,12 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
         uint32_t hoff = w.cell_offsets[h];
         if (threadIdx.x < 27) {
             uint32_t cell = stencil_cell(h - cell_base, threadIdx.x, g);
-            if (cell != TGL_NONE) cell += cell_base;
+            if (cell != TGL_NONE) {
+                st_face[threadIdx.x][0] = g.lower[0] + (float)(cell % g.cells[0]) * g.width[0];
+                st_face[threadIdx.x][1] = g.lower[1] + (float)((cell / g.cells[0]) % g.cells[1]) * g.width[1];
+                st_face[threadIdx.x][2] = g.lower[2] + (float)(cell / (g.cells[0] * g.cells[1])) * g.width[2];
+                cell += cell_base;
+            }
             st_count[threadIdx.x] = cell == TGL_NONE ? 0u : w.cell_counts[cell];
             st_off[threadIdx.x] = cell == TGL_NONE ? 0u : w.cell_offsets[cell];
         }
@@ -395,15 +426,47 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
         }
         __syncthreads();
         const uint32_t total = st_prefix[27];
+        // Rounding margin of the culling test: coordinates, corners and box
+        // lengths are all within f32 rounding of their true values.
+        float grid_scale = 0.0f, wmax = 0.0f;
+        for (int a = 0; a < 3; ++a) {
+            grid_scale += fabsf(g.lower[a]) + 2.0f * g.length[a];
+            wmax = fmaxf(wmax, g.width[a]);
+        }
         for (uint32_t base = 0; base < total; base += (uint32_t)ch) {
             uint32_t len = min((uint32_t)ch, total - base);
+            if (prefilter && threadIdx.x < 27) {
+                for (int a = 0; a < 3; ++a) {
+                    box_lo[threadIdx.x][a] = float_key(INFINITY);
+                    box_hi[threadIdx.x][a] = float_key(-INFINITY);
+                }
+                box_mag[threadIdx.x] = 0u;
+            }
+            __syncthreads();
             for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
                 uint32_t flat = base + i;
                 int k = 0;
                 while (k < 26 && st_prefix[k + 1] <= flat) ++k;
                 uint32_t slot = st_off[k] + (flat - st_prefix[k]);
                 slot_of[i] = slot;
-                build_smem[i] = w.slot_sphere[slot];
+                const float4 sp = w.slot_sphere[slot];
+                build_smem[i] = sp;
+                if (prefilter) {
+                    const float r = sp.w * 1.0003f;
+                    const float c[3] = {sp.x, sp.y, sp.z};
+                    for (int a = 0; a < 3; ++a) {
+                        float p = c[a] - st_face[k][a];
+                        if (g.periodic[a]) p -= rintf(p * g.inv_length[a]) * g.length[a];
+                        float lo = p - r, hi = p + r;
+                        if (!(isfinite(lo) && isfinite(hi))) {
+                            lo = -INFINITY;
+                            hi = INFINITY;
+                        }
+                        atomicMin(&box_lo[k][a], float_key(lo));
+                        atomicMax(&box_hi[k][a], float_key(hi));
+                    }
+                    atomicMax(&box_mag[k], __float_as_uint(fabsf(sp.x) + fabsf(sp.y) + fabsf(sp.z)));
+                }
             }
             __syncthreads();
             for (uint32_t hi = warp; hi < nh; hi += warps) {
@@ -418,15 +481,53 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
                 const float4 own = w.seg_static[segment];
                 uint32_t count = base == 0 ? 0u : w.nbr_count[segment];
                 uint32_t *list = w.nbr_list + (size_t)segment * block;
+                // Lane k < 27 decides whether stencil cell k is scanned.
+                bool scan = false;
+                if (lane < 27) {
+                    scan = max(st_prefix[lane], base) < min(st_prefix[lane + 1], base + len);
+                    if (scan && prefilter) {
+                        const float hc[3] = {hs.x, hs.y, hs.z};
+                        const int off[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
+                        float far2 = 0.0f;
+                        for (int ax = 0; ax < 3; ++ax) {
+                            float qh = hc[ax] - st_face[13][ax];
+                            if (g.periodic[ax]) qh -= rintf(qh * g.inv_length[ax]) * g.length[ax];
+                            const float shift = (float)off[ax] * g.width[ax] - qh;
+                            const float lo = key_float(box_lo[lane][ax]) + shift;
+                            const float hi_edge = key_float(box_hi[lane][ax]) + shift;
+                            float gap = interval_gap(lo, hi_edge);
+                            if (g.periodic[ax]) {
+                                gap = g.cells[ax] < 3 ? 0.0f
+                                                      : fminf(gap, fminf(interval_gap(lo + g.length[ax], hi_edge + g.length[ax]),
+                                                                         interval_gap(lo - g.length[ax], hi_edge - g.length[ax])));
+                            }
+                            far2 += gap * gap;
+                        }
+                        const float margin =
+                            1.0e-3f * wmax +
+                            8.0e-6f * (__uint_as_float(box_mag[lane]) + fabsf(hs.x) + fabsf(hs.y) + fabsf(hs.z) + grid_scale);
+                        const float reach = (hs.w + skin) * 1.0002f + sphere_eps + margin;
+                        scan = !(far2 > reach * reach);
+                    }
+                }
+                uint32_t cells_left = __ballot_sync(FULL, scan);
                 uint32_t queued = 0;
-                for (uint32_t c0 = 0; c0 < len || queued; c0 += 32) {
-                    if (c0 < len) {
-                        uint32_t c = c0 + lane;
+                uint32_t c = 0, c_end = 0;  // the current cell's staged range
+                for (;;) {
+                    if (c >= c_end && cells_left) {
+                        const int k = __ffs(cells_left) - 1;
+                        cells_left &= cells_left - 1u;
+                        c = max(st_prefix[k], base) - base;
+                        c_end = min(st_prefix[k + 1], base + len) - base;
+                    }
+                    const bool more = c < c_end;
+                    if (more) {
+                        const uint32_t cc = c + lane;
                         bool pass = false;
-                        if (c < len) {
+                        if (cc < c_end) {
                             pass = true;
                             if (prefilter) {
-                                float4 sp = build_smem[c];
+                                float4 sp = build_smem[cc];
                                 float dx = sp.x - hs.x, dy = sp.y - hs.y, dz = sp.z - hs.z;
                                 if (g.periodic[0]) dx -= rintf(dx * g.inv_length[0]) * g.length[0];
                                 if (g.periodic[1]) dy -= rintf(dy * g.inv_length[1]) * g.length[1];
@@ -436,12 +537,13 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
                             }
                         }
                         uint32_t ballot = __ballot_sync(FULL, pass);
-                        if (pass) q[queued + __popc(ballot & ((1u << lane) - 1u))] = c;
+                        if (pass) q[queued + __popc(ballot & ((1u << lane) - 1u))] = cc;
                         queued += __popc(ballot);
+                        c += 32;
                         __syncwarp();
                     }
                     // Exact tests, 32 at a time, or the remainder at the end.
-                    if (queued >= 32 || (c0 + 32 >= len && queued)) {
+                    if (queued >= 32 || (!more && queued)) {
                         uint32_t n = min(queued, 32u);
                         bool hit = false;
                         uint32_t other = 0;
@@ -459,6 +561,8 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
                         if ((uint32_t)lane < rest) q[lane] = moved_entry;
                         __syncwarp();
                         queued = rest;
+                    } else if (!more) {
+                        break;
                     }
                 }
                 if (lane == 0) w.nbr_count[segment] = count;
@@ -683,6 +787,7 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     __shared__ uint32_t segments[CONTACT_WARPS][32];
     __shared__ const uint32_t *sources[CONTACT_WARPS][32];
     __shared__ uint32_t kept_count[CONTACT_WARPS][32];
+    __shared__ uint32_t hit_mask[CONTACT_WARPS][32];   // queue lanes holding each owner's hits; zero between rounds
     __shared__ uint32_t lane_spec[A ? CONTACT_WARPS : 1][32];
     __shared__ uint32_t warp_max[CONTACT_WARPS];
     __shared__ int is_last;
@@ -700,6 +805,8 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     uint32_t *seg_of = segments[warp];
     const uint32_t **src = sources[warp];
     uint32_t *kept = kept_count[warp];
+    uint32_t *hm = hit_mask[warp];
+    hm[lane] = 0u;
     uint32_t thread_max = 0;
     const uint32_t warps_total = gridDim.x * CONTACT_WARPS;
     const uint64_t geom_policy = make_keep_policy();
@@ -844,18 +951,28 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
                     if (keep && lane == 31 - __clz(peers)) kept[h] += __popc(peers);
                     __syncwarp();
                 }
-                uint32_t bits = __ballot_sync(FULL, hit);
-                while (bits) {
-                    const int j = __ffs(bits) - 1;
-                    bits &= bits - 1u;
-                    const int owner = __shfl_sync(FULL, h, j);
-                    const float pen = __shfl_sync(FULL, pt.pen, j);
-                    const float t0x = __shfl_sync(FULL, pt.t0x, j), t0y = __shfl_sync(FULL, pt.t0y, j),
-                                t0z = __shfl_sync(FULL, pt.t0z, j);
-                    const float t1x = __shfl_sync(FULL, pt.t1x, j), t1y = __shfl_sync(FULL, pt.t1y, j),
-                                t1z = __shfl_sync(FULL, pt.t1z, j);
-                    const float aggw = __shfl_sync(FULL, pt.aggw, j);
-                    if (lane == owner) add_hit(acc, sp.contact_aggregation, pen, t0x, t0y, t0z, t1x, t1y, t1z, aggw);
+                if (__any_sync(FULL, hit)) {
+                    // Each hit parks its terms in its own (already consumed)
+                    // queue slot and the lowest lane of each owner's hits
+                    // posts their mask; every owner then adds its own hits in
+                    // ascending queue order, the order of the list, so the
+                    // owners sum in parallel and bit for bit as one by one.
+                    const uint32_t peers = __match_any_sync(FULL, hit ? (uint32_t)h : 32u + (uint32_t)lane);
+                    if (hit) {
+                        qg[2 * lane] = make_float4(pt.pen, pt.t0x, pt.t0y, pt.t0z);
+                        qg[2 * lane + 1] = make_float4(pt.t1x, pt.t1y, pt.t1z, pt.aggw);
+                        if (lane == __ffs(peers) - 1) hm[h] = peers;
+                    }
+                    __syncwarp();
+                    uint32_t mine = hm[lane];
+                    if (mine) hm[lane] = 0u;
+                    while (mine) {
+                        const int j = __ffs(mine) - 1;
+                        mine &= mine - 1u;
+                        const float4 ta = qg[2 * j], tb = qg[2 * j + 1];
+                        add_hit(acc, sp.contact_aggregation, ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w);
+                    }
+                    __syncwarp();
                 }
                 const uint32_t rest = queued - n;
                 float4 ma = make_float4(0.0f, 0.0f, 0.0f, 0.0f), mb = ma;
