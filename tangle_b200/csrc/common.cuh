@@ -226,6 +226,8 @@ struct Control {
     uint32_t cell_overflow;
     // Contact lists: refresh pending, refreshes done.
     uint32_t contact_state[2];
+    // Rebuild pipelines a batch graph's conditional node has run.
+    uint32_t rebuild_bodies;
 };
 
 }  // namespace tgl

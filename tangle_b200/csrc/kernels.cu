@@ -1,7 +1,9 @@
 // kernels.cu -- sm_100a kernels of the plain relaxation path.
 //
 // One relaxation step is three launches, fused from the reference's ~13:
-//   [rebuild, gated on neighbor_state[0]]  cell list + Verlet lists
+//   [rebuild, gated on neighbor_state[0]]  cell list + Verlet lists (in a
+//                     batch graph, the body of a conditional node that runs
+//                     it only when a rebuild is pending)
 //   contact_kernel    find_segment_corrections (contact.rs:232-902); the
 //                     last block to finish reduces the gate metrics and runs
 //                     assess_reduced_metrics (kernels.rs:129-162)
@@ -2107,6 +2109,20 @@ int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
     else
         enqueue_rebuild<false>(w, lp, st);
     return 10;
+}
+
+// The condition reads exactly the flag the gated rebuild kernels test on
+// entry, at the same point of the step, so a skipped body is one whose
+// kernels would all have returned at once. (Every kernel keeps its test.)
+__global__ void rebuild_condition_kernel(WorldDev w, cudaGraphConditionalHandle rebuild) {
+    const bool pending = w.ctl->neighbor_state[0] != 0;
+    cudaGraphSetConditional(rebuild, pending ? 1u : 0u);
+    if (pending) w.ctl->rebuild_bodies += 1;
+}
+
+int launch_rebuild_condition(const WorldDev &w, cudaGraphConditionalHandle rebuild, cudaStream_t st) {
+    rebuild_condition_kernel<<<1, 1, 0, st>>>(w, rebuild);
+    return 1;
 }
 
 int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, bool gate, cudaStream_t st) {

@@ -224,6 +224,9 @@ int launch_request_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t
 // refresh pass, each of which returns at once unless the device-side refresh
 // flag picks it; otherwise the full-list pass.
 int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, bool gate, cudaStream_t st);
+// Sets a batch graph's rebuild condition for one step from the pending
+// rebuild flag, and counts the rebuild pipelines it lets run.
+int launch_rebuild_condition(const WorldDev &w, cudaGraphConditionalHandle rebuild, cudaStream_t st);
 int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st);
 int launch_positions_from_stage(const WorldDev &w, cudaStream_t st);
 int launch_positions_to_stage(const WorldDev &w, cudaStream_t st);

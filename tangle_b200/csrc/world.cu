@@ -105,6 +105,11 @@ struct WarmGraph {
 struct tgl_world {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // Batch graphs skip gated-off steps with conditional nodes (driver and
+    // runtime 12.8 or later), their bodies captured on body_stream.
+    cudaStream_t body_stream = nullptr;
+    bool conditional = false;
+    uint32_t rebuild_bodies_seen = 0;
     WorldDev dev{};
     LaunchPlan lp{};
     float cell_size = 0.0f;
@@ -147,6 +152,7 @@ struct tgl_world {
         for (void *p : allocations) cudaFree(p);
         if (host_ctl) cudaFreeHost(host_ctl);
         if (stream) cudaStreamDestroy(stream);
+        if (body_stream) cudaStreamDestroy(body_stream);
     }
 
     template <typename T>
@@ -214,10 +220,68 @@ int validate_config(const tgl_relax_config &c) {
     return 0;
 }
 
+// The graph a stream is capturing into.
+static cudaError_t capture_graph(cudaStream_t st, cudaGraph_t *graph) {
+    cudaStreamCaptureStatus status;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, graph, nullptr, nullptr);
+    if (e != cudaSuccess) return e;
+    return status == cudaStreamCaptureStatusActive ? cudaSuccess : cudaErrorStreamCaptureInvalidated;
+}
+
+// Appends an IF node on `handle` (with an ELSE body when `size` is 2) after
+// the capture's current dependencies and makes it the capture's only
+// dependency; its bodies come back in `bodies`.
+static cudaError_t append_if(cudaStream_t st, cudaGraphConditionalHandle handle, unsigned size, cudaGraph_t *bodies) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams params{};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeIf;
+    params.conditional.size = size;
+    cudaGraphNode_t node;
+    if ((e = cudaGraphAddNode(&node, graph, deps, ndeps, &params)) != cudaSuccess) return e;
+    for (unsigned i = 0; i < size; ++i) bodies[i] = params.conditional.phGraph_out[i];
+    return cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+// Captures `enqueue(stream)` into a conditional body.
+template <typename F>
+static cudaError_t capture_body(tgl_world *w, cudaGraph_t body, F enqueue) {
+    cudaError_t e = cudaStreamBeginCaptureToGraph(w->body_stream, body, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    enqueue(w->body_stream);
+    cudaGraph_t out = nullptr;
+    return cudaStreamEndCapture(w->body_stream, &out);
+}
+
+// One step's rebuild as a conditional node: a kernel sets the condition
+// from the pending-rebuild flag and an IF node runs the rebuild pipeline
+// only then, so the ten gated-off launches are not made at all (every
+// kernel keeps its own test). The contact pass stays two gated launches:
+// an IF/ELSE node between them measured slower than the launch it saves.
+static cudaError_t enqueue_conditional_rebuild(tgl_world *w, int *kernels) {
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = capture_graph(w->stream, &graph);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle rebuild = 0;
+    if ((e = cudaGraphConditionalHandleCreate(&rebuild, graph, 0, 0)) != cudaSuccess) return e;
+    *kernels += launch_rebuild_condition(w->dev, rebuild, w->stream);
+    cudaGraph_t body = nullptr;
+    if ((e = append_if(w->stream, rebuild, 1, &body)) != cudaSuccess) return e;
+    return capture_body(w, body, [&](cudaStream_t st) { launch_rebuild(w->dev, w->lp, st); });
+}
+
 // run_batch's launch sequence (world.rs:1020-1505): begin, displacement
 // check, then iterations + 1 steps of [rebuild if flagged, contact pass with
 // the gate, fiber update]; kernels after the gate return at once once it
-// has stopped the batch.
+// has stopped the batch. Returns the kernels launched every time the graph
+// runs, or -1 with the error set.
 int enqueue_batch(tgl_world *w, const StepParams &sp, uint32_t iterations, std::vector<cudaEvent_t> *events) {
     int kernels = 0;
     kernels += launch_begin_batch(w->dev, w->lp, w->stream);
@@ -225,7 +289,15 @@ int enqueue_batch(tgl_world *w, const StepParams &sp, uint32_t iterations, std::
     kernels += launch_measure_start(w->dev, w->lp, w->stream);
     for (uint32_t step = 0; step <= iterations; ++step) {
         if (events) cudaEventRecordWithFlags((*events)[4 * step], w->stream, cudaEventRecordExternal);
-        kernels += launch_rebuild(w->dev, w->lp, w->stream);
+        if (w->conditional) {
+            cudaError_t e = enqueue_conditional_rebuild(w, &kernels);
+            if (e != cudaSuccess) {
+                set_error(TGL_ERR_CUDA, std::string("conditional graph node: ") + cudaGetErrorString(e));
+                return -1;
+            }
+        } else {
+            kernels += launch_rebuild(w->dev, w->lp, w->stream);
+        }
         if (events) cudaEventRecordWithFlags((*events)[4 * step + 1], w->stream, cudaEventRecordExternal);
         kernels += launch_contact(w->dev, w->lp, sp, true, w->stream);
         if (events) cudaEventRecordWithFlags((*events)[4 * step + 2], w->stream, cudaEventRecordExternal);
@@ -527,8 +599,14 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
     cudaDeviceProp prop{};
     cudaGetDeviceProperties(&prop, w->device);
     if (prop.major < 10) return fail(set_error(TGL_ERR_NO_DEVICE, "the relaxation kernels are built for sm_100a"));
-    if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&w->body_stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(set_error(TGL_ERR_CUDA, "cudaStreamCreate failed"));
+    {
+        int driver = 0, runtime = 0;
+        w->conditional = cudaDriverGetVersion(&driver) == cudaSuccess && cudaRuntimeGetVersion(&runtime) == cudaSuccess &&
+                         driver >= 12080 && runtime >= 12080 && std::getenv("TGL_NO_CONDITIONAL_GRAPHS") == nullptr;
+    }
     if (cudaMallocHost(&w->host_ctl, (hosts.size() > 1 || arena ? hosts.size() + 1 : 1) * sizeof(Control)) != cudaSuccess)
         return fail(set_error(TGL_ERR_MEMORY, "cudaMallocHost failed"));
 
@@ -841,6 +919,10 @@ int tgl_run_batch(tgl_world *w, const tgl_relax_config *config, uint32_t iterati
         TGL_CUDA(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
         entry.kernels = enqueue_batch(w, sp, iterations, w->timing ? &entry.events : nullptr);
         cudaError_t e = cudaStreamEndCapture(w->stream, &entry.graph);
+        if (entry.kernels < 0) {  // the error is set
+            destroy_entry(entry);
+            return TGL_ERR_CUDA;
+        }
         if (e != cudaSuccess) return set_error(TGL_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e));
         e = cudaGraphInstantiate(&entry.exec, entry.graph, 0);
         if (e != cudaSuccess) {
@@ -858,6 +940,11 @@ int tgl_run_batch(tgl_world *w, const tgl_relax_config *config, uint32_t iterati
     TGL_CUDA(cudaGraphLaunch(it->second.exec, w->stream));
     w->launches += (uint64_t)it->second.kernels;
     if (int rc = read_status(w, *config, status)) return rc;
+    if (w->conditional) {  // rebuild pipelines the graph ran (10 kernels each)
+        const uint32_t bodies = w->host_ctl[0].rebuild_bodies;
+        w->launches += 10ull * (bodies >= w->rebuild_bodies_seen ? bodies - w->rebuild_bodies_seen : bodies);
+        w->rebuild_bodies_seen = bodies;
+    }
     TGL_CUDA(cudaGetLastError());
     w->last = &it->second;
     w->last_batch_iterations = status->batch_iterations;
