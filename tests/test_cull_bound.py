@@ -7,7 +7,8 @@ farther than its reach. This restates both tests in f32, operation for
 operation (numpy rounds every f32 operation and contracts nothing, as the
 kernel is compiled), on random grids: periodic and walled axes, unwrapped
 coordinates several box lengths out, centres outside the walls, centres
-within 1e-7 of a cell face and partners placed at the sphere test's limit.
+within 1e-7 of a cell face and partners placed at the sphere test's limit
+(half of them along an axis, where the box bound is tight).
 Every pair that passes the sphere test must lie in a cell the home scans.
 The GPU pair-set tests check the kernel itself bit for bit.
 """
@@ -58,8 +59,12 @@ def make_spheres(rng, grid, n):
         i, j = rng.integers(0, n, size=2)
         if i == j:
             continue
-        u = rng.normal(size=3)
-        u /= np.linalg.norm(u)
+        if rng.random() < 0.5:  # along an axis: where the box bound is tight
+            u = np.zeros(3)
+            u[rng.integers(0, 3)] = rng.choice([-1.0, 1.0])
+        else:
+            u = rng.normal(size=3)
+            u /= np.linalg.norm(u)
         limit = float((radius[i] + radius[j] + skin) * 1.0002) + float(sphere_eps)
         c[j] = (c[i].astype(np.float64) + u * limit * (1.0 - rng.uniform(0.0, 2e-6))).astype(f32)
     return c, radius, skin, sphere_eps
