@@ -388,8 +388,11 @@ typedef struct {
  * and 262144 cells; larger inputs are rejected with TGL_ERR_UNSUPPORTED.
  * The kernels are queued on `stream` (a cudaStream_t, NULL = default) and
  * the call returns without waiting. The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture. All calls share the one
+ * array's device address (cudaGetSymbolAddress) with that device current,
+ * and so does the first call after that device's context was replaced (a
+ * cudaDeviceReset, say); make those calls before any stream capture. Each
+ * axis of `cells` and their product must be at most 262144; the check runs
+ * before anything is queued. All calls share the one
  * array: two calls whose kernels overlap on the GPU (different streams, or
  * different host threads) race and corrupt each other's results. */
 int tgl_contact_pass_noalloc(const tgl_noalloc_inputs *inputs, float *corrections, float *segment_max_penetration,

@@ -60,6 +60,21 @@ inline uint32_t f32_to_u32(float x) {
     return (uint32_t)x;
 }
 
+/* The cell count of a grid, or 0 when it is unusable: an axis with no cell
+ * or more than 2^30 cells (proxy_cell's periodic wrap (raw % n + n) % n is
+ * done in i32 and stays below 2^31 only then), or a product above `limit`,
+ * checked after every factor so it cannot wrap. world.rs:410-415 sizes each
+ * axis as `floor(extent / cell).max(1) as u32`. */
+inline uint64_t checked_cell_count(const uint32_t cells[3], uint64_t limit) {
+    uint64_t C = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (cells[a] == 0 || cells[a] > (1u << 30)) return 0;
+        C *= cells[a];
+        if (C > limit) return 0;
+    }
+    return C;
+}
+
 inline uint32_t f32_bits(float x) {
     uint32_t u;
     std::memcpy(&u, &x, 4);
@@ -307,8 +322,8 @@ int size_world(orc_world &w, const orc_cell_list_config &cl, float max_step) {
         float cells = std::fmax(std::floor(extent[a] / w.cell_size), 1.0f);
         dims[a] = f32_to_u32(cells);
     }
-    uint64_t cell_count = (uint64_t)dims[0] * dims[1] * dims[2];
-    if (cell_count > (1ull << 31)) return fail("cell grid too large: the cell size is tiny against the box");
+    uint64_t cell_count = checked_cell_count(dims, 1ull << 31);
+    if (cell_count == 0 || !(w.cell_size > 0.0f)) return fail("cell grid too large: the cell size is tiny against the box");
     w.grid.cx = dims[0];
     w.grid.cy = dims[1];
     w.grid.cz = dims[2];
@@ -1407,16 +1422,15 @@ int orc_compact_cell(orc_world *w, const float new_lower[3], const float new_upp
     if (!w || !new_lower || !new_upper) return fail("null argument");
     if (kinematics > 2) return fail("kinematics must be 0, 1 or 2");
     uint32_t cells[3];
-    uint64_t C = 1;
     for (int a = 0; a < 3; ++a) {
         if (!std::isfinite(new_lower[a]) || !std::isfinite(new_upper[a])) return fail("bounds must be finite");
         if (!(new_upper[a] - new_lower[a] > 2.0f * w->maximum_radius)) return fail("cell narrower than two radii");
         if (!(new_lower[a] >= w->grid.lower[a]) || !(new_upper[a] <= w->grid.upper[a]))
             return fail("compaction cannot grow the cell");
         cells[a] = f32_to_u32(std::fmax(std::floor((new_upper[a] - new_lower[a]) / w->cell_size), 1.0f));
-        C *= cells[a];
     }
-    if (C > w->allocated_cells) return fail("the compacted grid needs more cells than allocated");
+    const uint64_t C = checked_cell_count(cells, w->allocated_cells);
+    if (C == 0) return fail("the compacted grid needs more cells than allocated");
     const float *ol = w->grid.lower, *ou = w->grid.upper;
     if (kinematics == 0) {
         for (uint32_t f = 0; f < w->F; ++f) {

@@ -25,6 +25,7 @@ import dataclasses
 import io
 import os
 import tempfile
+import zipfile
 from dataclasses import dataclass
 from pathlib import Path
 from typing import Optional
@@ -138,12 +139,23 @@ def encode(checkpoint: RunCheckpoint) -> bytes:
 
 
 def decode(data: bytes, case_id: str) -> RunCheckpoint:
-    """load_checkpoint (lib.rs:347-377): magic, schema, then the case id."""
+    """load_checkpoint (lib.rs:347-377): magic, schema, then the case id.
+    Every failure to decode the body (a truncated file, a missing field, a
+    malformed array) is a CheckpointError, as in the reference."""
     magic = data[: len(MAGIC)]
     schema = int.from_bytes(data[len(MAGIC): len(MAGIC) + 4], "little") if len(data) >= len(MAGIC) + 4 else 0
     if magic != MAGIC or schema != SCHEMA:
         raise CheckpointError(f"incompatible checkpoint schema: magic {magic!r}, schema {schema}")
-    with np.load(io.BytesIO(data[len(MAGIC) + 4:])) as archive:
+    try:
+        return _decode_body(data[len(MAGIC) + 4:], case_id)
+    except CheckpointError:
+        raise
+    except (KeyError, ValueError, TypeError, EOFError, OSError, zipfile.BadZipFile) as error:
+        raise CheckpointError(f"failed to decode checkpoint: {type(error).__name__}: {error}") from error
+
+
+def _decode_body(body: bytes, case_id: str) -> RunCheckpoint:
+    with np.load(io.BytesIO(body)) as archive:
         found = bytes(archive["case_id"]).decode("utf-8")
         if found != case_id:
             raise CheckpointError(f"checkpoint case mismatch: expected {case_id!r}, found {found!r}")

@@ -15,6 +15,7 @@
 // (crates/tangle_contact/src/device/contact.rs:232-902) with every segment
 // taking the exact 27-cell scan (contact.rs:365-437): the contacts a world
 // of neighbor_capacity 1 finds, summed in the same cell order.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,8 +43,15 @@ constexpr uint32_t FULL = 0xFFFFFFFFu;
 constexpr size_t NOALLOC_WORDS = 2ull * NOALLOC_MAX_CELLS + 3ull * NOALLOC_MAX_SEGMENTS;
 static __device__ __align__(256) uint32_t noalloc_scratch[NOALLOC_WORDS];
 
+// The array's address per device, with the id of the CUDA context it was
+// looked up in: a context that is destroyed and created again (after
+// cudaDeviceReset, say) reloads the library's module, and the array may move.
+struct ScratchSlot {
+    unsigned long long context_id;
+    uint32_t *address;
+};
 std::mutex g_scratch_mutex;
-uint32_t *g_scratch[NOALLOC_MAX_DEVICES] = {};
+ScratchSlot g_scratch[NOALLOC_MAX_DEVICES] = {};
 
 // Messages go where tgl_last_error() reads them.
 int noalloc_error(int code, const std::string &message) {
@@ -218,22 +226,55 @@ __global__ void noalloc_contact(NoallocArgs a) {
     }
 }
 
-// The scratch array's device address on the current device, looked up once
-// per device (cudaGetSymbolAddress on a __device__ array; the host-side
-// name of the array is not a device address).
+// The unique id (cuCtxGetId, CUDA 12.0+) of the calling thread's current
+// context, through the runtime's driver entry points so the library does not
+// link libcuda itself. Ids are never reused within a process, unlike context
+// handles. False when no context is current yet or the driver lacks either
+// call.
+bool current_context_id(unsigned long long *id) {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa = cudaDriverEntryPointSymbolNotFound, qb = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+            qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b)
+            return false;
+        get_current = reinterpret_cast<GetCurrent>(a);
+        get_id = reinterpret_cast<GetId>(b);
+    }
+    CUcontext ctx = nullptr;
+    return get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// The scratch array's device address in the current device's context. The
+// host-side name of a __device__ array is not a device address, so it is
+// looked up with cudaGetSymbolAddress: on the first call on each device, and
+// again whenever that device's current context is a new one.
 int scratch_address(uint32_t **out) {
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= NOALLOC_MAX_DEVICES)
         return noalloc_error(TGL_ERR_NO_DEVICE, "no usable current CUDA device");
+    unsigned long long context = 0;
+    bool known = current_context_id(&context);
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch[device]) {
+    ScratchSlot &slot = g_scratch[device];
+    if (!known || !slot.address || slot.context_id != context) {
         void *ptr = nullptr;
+        // With no context current yet, this lookup makes the runtime create
+        // the device's primary context; its id is read afterwards.
         cudaError_t e = cudaGetSymbolAddress(&ptr, noalloc_scratch);
         if (e != cudaSuccess)
             return noalloc_error(TGL_ERR_CUDA, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-        g_scratch[device] = static_cast<uint32_t *>(ptr);
+        if (!known && !current_context_id(&context))
+            return noalloc_error(TGL_ERR_CUDA, "cannot identify the current CUDA context");
+        slot.address = static_cast<uint32_t *>(ptr);
+        slot.context_id = context;
     }
-    *out = g_scratch[device];
+    *out = slot.address;
     return 0;
 }
 
@@ -249,12 +290,22 @@ extern "C" int tgl_contact_pass_noalloc(const tgl_noalloc_inputs *in, float *cor
     if (in->segment_count > NOALLOC_MAX_SEGMENTS)
         return noalloc_error(TGL_ERR_UNSUPPORTED, "tgl_contact_pass_noalloc takes at most 262144 segments, got " +
                                                       std::to_string(in->segment_count));
-    uint64_t cells = (uint64_t)in->cells[0] * in->cells[1] * in->cells[2];
     if (in->cells[0] == 0 || in->cells[1] == 0 || in->cells[2] == 0)
         return noalloc_error(TGL_ERR_INVALID, "every axis needs at least one cell");
-    if (cells > NOALLOC_MAX_CELLS)
-        return noalloc_error(TGL_ERR_UNSUPPORTED,
-                             "tgl_contact_pass_noalloc takes at most 262144 cells, got " + std::to_string(cells));
+    // Each axis is bounded before it is multiplied, and the running product
+    // after every factor, so the count cannot wrap: a factor is at most
+    // 2^18 and the product before it at most 2^18.
+    uint64_t cells = 1;
+    for (int ax = 0; ax < 3; ++ax) {
+        if (in->cells[ax] > NOALLOC_MAX_CELLS)
+            return noalloc_error(TGL_ERR_UNSUPPORTED, "tgl_contact_pass_noalloc takes at most 262144 cells, got " +
+                                                          std::to_string(in->cells[ax]) + " on one axis");
+        cells *= in->cells[ax];
+        if (cells > NOALLOC_MAX_CELLS)
+            return noalloc_error(TGL_ERR_UNSUPPORTED, "tgl_contact_pass_noalloc takes at most 262144 cells, got " +
+                                                          std::to_string(in->cells[0]) + " x " + std::to_string(in->cells[1]) +
+                                                          " x " + std::to_string(in->cells[2]));
+    }
     if (!(in->correction_fraction > 0.0f && in->correction_fraction <= 1.0f) || in->contact_aggregation > 2)
         return noalloc_error(TGL_ERR_INVALID, "correction_fraction must be in (0, 1], contact_aggregation 0-2");
     uint32_t *scratch = nullptr;

@@ -44,6 +44,22 @@ uint32_t f32_to_u32_host(float x) {
     return (uint32_t)x;
 }
 
+// The cell count of a grid, or 0 when the grid is unusable: an axis with no
+// cell or more than 2^30 cells (proxy_cell and stencil_cell wrap periodic
+// axes in i32 as (raw % n + n) % n, which stays below 2^31 only then), or a
+// product above `limit`. The product is checked after every factor, so it
+// cannot wrap (a factor is at most 2^30 and the running product at most
+// `limit` <= 2^32 before it).
+uint64_t checked_cell_count(const uint32_t cells[3], uint64_t limit) {
+    uint64_t C = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (cells[a] == 0 || cells[a] > (1u << 30)) return 0;
+        C *= cells[a];
+        if (C > limit) return 0;
+    }
+    return C;
+}
+
 struct GraphKey {
     uint32_t iterations;
     StepParams sp;
@@ -454,7 +470,6 @@ int prepare_specimen(const tgl_packed *pk, const tgl_cell_list_config *cl, float
     float piece_length = std::fmin(maximum_length, std::fmax(maximum_length, 2.0f * interaction_margin));
     h.cell_size = (piece_length + interaction_margin) * cl->cell_size_scale;
     Grid grid{};
-    uint64_t C = 1;
     for (int a = 0; a < 3; ++a) {
         grid.lower[a] = pk->cell_lower[a];
         grid.upper[a] = pk->cell_upper[a];
@@ -464,9 +479,10 @@ int prepare_specimen(const tgl_packed *pk, const tgl_cell_list_config *cl, float
         grid.length[a] = extent;
         grid.width[a] = extent / (float)grid.cells[a];
         grid.inv_length[a] = 1.0f / extent;
-        C *= grid.cells[a];
     }
-    if (C > (1ull << 31)) return set_error(TGL_ERR_UNSUPPORTED, "cell grid too large: the cell size is tiny against the box");
+    const uint64_t C = checked_cell_count(grid.cells, 1ull << 31);
+    if (C == 0 || !(h.cell_size > 0.0f))
+        return set_error(TGL_ERR_UNSUPPORTED, "cell grid too large: the cell size is tiny against the box");
     // world.rs:476-509 and :874-917: list room and the byte cap.
     uint64_t max_bytes = cl->max_list_bytes ? cl->max_list_bytes : REFERENCE_MAX_LIST_BYTES;
     uint64_t slots = std::min<uint64_t>((uint64_t)cl->neighbor_capacity * S, max_bytes / 4);
@@ -1185,14 +1201,13 @@ int tgl_capture_contacts(tgl_world *w, float maximum_surface_gap, uint32_t capac
     // than the neighbor grid, whose cell buffers the capture reuses).
     WorldDev cap = w->dev;
     const float cell = w->cell_size + maximum_surface_gap;
-    uint64_t C = 1;
     for (int a = 0; a < 3; ++a) {
         const float extent = cap.grid.length[a];
         cap.grid.cells[a] = f32_to_u32_host(std::fmax(std::floor(extent / cell), 1.0f));
         cap.grid.width[a] = extent / (float)cap.grid.cells[a];
-        C *= cap.grid.cells[a];
     }
-    if (C > w->dev.C) return set_error(TGL_ERR_UNSUPPORTED, "capture grid finer than the neighbor grid");
+    const uint64_t C = checked_cell_count(cap.grid.cells, w->dev.C);
+    if (C == 0) return set_error(TGL_ERR_UNSUPPORTED, "capture grid finer than the neighbor grid");
     cap.C = (uint32_t)C;
     uint32_t *count_d = nullptr, *pairs_d = nullptr;
     float *coords_d = nullptr, *gaps_d = nullptr, *angles_d = nullptr;
@@ -1533,7 +1548,6 @@ int tgl_world_compact_cell(tgl_world *w, const float new_lower[3], const float n
     WorldDev &d = w->dev;
     // world.rs:1937-1950.
     uint32_t cells[3];
-    uint64_t C = 1;
     for (int a = 0; a < 3; ++a) {
         if (!std::isfinite(new_lower[a]) || !std::isfinite(new_upper[a]))
             return set_error(TGL_ERR_INVALID, "the new cell bounds must be finite");
@@ -1542,9 +1556,9 @@ int tgl_world_compact_cell(tgl_world *w, const float new_lower[3], const float n
         if (!(new_lower[a] >= d.grid.lower[a]) || !(new_upper[a] <= d.grid.upper[a]))
             return set_error(TGL_ERR_INVALID, "compaction cannot grow the cell");
         cells[a] = f32_to_u32_host(std::fmax(std::floor((new_upper[a] - new_lower[a]) / w->cell_size), 1.0f));
-        C *= cells[a];
     }
-    if (C > w->allocated_cells) return set_error(TGL_ERR_INVALID, "the compacted grid needs more cells than allocated");
+    const uint64_t C = checked_cell_count(cells, w->allocated_cells);
+    if (C == 0) return set_error(TGL_ERR_INVALID, "the compacted grid needs more cells than allocated");
     launch_compaction(d, new_lower, new_upper, kinematics, w->stream);
     w->launches += 1;
     // world.rs:2035-2053: the resident cell and the grid follow; the cell

@@ -163,3 +163,23 @@ def test_recipe_activates_inserted_fibers_step_by_step(cuda_lib):
     moved = [not np.array_equal(f.placed, p.placed) for f, p in zip(both.assembly.fibers[first.fiber_count:],
                                                                     second.fibers)]
     assert any(moved)
+
+
+def test_truncated_or_incomplete_files_raise_checkpoint_error(tmp_path):
+    """Every decode failure is a CheckpointError (lib.rs:347-377 maps them all)."""
+    import io as _io
+
+    path = tmp_path / "run.ckpt"
+    ckpt.save(path, _run_checkpoint("case"))
+    data = path.read_bytes()
+    header = len(ckpt.MAGIC) + 4
+    for cut in (header, header + 10, len(data) // 2, len(data) - 1):
+        path.write_bytes(data[:cut])
+        with pytest.raises(ckpt.CheckpointError, match="failed to decode"):
+            ckpt.load(path, "case")
+    # A well-formed archive that lacks the fields.
+    body = _io.BytesIO()
+    np.savez(body, case_id=np.frombuffer(b"case", dtype=np.uint8))
+    path.write_bytes(data[:header] + body.getvalue())
+    with pytest.raises(ckpt.CheckpointError, match="failed to decode"):
+        ckpt.load(path, "case")

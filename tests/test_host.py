@@ -13,7 +13,7 @@ import fixtures as fx
 from tangle_b200.assembly import NONE, Cell, FiberAssembly, Material, PackedAssembly
 from tangle_b200.generate import (SplitMix64, batched_specimens, cpu_runnable_specimen, mid_size_specimen,
                                   schladitz_axis_cosine_quantile)
-from tangle_b200.settings import RelaxationSettings
+from tangle_b200.settings import CellListConfig, RelaxationSettings
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -154,3 +154,28 @@ def test_no_fallback_when_the_library_is_missing(monkeypatch):
     monkeypatch.setattr(device, "LIB_PATH", "/nonexistent/libtangle_cuda.so")
     with pytest.raises(RuntimeError, match="no fallback"):
         device.load_library()
+
+
+@pytest.mark.parametrize("dims", [(1 << 21, 1 << 21, 1 << 22), (1 << 31, 1, 1), (1 << 16, 1 << 16, 1)],
+                         ids=["wrapping_product", "axis_beyond_i32", "product"])
+def test_grid_sizing_rejects_grids_whose_cell_count_would_overflow(dims):
+    """The world's grid sizing (world.rs:410-415) rejects, before touching a
+    GPU, a box whose per-axis cell counts overflow the 32-bit cell ids: an
+    axis above 2^30, or a product above 2^31 -- also one that wraps to 0 in
+    a 64-bit product (2^21 x 2^21 x 2^22 = 2^64)."""
+    from oracle import OracleWorld
+    from tangle_b200.device import DeviceWorld
+
+    assembly = cpu_runnable_specimen()
+    packed = PackedAssembly.from_assembly(assembly)
+    cell = np.float32(OracleWorld(packed, CellListConfig(), 0.06 * 10e-6).cell_size)
+    lower = np.zeros(3, dtype=np.float32)
+    upper = np.array([cell * np.float32(n + 0.5) for n in dims], dtype=np.float32)
+    # Each axis sizes to exactly the intended count (floor(extent / cell) in f32).
+    assert [int(np.floor(np.float32(u) / cell)) for u in upper] == list(dims)
+    packed.cell_lower[:] = lower
+    packed.cell_upper[:] = upper
+    with pytest.raises(Exception, match="cell grid too large"):
+        OracleWorld(packed, CellListConfig(), 0.06 * 10e-6)
+    with pytest.raises(Exception, match="cell grid too large"):
+        DeviceWorld(packed, CellListConfig(), 0.06 * 10e-6)

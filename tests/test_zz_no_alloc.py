@@ -109,18 +109,32 @@ def test_noalloc_contact_pass_matches_the_world(make, cuda_lib):
     assert float(expected_pen.max()) > 0.0  # the inputs do overlap
 
 
-def test_noalloc_rejects_inputs_beyond_its_fixed_scratch(cuda_lib):
+def rejection_inputs(segments, cells):
+    """Inputs whose pointers are never touched: the size checks come first."""
     inputs = NoallocInputs()
     inputs.positions = inputs.segment_vertices = inputs.segment_fibers = 1
     inputs.segment_radii = inputs.vertex_arc_lengths = 1
-    inputs.segment_count = (1 << 18) + 1
-    inputs.cells[:] = [1, 1, 1]
+    inputs.segment_count = segments
+    inputs.cells[:] = cells
     inputs.cell_upper[:] = [1.0, 1.0, 1.0]
     inputs.correction_fraction = 0.8
+    return inputs
+
+
+@pytest.mark.parametrize("segments, cells, message", [
+    ((1 << 18) + 1, [1, 1, 1], b"262144 segments"),
+    # 2^21 * 2^21 * 2^22 = 2^64 wraps to 0 in a 64-bit product.
+    (8, [1 << 21, 1 << 21, 1 << 22], b"262144 cells"),
+    (8, [1 << 22, 1 << 22, 1 << 20], b"262144 cells"),
+    (8, [512, 512, 2], b"262144 cells"),
+    (8, [(1 << 18) + 1, 1, 1], b"262144 cells"),
+], ids=["segments", "wrapping_product", "wrapping_product_2", "product", "axis"])
+def test_noalloc_rejects_inputs_beyond_its_fixed_scratch(segments, cells, message, cuda_lib):
+    inputs = rejection_inputs(segments, cells)
     fn = cuda_lib.tgl_contact_pass_noalloc
     fn.argtypes = [ctypes.POINTER(NoallocInputs), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     fn.restype = ctypes.c_int
     rc = fn(ctypes.byref(inputs), 1, 1, None)
-    assert rc == 5  # TGL_ERR_UNSUPPORTED, before touching any pointer
+    assert rc == 5  # TGL_ERR_UNSUPPORTED, before touching any pointer or queueing anything
     cuda_lib.tgl_last_error.restype = ctypes.c_char_p
-    assert b"262144 segments" in cuda_lib.tgl_last_error()
+    assert message in cuda_lib.tgl_last_error()
