@@ -74,9 +74,28 @@ def parse():
     ap.add_argument("--cpu-specimens", type=int, default=16, help="arena specimens the CPU baseline relaxes")
     ap.add_argument("--reference-iterations", type=int, default=4,
                     help="relaxation iterations per step of the reference arm (CPU)")
+    ap.add_argument("--beta", type=float, default=1.0 / 0.3,
+                    help="Schladitz beta of the mid-size specimen's orientation about z (0.3: z-aligned)")
+    ap.add_argument("--tta-betas", default="3.3333333333333335,0.3",
+                    help="betas of the time-to-admissible runs (comma separated; empty: the workload's only)")
     ap.add_argument("--save-positions", default=None, help="write the positions after the timed steps (.npy)")
     ap.add_argument("--load-positions", default=None, help="start from saved positions (.npy)")
     return ap.parse_args()
+
+
+def beta_label(beta: float) -> str:
+    if abs(beta - 1.0 / 0.3) < 1.0e-9:
+        return "Schladitz beta 1/0.3 about z (xy-biased)"
+    if abs(beta - 0.3) < 1.0e-9:
+        return "Schladitz beta 0.3 about z (z-aligned)"
+    return f"Schladitz beta {beta:g} about z"
+
+
+def bench_config(name, packs, config):
+    """The workload as both arms name it (same keys, same values)."""
+    return {"workload": name, "nodes": sum(p.vertex_count for p in packs),
+            "segments": sum(p.segment_count for p in packs), "fibers": sum(p.fiber_count for p in packs),
+            "specimens": len(packs), "neighbor_capacity": config.cell_list.neighbor_capacity}
 
 
 def dist_env():
@@ -121,9 +140,9 @@ def workload(args, rank):
         assembly = cpu_runnable_specimen(seed=1 + rank)
         name = "cpu_runnable: periodic 300 um cube, 40 straight 10 um fibers x 30 segments (1,240 nodes)"
     else:
-        assembly = mid_size_specimen(scale=args.scale, seed=1 + rank)
+        assembly = mid_size_specimen(scale=args.scale, seed=1 + rank, beta=args.beta)
         name = ("mid_size: periodic 2x2x2 mm, 20,000 wavy fibers 1.5 mm, d 7/19 um 50:50 by volume, "
-                "segment 2d, Schladitz beta 1/0.3 about z (xy-biased), curvature limit 1/(5d)")
+                f"segment 2d, {beta_label(args.beta)}, curvature limit 1/(5d)")
         if args.scale != 1.0:
             name += f", scaled {args.scale}"
     d_min = assembly.smallest_diameter()
@@ -453,9 +472,29 @@ def load_warmstart_net():
     return WarmStartNet.load(path)
 
 
-def cpu_baseline(packed, config, nodes, iterations):
-    """The oracle on the same specimen (or, for an arena, on the first
-    specimens of it, one after another), all host threads."""
+def cpu_model() -> str:
+    """The host CPU's model name (from /proc/cpuinfo), or the platform's."""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.lower().startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or platform.machine()
+
+
+def cpu_baseline(packed, config, iterations, d_min=None, start=None, compare=True):
+    """The oracle on the same specimen from the same start state (or, for an
+    arena, on its first specimens, one after another), all host threads: one
+    list-building iteration, then `iterations` timed. With `compare`, a fresh
+    CUDA world runs the same iterations from the same state and the line
+    carries the parity of the final positions (max |dx| / d and whether they
+    are bit-identical)."""
+    import numpy as np
+
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
 
@@ -464,19 +503,43 @@ def cpu_baseline(packed, config, nodes, iterations):
     packs = packed if isinstance(packed, list) else [packed]
     fixed = type(config)(**{**config.__dict__, "force_full_iterations": True})
     work, elapsed, done = 0.0, 0.0, 0
-    for p in packs:
+    parity = None
+    for i, p in enumerate(packs):
         world = orc.OracleWorld(p, config.cell_list, config.max_step)
+        if start is not None and i == 0:
+            world.upload_positions(start)
         world.run_batch(fixed, 1)  # builds the lists
         t0 = time.perf_counter()
         status = world.run_batch(fixed, iterations)
         elapsed += time.perf_counter() - t0
         done = max(status.batch_iterations, 1)
         work += p.vertex_count * done
+        if compare and i == 0 and d_min is not None:
+            from tangle_b200.device import DeviceWorld
+
+            cuda = DeviceWorld(p, config.cell_list, config.max_step)
+            if start is not None:
+                cuda.upload_positions(start)
+            cuda.run_batch(fixed, 1)
+            cuda_status = cuda.run_batch(fixed, iterations)
+            po, pd = world.download_positions(), cuda.download_positions()
+            cuda.close()
+            parity = {"iterations": 1 + iterations,
+                      "max_abs_over_d": float(np.abs(po.astype(np.float64) - pd.astype(np.float64)).max()) / d_min,
+                      "bit_exact": bool(np.array_equal(po.view(np.uint32), pd.view(np.uint32))),
+                      "tolerance_over_d": 1.0e-5,
+                      "verdict_identical": bool(status.converged == cuda_status.converged and
+                                                status.total_iterations == cuda_status.total_iterations),
+                      "specimen": "the first" if len(packs) > 1 else "the benchmarked one"}
         world.close()
     what = "the same specimen" if len(packs) == 1 else f"the first {len(packs)} specimens of the arena"
-    return {"value": work / elapsed, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{done} plain iterations of {what} after one list-building iteration, "
-                      f"{elapsed:.1f} s, OpenMP over {cores} threads"}
+    state = " from the timed region's start state" if start is not None else ""
+    out = {"value": work / elapsed, "unit": UNIT, "cores": cores, "cpu_model": cpu_model(), "kind": "port",
+           "sample": f"{done} plain iterations of {what}{state} after one list-building iteration, "
+                     f"{elapsed:.1f} s, OpenMP over {cores} threads"}
+    if parity is not None:
+        out["parity"] = parity
+    return out
 
 
 def run_reference(args):
@@ -491,8 +554,9 @@ def run_reference(args):
     assembly, config, name, d_min = workload(args, 0)
     # The arena's reference is the same algorithm world by world: a bounded
     # sample of its specimens relaxed one after another.
-    assemblies = assembly[: args.cpu_specimens] if isinstance(assembly, list) else [assembly]
-    packs = [PackedAssembly.from_assembly(a) for a in assemblies]
+    all_assemblies = assembly if isinstance(assembly, list) else [assembly]
+    all_packs = [PackedAssembly.from_assembly(a) for a in all_assemblies]
+    packs = all_packs[: args.cpu_specimens]
     cores = os.cpu_count() or 1
     orc.set_threads(cores)
     worlds = [orc.OracleWorld(p, config.cell_list, config.max_step) for p in packs]
@@ -515,10 +579,12 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": name, "nodes": nodes, "segments": sum(p.segment_count for p in packs),
-                   "specimens_timed": len(packs), "iterations_per_step": per_step,
-                   "neighbor_capacity": config.cell_list.neighbor_capacity},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+        "config": bench_config(name, all_packs, config),
+        "timing": {"iterations_per_step": per_step, "specimens_timed": len(packs),
+                   "start_state": "the initial specimen",
+                   "window": f"iterations {max(args.warmup, 1) * per_step} to "
+                             f"{(max(args.warmup, 1) + args.steps) * per_step} of the relaxation"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "cpu_model": cpu_model(), "kind": "port",
                          "sample": f"{args.steps} steps of {per_step} iterations of "
                                    + ("the same specimen" if len(packs) == 1
                                       else f"the first {len(packs)} specimens of the arena, one after another")
@@ -571,10 +637,15 @@ def run_cuda(args):
 
     for _ in range(args.warmup):
         world.run_batch(fixed, args.iterations)
-    # The state the timed steps start from; the end-to-end leg replays the
-    # same trajectory from it.
+    # The timed steps start from the initial specimen again (the warm-up
+    # batches only capture the graph and load the kernels), the state the
+    # reference arm and the CPU baseline start from too; an arena keeps the
+    # state the warm-up left. The end-to-end leg replays the same trajectory
+    # from this state.
     host = torch.empty(3 * nodes, dtype=torch.float32, pin_memory=True)
     host_np = host.numpy()
+    if not batched and not args.load_positions:
+        world.upload_positions(packed.positions)
     world.download_positions(host_np)
     bytes_start = contact_bytes(world)
     refreshes0 = world.contact_list_info()["refreshes"]
@@ -665,35 +736,71 @@ def run_cuda(args):
         e2e_value, _, _ = replica_throughput(time.perf_counter() - t0, float(nodes * done), world_size)
         e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 12 * nodes,
                "d2h_bytes_per_step": 12 * nodes + 64}
+    # The reference arm's own window of the same trajectory, on the GPU: from
+    # the initial specimen, max(W, 1) untimed steps then K timed steps of
+    # --reference-iterations iterations each (CUDA events, one host
+    # synchronisation per step as there).
+    window = None
+    if not batched and not args.load_positions:
+        world.upload_positions(packed.positions)
+        per_step = args.reference_iterations
+        for _ in range(max(args.warmup, 1)):
+            world.run_batch(fixed, per_step)
+        barrier()
+        done = 0
+        with torch.cuda.stream(stream):
+            start.record(stream)
+        for _ in range(args.steps):
+            done += world.run_batch(fixed, per_step).batch_iterations
+        with torch.cuda.stream(stream):
+            end.record(stream)
+        end.synchronize()
+        window_value, _, _ = replica_throughput(start.elapsed_time(end) / 1000.0, float(nodes * done), world_size)
+        window = {"value": window_value, "unit": UNIT, "iterations_per_step": per_step, "steps": args.steps,
+                  "first_iteration": max(args.warmup, 1) * per_step,
+                  "what": "the reference arm's iterations of the same trajectory from the initial specimen, "
+                          "timed on the GPU with CUDA events"}
     world.close()
 
     # Time to admissible from the initial specimen, plain PBD and with the
-    # learned warm start first (device-resident, same gates, same cap).
+    # learned warm start first (device-resident, same gates, same cap), for
+    # each orientation reading of the mid-size specimen.
     tta = None
     if not args.no_tta and batched:
         tta = {"plain": arena_time_to_admissible(packs, config, args.tta_iterations)}
     elif not args.no_tta:
-        tta = {"plain": time_to_admissible(packed, config, d_min, None, args.tta_iterations)}
+        from tangle_b200.generate import mid_size_specimen
+
         net = load_warmstart_net()
-        if net is not None:
-            tta["warm_start"] = time_to_admissible(packed, config, d_min, net, args.tta_iterations)
-        else:
-            tta["warm_start"] = {"unavailable": "no trained network (tangle_b200/warmstart_net.npz)"}
+        betas = [float(b) for b in args.tta_betas.split(",") if b.strip()] or [args.beta]
+        tta = {}
+        for beta in betas:
+            if args.workload == "mid_size" and abs(beta - args.beta) > 1.0e-9:
+                spec = PackedAssembly.from_assembly(mid_size_specimen(scale=args.scale, seed=1 + rank, beta=beta))
+            else:
+                spec = packed
+            entry = {"specimen": beta_label(beta),
+                     "plain": time_to_admissible(spec, config, d_min, None, args.tta_iterations)}
+            if net is not None:
+                entry["warm_start"] = time_to_admissible(spec, config, d_min, net, args.tta_iterations)
+            else:
+                entry["warm_start"] = {"unavailable": "no trained network (tangle_b200/warmstart_net.npz)"}
+            tta["beta_" + f"{beta:.2f}".rstrip("0").rstrip(".").replace(".", "_")] = entry
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu:
-        cpu = cpu_baseline(packs[: args.cpu_specimens] if batched else packed, config, None, args.cpu_iterations)
+        cpu = cpu_baseline(packs[: args.cpu_specimens] if batched else packed, config, args.cpu_iterations,
+                           d_min=d_min, start=np.load(args.load_positions) if args.load_positions else None)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-            "config": {"workload": name, "nodes": nodes,
-                       "segments": sum(p.segment_count for p in packs) if batched else packed.segment_count,
-                       "fibers": sum(p.fiber_count for p in packs) if batched else packed.fiber_count,
-                       "specimens": len(packs) if batched else 1, "iterations_per_step": args.iterations,
-                       "neighbor_capacity": config.cell_list.neighbor_capacity,
+            "config": bench_config(name, packs if batched else [packed], config),
+            "timing": {"iterations_per_step": args.iterations,
+                       "start_state": ("the state after the warm-up steps" if batched or args.load_positions
+                                       else "the initial specimen"),
                        "l2": "inputs larger than L2 (positions, geometry and lists exceed 126 MB)",
                        "parallelism": f"replicas x{world_size}"},
             "gpu_launches": int(launches),
@@ -703,6 +810,7 @@ def run_cuda(args):
             "roofline_contact": roofline_contact,
             "clocks": clock_summary,
             "e2e": e2e,
+            "reference_window": window,
             "time_to_admissible": tta,
             "cpu_baseline": cpu,
         }

@@ -80,6 +80,14 @@ class Cell:
         return f"Cell(lengths={self._lengths}, periodic={axes!r}, origin={self._origin})"
 
 
+def py_float(value: float) -> str:
+    """A float as the reference's Python reprs print it
+    (crates/tangle_python/src/common.rs:250-269): rounded to ten significant
+    digits, then Python's own repr (exponent form below 1e-4 and from 1e16,
+    with a two-digit exponent; a trailing .0 on whole numbers)."""
+    return repr(float(f"{float(value):.9e}"))
+
+
 class Material:
     """A round fiber type: `diameter` in metres and an optional
     `min_bend_radius` the relaxation keeps fibers above (_tangle.pyi:243-266)."""
@@ -102,7 +110,10 @@ class Material:
     min_bend_radius = property(lambda self: self._min_bend_radius)
 
     def __repr__(self) -> str:
-        return f'Material(name="{self._name}", diameter={self._diameter!r})'
+        text = f'Material(name="{self._name}", diameter={py_float(self._diameter)}'
+        if self._min_bend_radius is not None:
+            text += f", min_bend_radius={py_float(self._min_bend_radius)}"
+        return text + ")"
 
 
 @dataclass

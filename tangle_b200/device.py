@@ -636,6 +636,16 @@ class DeviceWorld(FormationHooks):
         self._check(self._lib.tgl_debug_cell_list(self._handle, _ptr(counts), _ptr(offsets), _ptr(segments)))
         return counts, offsets, segments
 
+    def debug_neighbor_lists_raw(self):
+        """Verlet lists as stored: true counts [S] and the block-strided list
+        array [block * S] (entries past a count, or of a segment whose count
+        exceeds the block, are unspecified)."""
+        block = self.neighbor_block
+        counts = np.empty(self.segment_count, dtype=np.uint32)
+        lists = np.empty(max(block * self.segment_count, 1), dtype=np.uint32)
+        self._check(self._lib.tgl_debug_neighbor_lists(self._handle, _ptr(counts), _ptr(lists)))
+        return counts, lists
+
     def debug_neighbor_lists(self):
         block = self.neighbor_block
         counts = np.empty(self.segment_count, dtype=np.uint32)

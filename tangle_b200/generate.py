@@ -186,6 +186,113 @@ def generate_fiber_population(cell: Cell, population: FiberPopulation) -> FiberA
     return assembly
 
 
+def sample_orientation(orientation, random: SplitMix64):
+    """sample_orientation (crates/tangle_generate/src/population.rs:567-655)
+    for the distributions the regression cases use: ("isotropic",),
+    ("aligned", axis, maximum_angle) -- a uniform cosine on the cap within
+    `maximum_angle` of `axis` and a uniform azimuth -- and ("planar", normal,
+    maximum_tilt) -- a uniform in-plane azimuth and a uniform tilt out of the
+    plane normal to `normal`."""
+    kind = orientation[0]
+    if kind == "isotropic":
+        return isotropic_direction(random)
+    if kind == "aligned":
+        axis = _normalize(orientation[1])
+        ta = perpendicular(axis)
+        tb = _normalize(_cross(axis, ta))
+        minimum_cosine = math.cos(orientation[2])
+        cosine = minimum_cosine + (1.0 - minimum_cosine) * random.unit()
+        sine = math.sqrt(max(1.0 - cosine * cosine, 0.0))
+        azimuth = 2.0 * math.pi * random.unit()
+        return [axis[i] * cosine + (ta[i] * math.cos(azimuth) + tb[i] * math.sin(azimuth)) * sine for i in range(3)]
+    if kind == "planar":
+        normal = _normalize(orientation[1])
+        a = perpendicular(normal)
+        b = _normalize(_cross(normal, a))
+        azimuth = 2.0 * math.pi * random.unit()
+        tilt = orientation[2] * (2.0 * random.unit() - 1.0)
+        return [(a[i] * math.cos(azimuth) + b[i] * math.sin(azimuth)) * math.cos(tilt) + normal[i] * math.sin(tilt)
+                for i in range(3)]
+    raise ValueError(f"unknown orientation distribution {kind!r}")
+
+
+def biased_fiber_population(cell: Cell, count: int, segments_per_fiber: int, seed: int, length: Range,
+                            radius: Range, curvature_amplitude: Range, orientation=("isotropic",),
+                            min_bend_radius: Optional[float] = None, max_attempts_per_fiber: int = 256,
+                            material: str = "fiber") -> FiberAssembly:
+    """generate_biased_fiber_population (crates/tangle_generate/src/population.rs:
+    246-357) with uniform positions: per fiber, draw length, radius, waviness
+    and handedness, reject shapes over the bend limit, orient the local
+    centerline by `sample_orientation`, and place its centre uniformly where
+    the whole fiber (with its radius) lies inside the walls
+    (sample_contained_center, :657-700). Ranges are (minimum, maximum)
+    uniform draws; a single number is a constant and draws nothing
+    (ScalarDistribution::sample, :27-32)."""
+    def sample(value, random):
+        if isinstance(value, (int, float)):
+            return float(value)
+        return float(value[0]) + (float(value[1]) - float(value[0])) * random.unit()
+
+    assembly = FiberAssembly(cell)
+    random = SplitMix64(seed)
+    low = np.array(cell.origin, dtype=np.float64)
+    high = low + np.array(cell.lengths, dtype=np.float64)
+    for fiber_index in range(count):
+        placed_fiber = None
+        for _ in range(max_attempts_per_fiber):
+            fiber_length = sample(length, random)
+            fiber_radius = sample(radius, random)
+            wave = sample(curvature_amplitude, random)
+            handedness = -1.0 if random.unit() < 0.5 else 1.0
+            intrinsic = local_centerline(segments_per_fiber, fiber_length, wave, handedness)
+            if min_bend_radius is not None and maximum_polyline_curvature(intrinsic) > (
+                    1.0 / min_bend_radius) * (1.0 + 1.0e-10):
+                continue
+            direction = sample_orientation(orientation, random)
+            ta = perpendicular(direction)
+            tb = _normalize(_cross(direction, ta))
+            offsets = (np.outer(intrinsic[:, 0], direction) + np.outer(intrinsic[:, 1], ta)
+                       + np.outer(intrinsic[:, 2], tb))
+            lower, upper = low.copy(), high.copy()
+            ok = True
+            for axis in range(3):
+                if cell.periodic[axis]:
+                    continue
+                lower[axis] = low[axis] + fiber_radius - offsets[:, axis].min()
+                upper[axis] = high[axis] - fiber_radius - offsets[:, axis].max()
+                if lower[axis] > upper[axis]:
+                    ok = False
+                    break
+            if not ok:
+                continue
+            center = np.array([lower[a] + (upper[a] - lower[a]) * random.unit() for a in range(3)])
+            placed_fiber = (intrinsic, center + offsets, fiber_radius)
+            break
+        if placed_fiber is None:
+            raise RuntimeError(f"could not place fiber {fiber_index} inside the cell")
+        intrinsic, placed, fiber_radius = placed_fiber
+        assembly.add_fiber(placed, intrinsic, radius=fiber_radius, min_bend_radius=min_bend_radius,
+                           material=material)
+    return assembly
+
+
+def orientation_tensor(centerlines) -> np.ndarray:
+    """The length-weighted orientation tensor of characterize_assembly
+    (crates/tangle_characterize/src/lib.rs:186-300, :447-463): sum over
+    segments of length * t t^T, divided by the total length (f64)."""
+    tensor = np.zeros((3, 3), dtype=np.float64)
+    total = 0.0
+    for line in centerlines:
+        points = np.asarray(line, dtype=np.float64)
+        delta = points[1:] - points[:-1]
+        lengths = np.sqrt((delta * delta).sum(axis=1))
+        keep = lengths > np.finfo(np.float64).eps
+        tangents = delta[keep] / lengths[keep, None]
+        tensor += np.einsum("n,ni,nj->ij", lengths[keep], tangents, tangents)
+        total += float(lengths[keep].sum())
+    return tensor / total if total > np.finfo(np.float64).eps else tensor
+
+
 def maximum_polyline_curvature(points: np.ndarray) -> float:
     """crates/tangle_core/src/curvature.rs:21-61 (f64)."""
     best = 0.0
