@@ -352,6 +352,46 @@ typedef struct {
     uint32_t reserved;
 } tgl_kernel_times;
 
+/* ---- Launch parameters and their autotuner (no reference counterpart: the
+ * reference's CubeCL kernels take fixed launch shapes). None of these
+ * parameters changes a result: every choice gives the same positions, bit
+ * for bit, and the same gate decisions; they only move time between
+ * kernels. */
+typedef struct {
+    uint32_t lanes_per_fiber;       /* lanes per fiber in the curvature sweeps: 2, 4, 8 or 32 */
+    uint32_t contact_blocks_per_sm; /* contact-pass blocks per SM (256 threads each): 1, 2 or 3 */
+    uint32_t build_chunk;           /* candidate slots a Verlet-build block stages at once: 512 to 4096 */
+    float contact_skin_fraction;    /* contact-list skin over the neighbor skin: 0 (lists off) or (0, 1];
+                                       above 0 only where the world allocated contact lists */
+    uint32_t reserved[4];
+} tgl_launch_params;
+
+int tgl_world_get_launch_params(tgl_world *world, tgl_launch_params *params);
+/* Applies `params` (validated first); the next batch recaptures its graph
+ * and refreshes the contact lists. */
+int tgl_world_set_launch_params(tgl_world *world, const tgl_launch_params *params);
+
+typedef struct {
+    uint32_t trials;            /* timed trial batches run */
+    uint32_t trial_iterations;  /* iterations per trial batch */
+    float default_ms;           /* the parameters the world had, per trial batch */
+    float best_ms;              /* the chosen parameters, per trial batch */
+} tgl_autotune_report;
+
+/* Searches the launch parameters one at a time (coordinate descent over the
+ * candidate sets above, starting from the world's current ones), timing
+ * each candidate with CUDA events on a batch of `trial_iterations`
+ * iterations of `config` (force_full_iterations implied), best of two after
+ * one untimed batch that captures its graph. Every trial starts from the
+ * world's state at the call: positions, last steps, formation commands and
+ * control words are saved first and restored after each trial and at the
+ * end, and the next batch rebuilds the neighbor lists, so the positions
+ * that follow are those the world would have given without the search (its
+ * rebuild count is one higher). The best parameters are applied and
+ * returned. */
+int tgl_autotune(tgl_world *world, const tgl_relax_config *config, uint32_t trial_iterations,
+                 tgl_launch_params *best, tgl_autotune_report *report);
+
 int tgl_set_kernel_timing(tgl_world *world, int enable);
 /* The cudaStream_t every kernel of this world runs on (as void*), so a
  * caller can order its own work or record CUDA events against it. */

@@ -1983,7 +1983,10 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
         for (int a = 0; a < 3; ++a) edge = std::max(edge, w.grid.length[a]);
         lp.line_eps = 4.0e-6f * edge;
     }
-    lp.contact_blocks = grid_for((w.NS + 31) / 32, CONTACT_WARPS, lp.num_sms * 3);
+    // Three 256-thread blocks are resident per SM at the kernel's launch
+    // bounds; fewer leave room to the kernels around it.
+    const int contact_per_sm = lp.tune_contact_per_sm >= 1 && lp.tune_contact_per_sm <= 3 ? lp.tune_contact_per_sm : 3;
+    lp.contact_blocks = grid_for((w.NS + 31) / 32, CONTACT_WARPS, lp.num_sms * contact_per_sm);
     // Update kernel: as many warps per block as fit 96 KB of staged fibers.
     size_t per_warp = (size_t)3 * w.max_fiber * sizeof(float4);
     int warps = 8;
@@ -1995,6 +1998,7 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     // 32 fibers per warp, an odd float4 stride per fiber so that the lanes'
     // same-index accesses spread over the banks.
     if (const char *env = std::getenv("TGL_LANES_PER_FIBER")) lp.lanes_per_fiber = std::atoi(env);
+    if (lp.tune_lanes) lp.lanes_per_fiber = lp.tune_lanes;
     if (lp.lanes_per_fiber != 2 && lp.lanes_per_fiber != 4 && lp.lanes_per_fiber != 8 && lp.lanes_per_fiber != 32)
         lp.lanes_per_fiber = 8;
     const int fpw = 32 / lp.lanes_per_fiber;
@@ -2003,7 +2007,7 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     lp.fiber_lanes = w.max_fiber <= 32u * LANES_KMAX && lp.lanes_smem <= 200 * 1024;
     lp.lanes_blocks = (int)((w.FA + fpw - 1) / fpw);
     lp.contact_lists = w.contact_skin > 0.0f;
-    lp.build_ch = 3072;
+    lp.build_ch = lp.tune_build_ch >= 512 && lp.tune_build_ch <= 4096 ? lp.tune_build_ch : 3072;
     lp.build_smem = (size_t)lp.build_ch * (sizeof(float4) + sizeof(uint32_t));
     // The sphere pre-test needs >= 3 cells on every periodic axis (see
     // rb_build_kernel); its absolute margin is 1e-6 of the largest box edge.

@@ -182,8 +182,13 @@ struct StepParams {
     uint32_t motion_model;    // 0 flexible, 1 rigid translation
 };
 
-// Launch plans, fixed per world.
+// Launch plans, fixed per world. The tune_* fields, when nonzero, override
+// the planner's own choice (tgl_world_set_launch_params and the autotuner
+// set them; no choice changes a result).
 struct LaunchPlan {
+    int tune_lanes = 0;           // lanes per fiber
+    int tune_contact_per_sm = 0;  // contact-pass blocks per SM
+    int tune_build_ch = 0;        // build chunk
     bool arena;             // the kernels' arena instantiations (several specimens)
     int num_sms;
     int contact_group;      // lanes per segment in the contact pass (8, 16 or 32)

@@ -162,6 +162,7 @@ struct tgl_world {
     float *metric_out_d = nullptr;
     uint64_t allocated_cells = 0;
     float maximum_radius = 0.0f, maximum_length = 0.0f;
+    float contact_fraction = 0.0f;  // contact-list skin over the neighbor skin (0: lists off)
 
     ~tgl_world() {
         for (auto &kv : graphs) destroy_entry(kv.second);
@@ -753,6 +754,7 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
     float longest_half = 0.5f * maximum_length;
     if (!(d.contact_half_limit > longest_half)) d.contact_skin = 0.0f;  // no room: full lists every pass
     d.contact_block = d.contact_skin > 0.0f ? CONTACT_BLOCK : 0u;
+    w->contact_fraction = d.contact_skin > 0.0f ? contact_fraction : 0.0f;
     int rc = 0;
     float4 *seg_static_d, *vtx_static_d;
     uint32_t *seg_v0_d, *fiber_s0_d, *pinned_d, *fiber_order_d;
@@ -1671,6 +1673,240 @@ int tgl_world_set_fiber_max_curvatures(tgl_world *w, const float *values, size_t
     cudaFree(values_d);
     if (e != cudaSuccess) return set_error(TGL_ERR_CUDA, std::string("curvature limits: ") + cudaGetErrorString(e));
     TGL_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The contact skin and its single-image bound for a fraction of the
+// neighbor skin (as build_world sets them); a fraction the bound leaves no
+// room for turns the lists off.
+void set_contact_skin(tgl_world *w, float fraction) {
+    WorldDev &d = w->dev;
+    d.contact_skin = fraction > 0.0f ? fraction * d.skin : 0.0f;
+    d.contact_half_limit = INFINITY;
+    for (int a = 0; a < 3; ++a)
+        if (d.grid.periodic[a])
+            d.contact_half_limit = std::fmin(
+                d.contact_half_limit, 0.999f * 0.5f * (0.5f * d.grid.length[a] - 2.0f * w->maximum_radius - d.contact_skin));
+    if (!(d.contact_half_limit > 0.5f * w->maximum_length)) d.contact_skin = 0.0f;
+    w->contact_fraction = d.contact_skin > 0.0f ? fraction : 0.0f;
+}
+
+void drop_graphs(tgl_world *w) {
+    for (auto &kv : w->graphs) destroy_entry(kv.second);
+    w->graphs.clear();
+    w->last = nullptr;
+}
+
+int check_launch_params(const tgl_world *w, const tgl_launch_params &p) {
+    if (p.lanes_per_fiber != 2 && p.lanes_per_fiber != 4 && p.lanes_per_fiber != 8 && p.lanes_per_fiber != 32)
+        return set_error(TGL_ERR_INVALID, "lanes_per_fiber must be 2, 4, 8 or 32");
+    if (p.contact_blocks_per_sm < 1 || p.contact_blocks_per_sm > 3)
+        return set_error(TGL_ERR_INVALID, "contact_blocks_per_sm must be 1, 2 or 3");
+    if (p.build_chunk < 512 || p.build_chunk > 4096)
+        return set_error(TGL_ERR_INVALID, "build_chunk must be between 512 and 4096");
+    if (!(p.contact_skin_fraction >= 0.0f && p.contact_skin_fraction <= 1.0f))
+        return set_error(TGL_ERR_INVALID, "contact_skin_fraction must be in [0, 1]");
+    if (p.contact_skin_fraction > 0.0f && w->dev.contact_block == 0)
+        return set_error(TGL_ERR_UNSUPPORTED, "this world has no contact lists to size");
+    return 0;
+}
+
+void current_launch_params(const tgl_world *w, tgl_launch_params *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->lanes_per_fiber = (uint32_t)w->lp.lanes_per_fiber;
+    const int per_sm = (w->lp.contact_blocks + w->lp.num_sms - 1) / std::max(w->lp.num_sms, 1);
+    p->contact_blocks_per_sm = (uint32_t)(w->lp.tune_contact_per_sm ? w->lp.tune_contact_per_sm : std::min(3, std::max(per_sm, 1)));
+    p->build_chunk = (uint32_t)w->lp.build_ch;
+    p->contact_skin_fraction = w->contact_fraction;
+}
+
+int apply_launch_params(tgl_world *w, const tgl_launch_params &p) {
+    if (int rc = check_launch_params(w, p)) return rc;
+    w->lp.tune_lanes = (int)p.lanes_per_fiber;
+    w->lp.tune_contact_per_sm = (int)p.contact_blocks_per_sm;
+    w->lp.tune_build_ch = (int)p.build_chunk;
+    if (w->dev.contact_block) set_contact_skin(w, p.contact_skin_fraction);
+    plan_launches(w->dev, w->lp);
+    drop_graphs(w);
+    // The contact lists were filtered at the old skin: refresh them first.
+    if (w->dev.contact_block) {
+        const uint32_t one = 1;
+        TGL_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(w->dev.ctl) + offsetof(Control, contact_state), &one,
+                                 sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
+        TGL_CUDA(cudaStreamSynchronize(w->stream));
+    }
+    return 0;
+}
+
+// The state a trial batch changes and the search restores: positions, the
+// last applied steps, the formation commands and the control words (the
+// lists, snapshots and corrections are rebuilt from these).
+struct SavedState {
+    float4 *pos = nullptr;
+    float *step = nullptr;
+    float *command = nullptr;
+    std::vector<Control> ctl;
+    ~SavedState() {
+        cudaFree(pos);
+        cudaFree(step);
+        cudaFree(command);
+    }
+};
+
+int save_state(tgl_world *w, SavedState &s) {
+    const WorldDev &d = w->dev;
+    if (cudaMalloc(&s.pos, d.V * sizeof(float4)) != cudaSuccess || cudaMalloc(&s.step, d.V * sizeof(float)) != cudaSuccess)
+        return set_error(TGL_ERR_MEMORY, "cudaMalloc of the autotuner's saved state failed");
+    if (w->target_count && cudaMalloc(&s.command, w->target_count * sizeof(float)) != cudaSuccess)
+        return set_error(TGL_ERR_MEMORY, "cudaMalloc of the autotuner's saved state failed");
+    const size_t words = w->arena ? (size_t)w->specimens + 1 : 1;
+    s.ctl.resize(words);
+    TGL_CUDA(cudaMemcpyAsync(s.pos, d.pos, d.V * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
+    TGL_CUDA(cudaMemcpyAsync(s.step, d.vertex_step, d.V * sizeof(float), cudaMemcpyDeviceToDevice, w->stream));
+    if (s.command)
+        TGL_CUDA(cudaMemcpyAsync(s.command, d.command_coord, w->target_count * sizeof(float), cudaMemcpyDeviceToDevice,
+                                 w->stream));
+    TGL_CUDA(cudaMemcpyAsync(s.ctl.data(), d.ctl, words * sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    return 0;
+}
+
+// Puts the saved state back and requests a neighbor-list rebuild and a
+// contact-list refresh for the next batch.
+int restore_state(tgl_world *w, const SavedState &s) {
+    const WorldDev &d = w->dev;
+    TGL_CUDA(cudaMemcpyAsync(d.pos, s.pos, d.V * sizeof(float4), cudaMemcpyDeviceToDevice, w->stream));
+    TGL_CUDA(cudaMemcpyAsync(d.vertex_step, s.step, d.V * sizeof(float), cudaMemcpyDeviceToDevice, w->stream));
+    if (s.command)
+        TGL_CUDA(cudaMemcpyAsync(d.command_coord, s.command, w->target_count * sizeof(float), cudaMemcpyDeviceToDevice,
+                                 w->stream));
+    std::vector<Control> ctl = s.ctl;
+    for (Control &c : ctl) {
+        c.neighbor_state[0] = 1;
+        c.contact_state[0] = 1;
+    }
+    TGL_CUDA(cudaMemcpyAsync(d.ctl, ctl.data(), ctl.size() * sizeof(Control), cudaMemcpyHostToDevice, w->stream));
+    w->launches += launch_refresh_geometry(d, w->stream);
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    return 0;
+}
+
+// One trial: the saved state, an untimed batch (graph capture), then the
+// better of two timed batches.
+int trial(tgl_world *w, const SavedState &s, const tgl_relax_config &config, uint32_t iterations, float *ms) {
+    tgl_batch_status st{};
+    cudaEvent_t start = nullptr, end = nullptr;
+    if (cudaEventCreate(&start) != cudaSuccess || cudaEventCreate(&end) != cudaSuccess) {
+        cudaEventDestroy(start);
+        return set_error(TGL_ERR_CUDA, "cudaEventCreate failed");
+    }
+    float best = INFINITY;
+    int rc = 0;
+    for (int run = 0; run < 3 && rc == 0; ++run) {
+        if ((rc = restore_state(w, s))) break;
+        cudaEventRecord(start, w->stream);
+        if ((rc = tgl_run_batch(w, &config, iterations, &st))) break;
+        cudaEventRecord(end, w->stream);
+        if (cudaEventSynchronize(end) != cudaSuccess) {
+            rc = set_error(TGL_ERR_CUDA, "trial batch failed");
+            break;
+        }
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, start, end);
+        if (run > 0) best = std::fmin(best, t);
+    }
+    cudaEventDestroy(start);
+    cudaEventDestroy(end);
+    *ms = best;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tgl_world_get_launch_params(tgl_world *w, tgl_launch_params *params) {
+    if (!w || !params) return set_error(TGL_ERR_INVALID, "null argument");
+    current_launch_params(w, params);
+    return 0;
+}
+
+int tgl_world_set_launch_params(tgl_world *w, const tgl_launch_params *params) {
+    if (!w || !params) return set_error(TGL_ERR_INVALID, "null argument");
+    return apply_launch_params(w, *params);
+}
+
+int tgl_autotune(tgl_world *w, const tgl_relax_config *config, uint32_t trial_iterations, tgl_launch_params *best,
+                 tgl_autotune_report *report) {
+    if (!w || !config || !best) return set_error(TGL_ERR_INVALID, "null argument");
+    if (trial_iterations == 0 || trial_iterations > 4096)
+        return set_error(TGL_ERR_INVALID, "trial_iterations must be between 1 and 4096");
+    if (int rc = validate_config(*config)) return rc;
+    tgl_relax_config trial_config = *config;
+    trial_config.force_full_iterations = 1;
+    const bool was_timing = w->timing;
+    if (was_timing) tgl_set_kernel_timing(w, 0);
+    SavedState saved;
+    if (int rc = save_state(w, saved)) return rc;
+    tgl_launch_params current{};
+    current_launch_params(w, &current);
+    const tgl_launch_params original = current;
+    float current_ms = INFINITY;
+    uint32_t trials = 0;
+    auto fail = [&](int rc) {
+        apply_launch_params(w, original);
+        restore_state(w, saved);
+        if (was_timing) tgl_set_kernel_timing(w, 1);
+        return rc;
+    };
+    if (int rc = apply_launch_params(w, current)) return fail(rc);
+    if (int rc = trial(w, saved, trial_config, trial_iterations, &current_ms)) return fail(rc);
+    ++trials;
+    const float default_ms = current_ms;
+    const bool lanes = w->lp.fiber_lanes && config->motion_model == 0;
+    const uint32_t lane_choices[] = {2, 4, 8, 32};
+    const uint32_t block_choices[] = {1, 2, 3};
+    const uint32_t chunk_choices[] = {1024, 2048, 3072, 4096};
+    const float skin_choices[] = {0.05f, 0.1f, 0.15f, 0.25f};
+    // Coordinate descent: each parameter in turn over its candidates, the
+    // others held at the best so far.
+    for (int parameter = 0; parameter < 4; ++parameter) {
+        std::vector<tgl_launch_params> candidates;
+        tgl_launch_params c = current;
+        if (parameter == 0 && lanes)
+            for (uint32_t v : lane_choices) c.lanes_per_fiber = v, candidates.push_back(c);
+        if (parameter == 1)
+            for (uint32_t v : block_choices) c.contact_blocks_per_sm = v, candidates.push_back(c);
+        if (parameter == 2)
+            for (uint32_t v : chunk_choices) c.build_chunk = v, candidates.push_back(c);
+        if (parameter == 3 && w->dev.contact_block)
+            for (float v : skin_choices) c.contact_skin_fraction = v, candidates.push_back(c);
+        for (const tgl_launch_params &candidate : candidates) {
+            if (std::memcmp(&candidate, &current, sizeof(candidate)) == 0) continue;
+            if (int rc = apply_launch_params(w, candidate)) return fail(rc);
+            float ms = INFINITY;
+            if (int rc = trial(w, saved, trial_config, trial_iterations, &ms)) return fail(rc);
+            ++trials;
+            if (ms < current_ms) {
+                current_ms = ms;
+                current = candidate;
+            }
+        }
+    }
+    if (int rc = apply_launch_params(w, current)) return fail(rc);
+    if (int rc = restore_state(w, saved)) return fail(rc);
+    if (was_timing) tgl_set_kernel_timing(w, 1);
+    *best = current;
+    if (report) {
+        report->trials = trials;
+        report->trial_iterations = trial_iterations;
+        report->default_ms = default_ms;
+        report->best_ms = current_ms;
+    }
     return 0;
 }
 

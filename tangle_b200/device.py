@@ -43,7 +43,8 @@ EXPORTS = (
     "tgl_convert_bf16", "tgl_world_set_active_fibers", "tgl_world_set_layer_targets", "tgl_world_set_vertex_targets",
     "tgl_world_vertex_target_state", "tgl_world_target_errors", "tgl_world_compact_cell", "tgl_world_cell_bounds",
     "tgl_world_compaction_metrics", "tgl_world_wall_reactions", "tgl_world_set_wall_reactions",
-    "tgl_world_set_fiber_max_curvatures",
+    "tgl_world_set_fiber_max_curvatures", "tgl_world_get_launch_params", "tgl_world_set_launch_params",
+    "tgl_autotune",
     "tgl_last_error",
 )
 
@@ -154,6 +155,42 @@ class KernelTimes(ctypes.Structure):
     ]
 
 
+class LaunchParams(ctypes.Structure):
+    """tgl_launch_params: launch shapes that never change a result."""
+
+    _fields_ = [
+        ("lanes_per_fiber", ctypes.c_uint32),
+        ("contact_blocks_per_sm", ctypes.c_uint32),
+        ("build_chunk", ctypes.c_uint32),
+        ("contact_skin_fraction", ctypes.c_float),
+        ("reserved", ctypes.c_uint32 * 4),
+    ]
+
+    FIELDS = ("lanes_per_fiber", "contact_blocks_per_sm", "build_chunk", "contact_skin_fraction")
+
+    def as_dict(self) -> dict:
+        return {name: (float(getattr(self, name)) if name == "contact_skin_fraction" else int(getattr(self, name)))
+                for name in self.FIELDS}
+
+    @classmethod
+    def from_dict(cls, values: dict) -> "LaunchParams":
+        out = cls()
+        for name in cls.FIELDS:
+            setattr(out, name, values[name])
+        return out
+
+
+class AutotuneReport(ctypes.Structure):
+    """tgl_autotune_report."""
+
+    _fields_ = [
+        ("trials", ctypes.c_uint32),
+        ("trial_iterations", ctypes.c_uint32),
+        ("default_ms", ctypes.c_float),
+        ("best_ms", ctypes.c_float),
+    ]
+
+
 class Status(ctypes.Structure):
     """tgl_batch_status."""
 
@@ -231,6 +268,13 @@ def load_library():
     lib.tgl_debug_corrections.restype = ctypes.c_int
     lib.tgl_kernel_launches.argtypes = [P]
     lib.tgl_kernel_launches.restype = ctypes.c_uint64
+    lib.tgl_world_get_launch_params.argtypes = [P, ctypes.POINTER(LaunchParams)]
+    lib.tgl_world_get_launch_params.restype = ctypes.c_int
+    lib.tgl_world_set_launch_params.argtypes = [P, ctypes.POINTER(LaunchParams)]
+    lib.tgl_world_set_launch_params.restype = ctypes.c_int
+    lib.tgl_autotune.argtypes = [P, ctypes.POINTER(Config), ctypes.c_uint32, ctypes.POINTER(LaunchParams),
+                                 ctypes.POINTER(AutotuneReport)]
+    lib.tgl_autotune.restype = ctypes.c_int
     lib.tgl_set_kernel_timing.argtypes = [P, ctypes.c_int]
     lib.tgl_set_kernel_timing.restype = ctypes.c_int
     lib.tgl_last_kernel_times.argtypes = [P, ctypes.POINTER(KernelTimes)]
@@ -588,6 +632,28 @@ class DeviceWorld(FormationHooks):
     def stream_handle(self) -> int:
         """The cudaStream_t (as an int) this world's kernels run on."""
         return int(self._lib.tgl_world_stream(self._handle) or 0)
+
+    def launch_params(self) -> dict:
+        """The launch shapes in use (tgl_world_get_launch_params)."""
+        out = LaunchParams()
+        self._check(self._lib.tgl_world_get_launch_params(self._handle, ctypes.byref(out)))
+        return out.as_dict()
+
+    def set_launch_params(self, params: dict) -> None:
+        """Applies launch shapes (tgl_world_set_launch_params); results do
+        not change."""
+        self._check(self._lib.tgl_world_set_launch_params(self._handle, ctypes.byref(LaunchParams.from_dict(params))))
+
+    def autotune_trials(self, config: RelaxationConfig, trial_iterations: int = 32):
+        """tgl_autotune: searches the launch shapes on this world's current
+        state (which it leaves as it found it) and applies the fastest.
+        Returns (params, report)."""
+        best = LaunchParams()
+        report = AutotuneReport()
+        self._check(self._lib.tgl_autotune(self._handle, ctypes.byref(config_struct(config)), int(trial_iterations),
+                                           ctypes.byref(best), ctypes.byref(report)))
+        return best.as_dict(), {"trials": int(report.trials), "trial_iterations": int(report.trial_iterations),
+                                "default_ms": float(report.default_ms), "best_ms": float(report.best_ms)}
 
     def set_kernel_timing(self, enable: bool) -> None:
         self._check(self._lib.tgl_set_kernel_timing(self._handle, 1 if enable else 0))

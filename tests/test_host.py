@@ -179,3 +179,26 @@ def test_grid_sizing_rejects_grids_whose_cell_count_would_overflow(dims):
         OracleWorld(packed, CellListConfig(), 0.06 * 10e-6)
     with pytest.raises(Exception, match="cell grid too large"):
         DeviceWorld(packed, CellListConfig(), 0.06 * 10e-6)
+
+
+def test_autotune_cache_keys_store_and_reload(tmp_path):
+    """The autotuner's cache: one entry per (GPU, workload shape), written
+    atomically and read back; a different shape or GPU misses."""
+    from tangle_b200 import autotune as at
+
+    shape = {"vertices": 10, "segments": 9, "cells": 27, "cell_dims": [3, 3, 3], "neighbor_block": 256,
+             "specimens": 1, "contact_lists": True, "motion_model": "flexible"}
+    key = at.workload_key("NVIDIA B200", shape)
+    assert key == at.workload_key("NVIDIA B200", dict(reversed(list(shape.items()))))
+    assert key != at.workload_key("NVIDIA H100", shape)
+    assert key != at.workload_key("NVIDIA B200", {**shape, "vertices": 11})
+    path = tmp_path / "sub" / "autotune.json"
+    entry = {"params": {"lanes_per_fiber": 8, "contact_blocks_per_sm": 3, "build_chunk": 3072,
+                        "contact_skin_fraction": 0.1}, "report": {"trials": 12}}
+    at.store(path, key, entry)
+    at.store(path, "other", {"params": {}})
+    assert at.load(path)[key] == entry
+    assert sorted(p.name for p in path.parent.iterdir()) == ["autotune.json"]  # no temporary left behind
+    path.write_text("not json")
+    assert at.load(path) == {}
+    assert at.cache_path(str(path)) == path
