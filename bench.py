@@ -626,7 +626,6 @@ def run_cuda(args):
     fixed = type(config)(**{**config.__dict__, "force_full_iterations": True})
     if args.load_positions:
         world.upload_positions(np.load(args.load_positions))
-    world.set_kernel_timing(True)
     stream = torch.cuda.ExternalStream(world.stream_handle)
 
     def barrier():
@@ -635,26 +634,22 @@ def run_cuda(args):
             torch.distributed.barrier()
             torch.cuda.synchronize()
 
+    # The production batch graphs (one device-side loop per batch) serve the
+    # warm-up and the timed steps; per-kernel times come from an instrumented
+    # replay of the same steps afterwards.
     for _ in range(args.warmup):
         world.run_batch(fixed, args.iterations)
     # The timed steps start from the initial specimen again (the warm-up
     # batches only capture the graph and load the kernels), the state the
     # reference arm and the CPU baseline start from too; an arena keeps the
-    # state the warm-up left. The end-to-end leg replays the same trajectory
-    # from this state.
+    # state the warm-up left. The end-to-end leg and the instrumented replay
+    # run the same trajectory from this state.
     host = torch.empty(3 * nodes, dtype=torch.float32, pin_memory=True)
     host_np = host.numpy()
     if not batched and not args.load_positions:
         world.upload_positions(packed.positions)
     world.download_positions(host_np)
-    bytes_start = contact_bytes(world)
-    refreshes0 = world.contact_list_info()["refreshes"]
-    launches0 = world.kernel_launches
-    contact_ms = 0.0
-    contact_passes = 0
-    update_ms = 0.0
-    updates = 0
-    rebuild_ms = 0.0
+    start_state = host_np.copy()
     iterations_done = 0
     rebuilds0 = world.neighbor_list_rebuilds()
     launches0 = world.kernel_launches
@@ -667,12 +662,6 @@ def run_cuda(args):
         for _ in range(args.steps):
             st = world.run_batch(fixed, args.iterations)
             iterations_done += st.batch_iterations
-            kt = world.last_kernel_times()
-            contact_ms += kt["contact_ms"]
-            contact_passes += kt["contact_passes"]
-            update_ms += kt["update_ms"]
-            updates += kt["updates"]
-            rebuild_ms += kt["rebuild_ms"]
         with torch.cuda.stream(stream):
             end.record(stream)
         end.synchronize()
@@ -680,15 +669,37 @@ def run_cuda(args):
     rebuilds = world.neighbor_list_rebuilds() - rebuilds0
     if args.save_positions and rank == 0:
         np.save(args.save_positions, world.download_positions())
-    bytes_end = contact_bytes(world)
-    contact_info = world.contact_list_info()
-    refreshes = contact_info["refreshes"] - refreshes0
     elapsed_ms = start.elapsed_time(end)
     barrier()
     value, elapsed_s, total_work = replica_throughput(elapsed_ms / 1000.0, float(nodes * iterations_done),
                                                      world_size)
     elapsed_ms = elapsed_s * 1000.0
     clock_summary = clocks.summary()
+
+    # Per-kernel device times: the same steps from the same state, with CUDA
+    # events recorded around every step's kernels (an unrolled graph holding
+    # the same kernels). One untimed batch captures it first.
+    world.set_kernel_timing(True)
+    world.upload_positions(start_state)
+    world.run_batch(fixed, args.iterations)
+    world.upload_positions(start_state)
+    bytes_start = contact_bytes(world)
+    refreshes0 = world.contact_list_info()["refreshes"]
+    contact_ms = update_ms = rebuild_ms = 0.0
+    contact_passes = updates = 0
+    for _ in range(args.steps):
+        world.run_batch(fixed, args.iterations)
+        kt = world.last_kernel_times()
+        contact_ms += kt["contact_ms"]
+        contact_passes += kt["contact_passes"]
+        update_ms += kt["update_ms"]
+        updates += kt["updates"]
+        rebuild_ms += kt["rebuild_ms"]
+    bytes_end = contact_bytes(world)
+    contact_info = world.contact_list_info()
+    refreshes = contact_info["refreshes"] - refreshes0
+    world.set_kernel_timing(False)
+    host_np[:] = start_state
 
     # Roofline of the contact pass: the passes' algorithmic bytes (listed and
     # refresh passes weighted by their counts, list sizes averaged over the

@@ -228,6 +228,8 @@ struct Control {
     uint32_t contact_state[2];
     // Rebuild pipelines a batch graph's conditional node has run.
     uint32_t rebuild_bodies;
+    // Steps a looped batch graph has begun (its WHILE node's counter).
+    uint32_t loop_step;
 };
 
 }  // namespace tgl

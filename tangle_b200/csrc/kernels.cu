@@ -77,6 +77,7 @@ __device__ inline void begin_batch(Control *ctl) {
 
 template <bool A>
 __global__ void begin_batch_kernel(WorldDev w) {
+    if (threadIdx.x == 0) w.ctl->loop_step = 0;
     if (!A) {
         if (threadIdx.x == 0) begin_batch(w.ctl);
         return;
@@ -2126,6 +2127,26 @@ __global__ void rebuild_condition_kernel(WorldDev w, cudaGraphConditionalHandle 
 
 int launch_rebuild_condition(const WorldDev &w, cudaGraphConditionalHandle rebuild, cudaStream_t st) {
     rebuild_condition_kernel<<<1, 1, 0, st>>>(w, rebuild);
+    return 1;
+}
+
+// The step of a looped batch graph: the rebuild condition as above, and the
+// loop's own condition for after this step -- another step follows while
+// the gate keeps the batch active and fewer than `steps` have begun. A
+// batch the gate stops runs one more step, whose kernels all return at once
+// (they test the same active flag), and the loop ends.
+__global__ void step_condition_kernel(WorldDev w, cudaGraphConditionalHandle rebuild, cudaGraphConditionalHandle loop,
+                                      uint32_t steps) {
+    const bool pending = w.ctl->neighbor_state[0] != 0;
+    cudaGraphSetConditional(rebuild, pending ? 1u : 0u);
+    if (pending) w.ctl->rebuild_bodies += 1;
+    const uint32_t begun = ++w.ctl->loop_step;
+    cudaGraphSetConditional(loop, (w.ctl->control[0] != 0 && begun < steps) ? 1u : 0u);
+}
+
+int launch_step_condition(const WorldDev &w, cudaGraphConditionalHandle rebuild, cudaGraphConditionalHandle loop,
+                          uint32_t steps, cudaStream_t st) {
+    step_condition_kernel<<<1, 1, 0, st>>>(w, rebuild, loop, steps);
     return 1;
 }
 

@@ -232,6 +232,10 @@ int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp
 // Sets a batch graph's rebuild condition for one step from the pending
 // rebuild flag, and counts the rebuild pipelines it lets run.
 int launch_rebuild_condition(const WorldDev &w, cudaGraphConditionalHandle rebuild, cudaStream_t st);
+// One step of a looped batch graph: the rebuild condition and the loop's
+// condition (another step while active and fewer than `steps` begun).
+int launch_step_condition(const WorldDev &w, cudaGraphConditionalHandle rebuild, cudaGraphConditionalHandle loop,
+                          uint32_t steps, cudaStream_t st);
 int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st);
 int launch_positions_from_stage(const WorldDev &w, cudaStream_t st);
 int launch_positions_to_stage(const WorldDev &w, cudaStream_t st);

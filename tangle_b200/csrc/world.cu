@@ -72,7 +72,8 @@ struct GraphKey {
 struct GraphEntry {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int kernels = 0;
+    int kernels = 0;      // kernels per replay (a looped graph: those before its loop)
+    bool looped = false;  // one WHILE node over a step (4 kernels per step that ran)
     uint32_t iterations = 0;
     // With kernel timing on: four events per step (before the rebuild,
     // before the contact pass, before the fiber update, after it).
@@ -125,6 +126,10 @@ struct tgl_world {
     // runtime 12.8 or later), their bodies captured on body_stream.
     cudaStream_t body_stream = nullptr;
     bool conditional = false;
+    // Batch graphs loop on the device (a WHILE node over one step) unless
+    // kernel timing, which needs events per step, is on.
+    cudaStream_t loop_stream = nullptr;
+    bool loop = false;
     uint32_t rebuild_bodies_seen = 0;
     WorldDev dev{};
     LaunchPlan lp{};
@@ -170,6 +175,7 @@ struct tgl_world {
         if (host_ctl) cudaFreeHost(host_ctl);
         if (stream) cudaStreamDestroy(stream);
         if (body_stream) cudaStreamDestroy(body_stream);
+        if (loop_stream) cudaStreamDestroy(loop_stream);
     }
 
     template <typename T>
@@ -248,7 +254,8 @@ static cudaError_t capture_graph(cudaStream_t st, cudaGraph_t *graph) {
 // Appends an IF node on `handle` (with an ELSE body when `size` is 2) after
 // the capture's current dependencies and makes it the capture's only
 // dependency; its bodies come back in `bodies`.
-static cudaError_t append_if(cudaStream_t st, cudaGraphConditionalHandle handle, unsigned size, cudaGraph_t *bodies) {
+static cudaError_t append_conditional(cudaStream_t st, cudaGraphConditionalHandle handle, cudaGraphConditionalNodeType type,
+                                      unsigned size, cudaGraph_t *bodies) {
     cudaStreamCaptureStatus status;
     cudaGraph_t graph = nullptr;
     const cudaGraphNode_t *deps = nullptr;
@@ -258,7 +265,7 @@ static cudaError_t append_if(cudaStream_t st, cudaGraphConditionalHandle handle,
     cudaGraphNodeParams params{};
     params.type = cudaGraphNodeTypeConditional;
     params.conditional.handle = handle;
-    params.conditional.type = cudaGraphCondTypeIf;
+    params.conditional.type = type;
     params.conditional.size = size;
     cudaGraphNode_t node;
     if ((e = cudaGraphAddNode(&node, graph, deps, ndeps, &params)) != cudaSuccess) return e;
@@ -266,15 +273,27 @@ static cudaError_t append_if(cudaStream_t st, cudaGraphConditionalHandle handle,
     return cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
 }
 
-// Captures `enqueue(stream)` into a conditional body.
+static cudaError_t append_if(cudaStream_t st, cudaGraphConditionalHandle handle, unsigned size, cudaGraph_t *bodies) {
+    return append_conditional(st, handle, cudaGraphCondTypeIf, size, bodies);
+}
+
+// Captures `enqueue(stream)` into a conditional body on `st`.
+template <typename F>
+static cudaError_t capture_body_on(cudaStream_t st, cudaGraph_t body, F enqueue) {
+    cudaError_t e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    cudaError_t inner = enqueue(st);
+    cudaGraph_t out = nullptr;
+    e = cudaStreamEndCapture(st, &out);
+    return inner != cudaSuccess ? inner : e;
+}
+
 template <typename F>
 static cudaError_t capture_body(tgl_world *w, cudaGraph_t body, F enqueue) {
-    cudaError_t e = cudaStreamBeginCaptureToGraph(w->body_stream, body, nullptr, nullptr, 0,
-                                                  cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return e;
-    enqueue(w->body_stream);
-    cudaGraph_t out = nullptr;
-    return cudaStreamEndCapture(w->body_stream, &out);
+    return capture_body_on(w->body_stream, body, [&](cudaStream_t st) {
+        enqueue(st);
+        return cudaSuccess;
+    });
 }
 
 // One step's rebuild as a conditional node: a kernel sets the condition
@@ -320,6 +339,49 @@ int enqueue_batch(tgl_world *w, const StepParams &sp, uint32_t iterations, std::
         if (events) cudaEventRecordWithFlags((*events)[4 * step + 2], w->stream, cudaEventRecordExternal);
         kernels += launch_fiber_update(w->dev, w->lp, sp, w->stream);
         if (events) cudaEventRecordWithFlags((*events)[4 * step + 3], w->stream, cudaEventRecordExternal);
+    }
+    return kernels;
+}
+
+// run_batch's loop on the device: begin, displacement check and start
+// metrics, then one WHILE node whose body is one step -- the step condition
+// (rebuild flag, and whether another step follows), an IF node holding the
+// rebuild pipeline, the contact pass with the gate and the fiber update. The
+// gate in the contact pass ends the loop (the residual check); at most
+// iterations + 1 steps run, as in the unrolled graph, whose steps after the
+// gate stops are launches that return at once. Returns the kernels launched
+// before the loop, or -1 with the error set.
+int enqueue_batch_loop(tgl_world *w, const StepParams &sp, uint32_t iterations) {
+    int kernels = 0;
+    kernels += launch_begin_batch(w->dev, w->lp, w->stream);
+    kernels += launch_flag_displacement(w->dev, w->lp, w->stream);
+    kernels += launch_measure_start(w->dev, w->lp, w->stream);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = capture_graph(w->stream, &graph);
+    cudaGraphConditionalHandle loop = 0;
+    cudaGraph_t body = nullptr;
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) e = append_conditional(w->stream, loop, cudaGraphCondTypeWhile, 1, &body);
+    if (e == cudaSuccess)
+        e = capture_body_on(w->loop_stream, body, [&](cudaStream_t st) -> cudaError_t {
+            cudaGraph_t step_graph = nullptr;
+            cudaError_t f = capture_graph(st, &step_graph);
+            cudaGraphConditionalHandle rebuild = 0;
+            if (f == cudaSuccess) f = cudaGraphConditionalHandleCreate(&rebuild, step_graph, 0, 0);
+            if (f != cudaSuccess) return f;
+            launch_step_condition(w->dev, rebuild, loop, iterations + 1, st);
+            cudaGraph_t rebuild_body = nullptr;
+            if ((f = append_if(st, rebuild, 1, &rebuild_body)) != cudaSuccess) return f;
+            if ((f = capture_body(w, rebuild_body, [&](cudaStream_t bs) { launch_rebuild(w->dev, w->lp, bs); })) !=
+                cudaSuccess)
+                return f;
+            launch_contact(w->dev, w->lp, sp, true, st);
+            launch_fiber_update(w->dev, w->lp, sp, st);
+            return cudaGetLastError();
+        });
+    if (e != cudaSuccess) {
+        set_error(TGL_ERR_CUDA, std::string("looped batch graph: ") + cudaGetErrorString(e));
+        return -1;
     }
     return kernels;
 }
@@ -617,12 +679,14 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
     cudaGetDeviceProperties(&prop, w->device);
     if (prop.major < 10) return fail(set_error(TGL_ERR_NO_DEVICE, "the relaxation kernels are built for sm_100a"));
     if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&w->body_stream, cudaStreamNonBlocking) != cudaSuccess)
+        cudaStreamCreateWithFlags(&w->body_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&w->loop_stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(set_error(TGL_ERR_CUDA, "cudaStreamCreate failed"));
     {
         int driver = 0, runtime = 0;
         w->conditional = cudaDriverGetVersion(&driver) == cudaSuccess && cudaRuntimeGetVersion(&runtime) == cudaSuccess &&
                          driver >= 12080 && runtime >= 12080 && std::getenv("TGL_NO_CONDITIONAL_GRAPHS") == nullptr;
+        w->loop = w->conditional && std::getenv("TGL_NO_LOOP_GRAPHS") == nullptr;
     }
     if (cudaMallocHost(&w->host_ctl, (hosts.size() > 1 || arena ? hosts.size() + 1 : 1) * sizeof(Control)) != cudaSuccess)
         return fail(set_error(TGL_ERR_MEMORY, "cudaMallocHost failed"));
@@ -934,8 +998,10 @@ int tgl_run_batch(tgl_world *w, const tgl_relax_config *config, uint32_t iterati
                     return set_error(TGL_ERR_CUDA, "cudaEventCreate failed");
                 }
         }
+        entry.looped = w->loop && !w->timing;
         TGL_CUDA(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
-        entry.kernels = enqueue_batch(w, sp, iterations, w->timing ? &entry.events : nullptr);
+        entry.kernels = entry.looped ? enqueue_batch_loop(w, sp, iterations)
+                                     : enqueue_batch(w, sp, iterations, w->timing ? &entry.events : nullptr);
         cudaError_t e = cudaStreamEndCapture(w->stream, &entry.graph);
         if (entry.kernels < 0) {  // the error is set
             destroy_entry(entry);
@@ -958,6 +1024,8 @@ int tgl_run_batch(tgl_world *w, const tgl_relax_config *config, uint32_t iterati
     TGL_CUDA(cudaGraphLaunch(it->second.exec, w->stream));
     w->launches += (uint64_t)it->second.kernels;
     if (int rc = read_status(w, *config, status)) return rc;
+    if (it->second.looped)  // the step condition, two contact passes and the update per step that ran
+        w->launches += 4ull * w->host_ctl[0].loop_step;
     if (w->conditional) {  // rebuild pipelines the graph ran (10 kernels each)
         const uint32_t bodies = w->host_ctl[0].rebuild_bodies;
         w->launches += 10ull * (bodies >= w->rebuild_bodies_seen ? bodies - w->rebuild_bodies_seen : bodies);

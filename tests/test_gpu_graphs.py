@@ -1,4 +1,5 @@
-"""Batch graphs with the rebuild pipeline as a conditional node.
+"""Batch graphs with the rebuild pipeline as a conditional node, looped on
+the device.
 
 A one-thread kernel sets an IF node's condition from the pending-rebuild
 flag, so the ten gated rebuild kernels launch only when a rebuild runs. The
@@ -6,6 +7,13 @@ alternative capture (`TGL_NO_CONDITIONAL_GRAPHS=1`, read when a world is
 created) launches them every step and lets each return at once. Both must
 give the same bits, and the launch count of the conditional graph must add
 the ten kernels only for the pipelines that ran.
+
+By default the batch graph is one WHILE node over a single step: a kernel
+sets the rebuild condition and the loop's own (another step while the gate
+keeps the batch active and fewer than iterations + 1 steps have begun). The
+unrolled capture (`TGL_NO_LOOP_GRAPHS=1`) holds iterations + 1 copies of
+the step. Both give the same bits, statuses and rebuilds; the looped graph
+stops launching once the gate has stopped the batch.
 """
 
 import os
@@ -22,17 +30,21 @@ pytestmark = pytest.mark.gpu
 REBUILD_KERNELS = 10
 
 
-def make_world(packed, cell_list, max_step, conditional: bool):
+def make_world(packed, cell_list, max_step, conditional: bool, looped: bool = True):
     from tangle_b200.device import DeviceWorld
 
-    if conditional:
-        os.environ.pop("TGL_NO_CONDITIONAL_GRAPHS", None)
-        return DeviceWorld(packed, cell_list, max_step)
-    os.environ["TGL_NO_CONDITIONAL_GRAPHS"] = "1"
+    saved = {k: os.environ.pop(k, None) for k in ("TGL_NO_CONDITIONAL_GRAPHS", "TGL_NO_LOOP_GRAPHS")}
+    if not conditional:
+        os.environ["TGL_NO_CONDITIONAL_GRAPHS"] = "1"
+    if not looped:
+        os.environ["TGL_NO_LOOP_GRAPHS"] = "1"
     try:
         return DeviceWorld(packed, cell_list, max_step)
     finally:
-        os.environ.pop("TGL_NO_CONDITIONAL_GRAPHS", None)
+        for k, v in saved.items():
+            os.environ.pop(k, None)
+            if v is not None:
+                os.environ[k] = v
 
 
 def cases():
@@ -96,3 +108,24 @@ def test_conditional_graph_with_frequent_rebuilds(cuda_lib):
         (REBUILD_KERNELS - 1) * steps - REBUILD_KERNELS * rebuilds
     np.testing.assert_array_equal(cond.download_positions().view(np.uint32),
                                   gated.download_positions().view(np.uint32))
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_looped_graph_matches_the_unrolled_one(case, cuda_lib):
+    """Fixed-length batches and batches the gate stops early (the specimen
+    converges): same statuses, rebuilds and bits; after the gate stops, the
+    looped graph launches one more step and no further ones."""
+    name, assembly, cfg = case
+    packed = PackedAssembly.from_assembly(assembly, False)
+    fixed = RelaxationConfig(**{**cfg.__dict__, "force_full_iterations": True})
+    looped = make_world(packed, cfg.cell_list, cfg.max_step, True, True)
+    unrolled = make_world(packed, cfg.cell_list, cfg.max_step, True, False)
+    for config, batch in ((fixed, 9), (fixed, 40), (cfg, 128), (cfg, 128), (cfg, 64)):
+        launches = (looped.kernel_launches, unrolled.kernel_launches)
+        sl = looped.run_batch(config, batch)
+        su = unrolled.run_batch(config, batch)
+        assert sl == su, name
+        assert looped.neighbor_list_rebuilds() == unrolled.neighbor_list_rebuilds()
+        assert looped.kernel_launches - launches[0] <= unrolled.kernel_launches - launches[1]
+        np.testing.assert_array_equal(looped.download_positions().view(np.uint32),
+                                      unrolled.download_positions().view(np.uint32))
