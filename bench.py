@@ -235,12 +235,14 @@ def contact_bytes(world):
     info = world.contact_list_info()
     if info["block"] == 0:
         return full, full
-    ccounts, _ = world.debug_contact_lists()
+    ccounts, clists = world.debug_contact_lists()
     _, _, slot_segment = world.debug_cell_list()
     verlet_by_slot = listed_verlet[slot_segment]
-    walked = np.where(ccounts <= info["block"], ccounts, verlet_by_slot)
+    on_verlet = np.array([entries is None for entries in clists], dtype=bool)
+    chunked = np.where(on_verlet, 0, ccounts).astype(np.float64)
+    walked = np.where(on_verlet, verlet_by_slot, chunked)
     listed = 60.0 * S + 4.0 * float(walked.sum())
-    kept = np.minimum(ccounts, info["block"]).astype(np.float64)
+    kept = chunked
     refresh = full + 4.0 * float(kept.sum()) + 4.0 * S + 32.0 * world.vertex_count
     return listed, refresh
 

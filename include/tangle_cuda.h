@@ -324,10 +324,14 @@ int tgl_debug_cell_list(tgl_world *world, uint32_t *cell_counts, uint32_t *cell_
 /* True neighbor counts [S] and lists [S * block], segment-major; lists of
  * segments whose count exceeds the block are not meaningful. */
 int tgl_debug_neighbor_lists(tgl_world *world, uint32_t *counts, uint32_t *lists);
-/* Contact lists by cell-list slot: counts [S] (a count above the block means
- * the slot's contact pass reads the Verlet list) and lists [S * block].
- * TGL_ERR_UNSUPPORTED when contact lists are off. */
-int tgl_debug_contact_lists(tgl_world *world, uint32_t *counts, uint32_t *lists);
+/* Contact lists as the contact pass stores them: a state per cell-list slot
+ * [S] -- the slot's list length, 0xFFFFFFFE where its list ran past its
+ * batch's chunk (the pass reads the Verlet list) or 0xFFFFFFFF where the
+ * Verlet list overflowed (the pass scans the cells) -- and the chunks
+ * [ceil(S / 32) * 32 * block]: the 32 slots of batch b (slots 32b to
+ * 32b + 31) keep their lists back to back, in slot order, from entry
+ * 32b * block on. TGL_ERR_UNSUPPORTED when contact lists are off. */
+int tgl_debug_contact_lists(tgl_world *world, uint32_t *states, uint32_t *chunks);
 /* One contact pass (find_segment_corrections, contact.rs:232-902) on the
  * current positions and lists, moving nothing: corrections [6S] and
  * per-segment maximum penetration [S]. */

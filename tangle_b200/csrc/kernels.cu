@@ -78,14 +78,14 @@ __device__ inline void begin_batch(Control *ctl) {
 template <bool A>
 __global__ void begin_batch_kernel(WorldDev w) {
     if (threadIdx.x == 0) w.ctl->loop_step = 0;
-    if (!A) {
+    if constexpr (!A) {
         if (threadIdx.x == 0) begin_batch(w.ctl);
-        return;
-    }
-    for (uint32_t p = threadIdx.x; p < w.P; p += blockDim.x) begin_batch(w.ctl + 1 + p);
-    if (threadIdx.x == 0) {
-        w.ctl->control[0] = 1;  // some specimen may run; the first gate refines it
-        w.ctl->done_blocks = 0;
+    } else {
+        for (uint32_t p = threadIdx.x; p < w.P; p += blockDim.x) begin_batch(w.ctl + 1 + p);
+        if (threadIdx.x == 0) {
+            w.ctl->control[0] = 1;  // some specimen may run; the first gate refines it
+            w.ctl->done_blocks = 0;
+        }
     }
 }
 
@@ -826,16 +826,31 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         const uint32_t my_spec = A && in_range ? spec_of_seg<A>(w, segment) : 0u;
         // Segments of an arena specimen whose gate has stopped it are skipped.
         const bool valid = in_range && (!A || ctl_of<A>(w, my_spec)->control[0] != 0);
-        uint32_t count = valid ? w.nbr_count[segment] : 0u;
-        const bool listed = valid && count <= block;
+        // A listed pass reads the slot's contact-list state (coalesced), and
+        // the segment's Verlet count only where its contact list did not fit
+        // the batch's chunk; the other passes walk the Verlet lists.
+        const uint32_t cstate = MODE == CONTACT_LISTED && valid ? w.contact_count[base + lane] : 0u;
+        uint32_t count = 0u;
+        if (MODE != CONTACT_LISTED) count = valid ? w.nbr_count[segment] : 0u;
+        else if (valid && cstate == CONTACT_USE_VERLET) count = w.nbr_count[segment];
+        const bool listed = MODE == CONTACT_LISTED ? valid && cstate != CONTACT_USE_SCAN : valid && count <= block;
         if (A) lane_spec[A ? warp : 0][lane] = my_spec;
         uint32_t k = listed ? count : 0u;
         const uint32_t *source = w.nbr_list + (size_t)segment * block;
-        if (MODE == CONTACT_LISTED && listed) {
-            const uint32_t listed_count = w.contact_count[base + lane];
-            if (listed_count <= cblock) {
-                k = listed_count;
-                source = w.contact_list + (size_t)(base + lane) * cblock;
+        if (MODE == CONTACT_LISTED) {
+            // The batch's contact lists lie back to back in its chunk, in
+            // lane order: a lane's list starts after the lists of the lanes
+            // before it that read the chunk.
+            const bool chunked = listed && cstate != CONTACT_USE_VERLET;  // cstate <= 32 * cblock
+            uint32_t before = chunked ? cstate : 0u;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(FULL, before, o);
+                if (lane >= o) before += t;
+            }
+            if (chunked) {
+                k = cstate;
+                source = w.contact_list + (size_t)base * cblock + (before - cstate);
             }
         }
         uint32_t incl = k;
@@ -857,6 +872,10 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         const uint32_t total = pre[32];
         ContactAcc acc = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
         uint32_t queued = 0;
+        // Refresh: entries kept so far in this batch (the chunk's fill level;
+        // owners' lists are emitted in lane order) and the owners whose list
+        // ran past the chunk's end.
+        uint32_t emitted = 0, spilled_owners = 0;
         // Software pipeline over the flat candidate sequence: the list entry
         // of round r + 2 and the geometry of round r + 1 are in flight while
         // round r is tested.
@@ -941,17 +960,21 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
                         keep = within_contact_skin(home, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z, ea.w, cskin, line_eps_world);
                 }
                 if (MODE == CONTACT_REFRESH) {
-                    // Append the kept entries to their owners' contact lists
-                    // in queue (= list) order.
+                    // Append the kept entries to the batch's chunk in queue
+                    // order, which is list order owner after owner, so each
+                    // owner's contact list is one contiguous, ordered run.
+                    const uint32_t keeps = __ballot_sync(FULL, keep);
                     const uint32_t peers = __match_any_sync(FULL, keep ? (uint32_t)h : 32u + (uint32_t)lane);
-                    uint32_t at = 0;
                     if (keep) {
-                        at = kept[h] + __popc(peers & ((1u << lane) - 1u));
-                        if (at < cblock)
-                            w.contact_list[(size_t)(base + h) * cblock + at] = __float_as_uint(qg[2 * lane + 1].w);
+                        const uint32_t at = emitted + __popc(keeps & ((1u << lane) - 1u));
+                        if (at < 32u * cblock)
+                            w.contact_list[(size_t)base * cblock + at] = __float_as_uint(qg[2 * lane + 1].w);
+                        else
+                            spilled_owners |= 1u << h;
                     }
                     __syncwarp();
                     if (keep && lane == 31 - __clz(peers)) kept[h] += __popc(peers);
+                    emitted += __popc(keeps);
                     __syncwarp();
                 }
                 if (__any_sync(FULL, hit)) {
@@ -1003,7 +1026,13 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
             atomicMax(&ctl_of<A>(w, my_spec)->acc[0], thread_max);
             thread_max = 0;
         }
-        if (MODE == CONTACT_REFRESH && valid) w.contact_count[base + lane] = listed ? kept[lane] : 0u;
+        if (MODE == CONTACT_REFRESH) {
+            spilled_owners = __reduce_or_sync(FULL, spilled_owners);
+            if (valid)
+                w.contact_count[base + lane] = !listed ? CONTACT_USE_SCAN
+                                               : (spilled_owners >> lane) & 1u ? CONTACT_USE_VERLET
+                                                                               : kept[lane];
+        }
         uint32_t spill = __ballot_sync(FULL, valid && !listed);
         while (spill) {
             const int j = __ffs(spill) - 1;

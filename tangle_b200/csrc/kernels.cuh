@@ -62,9 +62,12 @@ struct WorldDev {
     // Verlet lists.
     uint32_t *nbr_count; // [S] true neighbor count
     uint32_t *nbr_list;  // [S * block]
-    // Contact lists (allocated only when contact_skin > 0).
-    uint32_t *contact_count; // [S] per slot; above contact_block = use the Verlet list
-    uint32_t *contact_list;  // [S * contact_block] per slot, ascending segment order
+    // Contact lists (allocated only when contact_skin > 0). The 32 slots of
+    // a contact-pass batch (slots 32b .. 32b + 31) share one chunk of
+    // 32 * contact_block entries, their lists back to back in slot order,
+    // each in ascending segment order.
+    uint32_t *contact_count; // [S] per slot: list length, CONTACT_USE_VERLET or CONTACT_USE_SCAN
+    uint32_t *contact_list;  // [S * contact_block] the chunks
     float4 *contact_ref;     // [V] positions the contact lists were filtered at
     Control *ctl;
     float *xyz_stage;    // [3V] interleaved staging for host copies
@@ -102,6 +105,12 @@ struct WorldDev {
     uint32_t target_axis;
     float target_stiffness, target_max_translation;
 };
+
+// Contact-list states of a slot besides its list length: the list ran past
+// its batch's chunk (walk the Verlet list), or the Verlet list itself
+// overflowed (the exact cell scan).
+constexpr uint32_t CONTACT_USE_VERLET = 0xFFFFFFFEu;
+constexpr uint32_t CONTACT_USE_SCAN = 0xFFFFFFFFu;
 
 // Is segment s on a fiber that takes part (staged activation)?
 __device__ inline bool segment_on(const WorldDev &w, uint32_t s) {

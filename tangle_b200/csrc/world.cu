@@ -844,7 +844,8 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
         (rc = w->alloc(&d.xyz_stage, 3 * (size_t)V)))
         return fail(rc);
     if (d.contact_block &&
-        ((rc = w->alloc(&d.contact_count, S)) || (rc = w->alloc(&d.contact_list, (size_t)S * d.contact_block)) ||
+        ((rc = w->alloc(&d.contact_count, S)) ||
+         (rc = w->alloc(&d.contact_list, (size_t)(S + 31) / 32 * 32 * d.contact_block)) ||  // whole chunks
          (rc = w->upload(&d.contact_ref, pos))))
         return fail(rc);
     d.seg_static = seg_static_d;
@@ -1133,9 +1134,10 @@ int tgl_contact_list_info(tgl_world *w, float *contact_skin, uint32_t *block, ui
 int tgl_debug_contact_lists(tgl_world *w, uint32_t *counts, uint32_t *lists) {
     if (!w || !counts || !lists) return set_error(TGL_ERR_INVALID, "null argument");
     if (!w->dev.contact_block) return set_error(TGL_ERR_UNSUPPORTED, "contact lists are off for this world");
-    TGL_CUDA(cudaMemcpyAsync(counts, w->dev.contact_count, w->dev.S * 4ull, cudaMemcpyDeviceToHost, w->stream));
-    TGL_CUDA(cudaMemcpyAsync(lists, w->dev.contact_list, (size_t)w->dev.S * w->dev.contact_block * 4ull,
-                             cudaMemcpyDeviceToHost, w->stream));
+    const size_t S = w->dev.S, padded = (S + 31) / 32 * 32;
+    TGL_CUDA(cudaMemcpyAsync(counts, w->dev.contact_count, S * 4ull, cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaMemcpyAsync(lists, w->dev.contact_list, padded * w->dev.contact_block * 4ull, cudaMemcpyDeviceToHost,
+                             w->stream));
     TGL_CUDA(cudaStreamSynchronize(w->stream));
     return 0;
 }

@@ -28,6 +28,8 @@ _lib = None
 
 TGL_ERR_INVALID = 1
 TGL_ERR_UNSUPPORTED = 5
+#: Contact-list state of a slot whose list ran past its batch's chunk.
+CONTACT_USE_VERLET = 0xFFFFFFFE
 
 #: Every symbol include/tangle_cuda.h declares.
 EXPORTS = (
@@ -679,16 +681,32 @@ class DeviceWorld(FormationHooks):
         return {"skin": float(skin.value), "block": int(block.value), "refreshes": int(refreshes.value)}
 
     def debug_contact_lists(self):
-        """Contact lists by cell-list slot: counts [S] and a list per slot
-        (None where the count exceeds the block and the Verlet list is read)."""
+        """Contact lists by cell-list slot: counts [S] and a list per slot.
+        A list of None (count CONTACT_USE_VERLET) marks a slot whose list ran
+        past its batch's chunk (its contact pass reads the Verlet list); an
+        empty list with count 0 also stands for a slot whose Verlet list
+        overflowed (it scans the cells). Unpacked from the per-batch chunks
+        tgl_debug_contact_lists returns."""
         block = self.contact_list_info()["block"]
-        counts = np.empty(self.segment_count, dtype=np.uint32)
-        lists = np.empty(max(block * self.segment_count, 1), dtype=np.uint32)
-        self._check(self._lib.tgl_debug_contact_lists(self._handle, _ptr(counts), _ptr(lists)))
+        S = self.segment_count
+        states = np.empty(S, dtype=np.uint32)
+        chunks = np.empty(max((S + 31) // 32 * 32 * block, 1), dtype=np.uint32)
+        self._check(self._lib.tgl_debug_contact_lists(self._handle, _ptr(states), _ptr(chunks)))
+        counts = np.zeros(S, dtype=np.uint32)
         out = []
-        for s in range(self.segment_count):
-            n = int(counts[s])
-            out.append(lists[block * s: block * s + n].copy() if n <= block else None)
+        for base in range(0, S, 32):
+            at = base * block
+            for slot in range(base, min(S, base + 32)):
+                state = int(states[slot])
+                if state == 0xFFFFFFFF:
+                    out.append(np.empty(0, dtype=np.uint32))
+                elif state == CONTACT_USE_VERLET:
+                    counts[slot] = CONTACT_USE_VERLET
+                    out.append(None)
+                else:
+                    counts[slot] = state
+                    out.append(chunks[at: at + state].copy())
+                    at += state
         return counts, out
 
     def debug_rebuild(self) -> None:

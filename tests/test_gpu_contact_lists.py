@@ -81,10 +81,30 @@ def test_contact_lists_are_ordered_sub_sequences_of_the_verlet_lists(case, cuda_
         full = verlet[segment]
         if full is None or entries is None:
             continue
-        assert counts[slot] <= verlet_counts[segment] and counts[slot] <= block
+        assert counts[slot] == len(entries) <= verlet_counts[segment]
         assert np.all(np.diff(entries.astype(np.int64)) > 0), f"slot {slot} not ascending"
         assert np.isin(entries, full).all(), f"slot {slot} holds entries outside its Verlet list"
         checked += 1
     assert checked > 0
-    # The contact lists are shorter than the Verlet lists they filter.
-    assert counts.sum() <= verlet_counts.sum()
+    # The contact lists are shorter than the Verlet lists they filter, and a
+    # batch's lists fit its chunk of 32 * block entries.
+    chunked = np.array([0 if entries is None else len(entries) for entries in lists], dtype=np.int64)
+    assert chunked.sum() <= verlet_counts.astype(np.int64).sum()
+    padded = np.zeros((len(lists) + 31) // 32 * 32, dtype=np.int64)
+    padded[:len(lists)] = chunked
+    assert padded.reshape(-1, 32).sum(axis=1).max() <= 32 * block
+
+
+def test_a_full_chunk_sends_its_last_lists_to_the_verlet_lists(cuda_lib, monkeypatch):
+    """With the whole neighbor skin as contact skin the lists nearly equal
+    the Verlet lists (about 41 entries a segment), more than a batch's chunk
+    of 32 * 32 entries holds: the slots whose lists run past the chunk read
+    their Verlet lists, and the positions stay the oracle's bit for bit."""
+    name, assembly, cfg = SPECIMENS[1]
+    monkeypatch.setenv("TGL_CONTACT_SKIN", "1")
+    orc, dev = run_pair(assembly, cfg, iterations=(3, 5))
+    counts, lists = dev.debug_contact_lists()
+    on_verlet = sum(1 for entries in lists if entries is None)
+    assert on_verlet > 0
+    assert any(entries is not None and len(entries) > 0 for entries in lists)
+    np.testing.assert_array_equal(orc.download_positions().view(np.uint32), dev.download_positions().view(np.uint32))
