@@ -58,7 +58,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
-    ap.add_argument("--workload", choices=["mid_size", "cpu_runnable", "batched", "ply_stack"], default="mid_size")
+    ap.add_argument("--workload", choices=["mid_size", "cpu_runnable", "batched", "ply_stack", "gemm"],
+                    default="mid_size")
     ap.add_argument("--plies", type=int, default=20, help="plies of the ply_stack workload")
     ap.add_argument("--ply-budget", type=int, default=1024, help="iteration cap per ply of the ply_stack workload")
     ap.add_argument("--ply-side", type=float, default=2.0e-3, help="ply edge of the ply_stack workload (m)")
@@ -834,12 +835,101 @@ def run_cuda(args):
     return 0
 
 
+def measured_tensor_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
+def run_gemm(args):
+    """tgl_gemm_bf16 (the warm-start network's tensor-core kernel) timed with
+    CUDA events on the network's own shapes at the mid-size specimen's scale
+    (rows = directed contact edges or vertices, the layer widths as N and
+    K) and on one large square-ish product, against the measured HBM and
+    bf16 peaks. Each shape: 3 untimed launches, then the mean of --steps."""
+    import ctypes
+
+    import torch
+
+    from tangle_b200.build import build
+    from tangle_b200.device import load_library
+
+    build()
+    torch.cuda.set_device(0)
+    lib = load_library()
+
+    class Gemm(ctypes.Structure):
+        _fields_ = [("a", ctypes.c_void_p), ("b", ctypes.c_void_p), ("lda", ctypes.c_int64), ("ldb", ctypes.c_int64),
+                    ("m", ctypes.c_int32), ("n", ctypes.c_int32), ("k", ctypes.c_int64), ("a_mn", ctypes.c_int32),
+                    ("b_mn", ctypes.c_int32), ("k_split", ctypes.c_int64), ("bias", ctypes.c_void_p),
+                    ("relu", ctypes.c_int32), ("reserved", ctypes.c_int32), ("mask", ctypes.c_void_p),
+                    ("ld_mask", ctypes.c_int64), ("residual", ctypes.c_void_p), ("ld_res", ctypes.c_int64),
+                    ("out_f32", ctypes.c_void_p), ("ldo", ctypes.c_int64), ("out_bf16", ctypes.c_void_p),
+                    ("ldo_bf16", ctypes.c_int64), ("error", ctypes.c_void_p)]
+
+    fn = lib.tgl_gemm_bf16
+    fn.argtypes = [ctypes.POINTER(Gemm), ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    hbm, hbm_kind = measured_peak()
+    tensor, tensor_kind = measured_tensor_peak()
+    shapes = [
+        # (label, m, n, k): forward products, K-major operands, bf16 output.
+        ("edge MLP layer 1 (E x 80 -> 64)", 16_000_000, 64, 80),
+        ("edge MLP layer 2 (E x 64 -> 64)", 16_000_000, 64, 64),
+        ("node MLP layer 1 (V x 192 -> 64)", 2_000_000, 64, 192),
+        ("large product (16384 x 8192 -> 256)", 16384, 256, 8192),
+    ]
+    results = []
+    for label, m, n, k in shapes:
+        a = (torch.randn(m, k, device=dev) * 0.1).to(torch.bfloat16)
+        b = (torch.randn(n, k, device=dev) * 0.1).to(torch.bfloat16)
+        out = torch.empty(m, n, dtype=torch.bfloat16, device=dev)
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+        g = Gemm(a.data_ptr(), b.data_ptr(), k, k, m, n, k, 0, 0, 0, None, 0, 0, None, 0, None, 0, None, n,
+                 out.data_ptr(), n, err.data_ptr())
+        for _ in range(3):
+            assert fn(ctypes.byref(g), stream.cuda_stream) == 0, lib.tgl_last_error()
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(args.steps):
+            fn(ctypes.byref(g), stream.cuda_stream)
+        end.record(stream)
+        end.synchronize()
+        assert int(err.item()) == 0
+        seconds = start.elapsed_time(end) / 1000.0 / args.steps
+        flops = 2.0 * m * n * k
+        traffic = 2.0 * (m * k + n * k + m * n)  # bf16 operands read once, bf16 result written
+        ref = (a[:4096].float() @ b.float().T)
+        rel = float(((out[:4096].float() - ref).abs().max() / (ref.abs().max() + 1e-30)).item())
+        results.append({"shape": label, "m": m, "n": n, "k": k, "ms": seconds * 1000.0,
+                        "tflops": flops / seconds / 1.0e12, "tensor_frac": flops / seconds / 1.0e12 / tensor,
+                        "gbs": traffic / seconds / 1.0e9, "hbm_frac": traffic / seconds / 1.0e9 / hbm,
+                        "max_rel_err_vs_f32": rel})
+        del a, b, out
+    line = {"metric": "tgl_gemm_bf16 throughput on the warm-start network's shapes", "impl": "cuda",
+            "unit": "TFLOP/s", "value": max(r["tflops"] for r in results), "steps": args.steps,
+            "dtype": "bf16 operands, f32 accumulate (tensor memory)", "data": "synthetic normal operands",
+            "peaks": {"bf16_tflops": tensor, "bf16_source": tensor_kind, "hbm_gbs": hbm, "hbm_source": hbm_kind},
+            "shapes": results}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "ply_stack":
         return run_ply_stack(args)
+    if args.workload == "gemm":
+        return run_gemm(args)
     return run_cuda(args)
 
 

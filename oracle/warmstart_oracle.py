@@ -4,8 +4,9 @@ The learned warm start has no counterpart in the reference; its gradients
 are checked against PyTorch CPU autograd in float64 on the same graph,
 features and weights. `forward` mirrors tangle_b200/warmstart.py layer by
 layer; with `round_bf16` it rounds to bf16 exactly where the device path
-stores bf16 activations, so the remaining difference is the device's bf16
-rounding of gradients and its f32 accumulation.
+stores bf16 activations, and with `round_gradients` it also rounds every
+layer's incoming gradient as the device does, so that what remains is the
+device's f32 accumulation (and the bf16 roundings its f32 sums flip).
 """
 
 from __future__ import annotations
@@ -36,15 +37,37 @@ def graph_to_cpu(graph):
     }
 
 
-def forward(g, params, round_bf16: bool = True):
-    """params: list of (W [out x in], b [out]) f64 tensors in WarmStartNet.layers() order."""
-    rb = round_bf16
+class _DeviceLinear(torch.autograd.Function):
+    """y = round(x) round(W)^T + b whose backward rounds the incoming
+    gradient dy to bf16 where the device does (tangle_b200/warmstart.py
+    Linear.backward: the weight gradient dy_bf16^T x_bf16 and the input
+    gradient dy_bf16 W_bf16 take the rounded dy, the bias gradient the f32
+    dy), with f64 arithmetic everywhere else."""
+
+    @staticmethod
+    def forward(ctx, x, w, b):
+        xr, wr = _bf16(x, True), _bf16(w, True)
+        ctx.save_for_backward(xr, wr)
+        return xr @ wr.T + b
+
+    @staticmethod
+    def backward(ctx, dy):
+        xr, wr = ctx.saved_tensors
+        dyr = _bf16(dy, True)
+        return dyr @ wr, dyr.T @ xr, dy.sum(0)
+
+
+def forward(g, params, round_bf16: bool = True, round_gradients: bool = False):
+    """params: list of (W [out x in], b [out]) f64 tensors in WarmStartNet.layers() order.
+    With `round_gradients` (implies round_bf16), every layer's backward also
+    rounds its incoming gradient to bf16 as the device does (_DeviceLinear)."""
+    rb = round_bf16 or round_gradients
     V, E = g["V"], g["E"]
     it = iter(params)
 
     def lin(x, relu):
         w, b = next(it)
-        y = _bf16(x, rb) @ _bf16(w, rb).T + b
+        y = _DeviceLinear.apply(x, w, b) if round_gradients else _bf16(x, rb) @ _bf16(w, rb).T + b
         return torch.relu(y) if relu else y
 
     a1 = _bf16(lin(g["node_features"], True), rb)
@@ -79,13 +102,13 @@ def forward(g, params, round_bf16: bool = True):
     return lin(d1, False)
 
 
-def loss_and_gradients(g, params_np, target, round_bf16: bool = True):
+def loss_and_gradients(g, params_np, target, round_bf16: bool = True, round_gradients: bool = False):
     """MSE of the first 3 outputs against target [V x 3]; returns
     (loss, output, [(dW, db)] as numpy) in f64."""
     params = [(torch.tensor(w, dtype=torch.float64, requires_grad=True),
                torch.tensor(b, dtype=torch.float64, requires_grad=True)) for w, b in params_np]
-    y = forward(g, params, round_bf16)
+    y = forward(g, params, round_bf16, round_gradients)
     tgt = torch.as_tensor(np.asarray(target), dtype=torch.float64)
     loss = ((y[:, :3] - tgt) ** 2).mean()
     loss.backward()
-    return float(loss), y.detach().numpy(), [(w.grad.numpy(), b.grad.numpy()) for w, b in params]
+    return float(loss.detach()), y.detach().numpy(), [(w.grad.numpy(), b.grad.numpy()) for w, b in params]

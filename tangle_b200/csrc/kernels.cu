@@ -1569,59 +1569,72 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             }
             __syncwarp();
             // find/apply_internal_corrections x constraint_iterations (Jacobi).
+            // Every edge's magnitude -- 0.5 k (length - rest) / length, the
+            // same for both endpoints, whose differences are exact negatives
+            // with equal squares -- is computed once, by the edge's lower
+            // vertex, and handed to the upper one by a shuffle (across a
+            // 32-vertex chunk boundary through the carries). A NaN stands for
+            // an edge shorter than 1e-7, whose term both endpoints skip. Each
+            // vertex still forms its own differences and adds its terms in
+            // the reference's order (i-1, i+1, i-2, i+2).
             for (uint32_t pass = 0; pass < sp.constraint_iterations; ++pass) {
                 float cxs[LANES_KMAX], cys[LANES_KMAX], czs[LANES_KMAX];
+                const float skip = __int_as_float(0x7fffffff);
+                float carry_s = skip, carry_b0 = skip, carry_b1 = skip;
 #pragma unroll
                 for (int k = 0; k < LANES_KMAX; ++k) {
+                    cxs[k] = 0.0f;
+                    cys[k] = 0.0f;
+                    czs[k] = 0.0f;
+                    if (32 * k >= n) continue;  // warp-uniform
                     const int i = lane + 32 * k;
+                    const float4 x = i < n ? P[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    float ms = skip, mb = skip;  // edges (i, i+1) and (i, i+2)
+                    if (i + 1 < n) {
+                        const float4 o = P[i + 1];
+                        const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
+                        const float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                        if (length > 1.0e-7f) ms = 0.5f * sp.stretch_stiffness * (length - w.rest[s0 + i]) / length;
+                    }
+                    if (i + 2 < n) {
+                        const float4 o = P[i + 2];
+                        const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
+                        const float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                        if (length > 1.0e-7f) mb = 0.5f * sp.bend_stiffness * (length - w.vtx_static[v0 + i].z) / length;
+                    }
+                    float ms_back = __shfl_up_sync(FULL, ms, 1);
+                    float mb_back = __shfl_up_sync(FULL, mb, 2);
+                    if (lane == 0) ms_back = carry_s;
+                    if (lane == 0) mb_back = carry_b0;
+                    if (lane == 1) mb_back = carry_b1;
+                    carry_s = __shfl_sync(FULL, ms, 31);
+                    carry_b0 = __shfl_sync(FULL, mb, 30);
+                    carry_b1 = __shfl_sync(FULL, mb, 31);
                     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-                    if (i < n) {
-                        const float4 x = P[i];
-                        if (!lanes_pinned(x)) {
-                            if (i > 0) {
-                                float4 o = P[i - 1];
-                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
-                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
-                                if (length > 1.0e-7f) {
-                                    float magnitude = 0.5f * sp.stretch_stiffness * (length - w.rest[s0 + i - 1]) / length;
-                                    cx += dx * magnitude;
-                                    cy += dy * magnitude;
-                                    cz += dz * magnitude;
-                                }
-                            }
-                            if (i + 1 < n) {
-                                float4 o = P[i + 1];
-                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
-                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
-                                if (length > 1.0e-7f) {
-                                    float magnitude = 0.5f * sp.stretch_stiffness * (length - w.rest[s0 + i]) / length;
-                                    cx += dx * magnitude;
-                                    cy += dy * magnitude;
-                                    cz += dz * magnitude;
-                                }
-                            }
-                            if (i > 1) {
-                                float4 o = P[i - 2];
-                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
-                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
-                                if (length > 1.0e-7f) {
-                                    float magnitude = 0.5f * sp.bend_stiffness * (length - w.vtx_static[v0 + i].y) / length;
-                                    cx += dx * magnitude;
-                                    cy += dy * magnitude;
-                                    cz += dz * magnitude;
-                                }
-                            }
-                            if (i + 2 < n) {
-                                float4 o = P[i + 2];
-                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
-                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
-                                if (length > 1.0e-7f) {
-                                    float magnitude = 0.5f * sp.bend_stiffness * (length - w.vtx_static[v0 + i].z) / length;
-                                    cx += dx * magnitude;
-                                    cy += dy * magnitude;
-                                    cz += dz * magnitude;
-                                }
-                            }
+                    if (i < n && !lanes_pinned(x)) {
+                        if (i > 0 && ms_back == ms_back) {
+                            const float4 o = P[i - 1];
+                            cx += (o.x - x.x) * ms_back;
+                            cy += (o.y - x.y) * ms_back;
+                            cz += (o.z - x.z) * ms_back;
+                        }
+                        if (i + 1 < n && ms == ms) {
+                            const float4 o = P[i + 1];
+                            cx += (o.x - x.x) * ms;
+                            cy += (o.y - x.y) * ms;
+                            cz += (o.z - x.z) * ms;
+                        }
+                        if (i > 1 && mb_back == mb_back) {
+                            const float4 o = P[i - 2];
+                            cx += (o.x - x.x) * mb_back;
+                            cy += (o.y - x.y) * mb_back;
+                            cz += (o.z - x.z) * mb_back;
+                        }
+                        if (i + 2 < n && mb == mb) {
+                            const float4 o = P[i + 2];
+                            cx += (o.x - x.x) * mb;
+                            cy += (o.y - x.y) * mb;
+                            cz += (o.z - x.z) * mb;
                         }
                     }
                     cxs[k] = cx;
@@ -1753,8 +1766,21 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             const float radius = w.seg_static[s0].x;
             float4 *P = lanes_smem + (size_t)j * stride;
             if (FM) formation_targets_staged(w, f, P, n, v0, lane);
-            for (int i = lane; i < n; i += 32) {
-                const float4 x = P[i];
+            // Each edge's length, |P[i+1] - P[i]|, is taken once: it is the
+            // segment's geometry record (half of it), vertex i's second
+            // length and, through a shuffle, vertex i+1's first length of
+            // the curvature ratio -- the same expression in each place.
+            float carry_length = 0.0f;
+            for (int base = 0; base < n; base += 32) {  // warp-uniform
+                const int i = base + lane;
+                const float4 x = i < n ? P[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                const float4 y = i + 1 < n ? P[i + 1] : x;
+                const float ex = y.x - x.x, ey = y.y - x.y, ez = y.z - x.z;
+                const float length = i + 1 < n ? sqrtf(ex * ex + ey * ey + ez * ez) : 0.0f;
+                float previous_length = __shfl_up_sync(FULL, length, 1);
+                if (lane == 0) previous_length = carry_length;
+                carry_length = __shfl_sync(FULL, length, 31);
+                if (i >= n) continue;
                 w.pos[v0 + i] = make_float4(x.x, x.y, x.z, 0.0f);
                 const float4 r = w.ref_pos[v0 + i];
                 const float dx = x.x - r.x, dy = x.y - r.y, dz = x.z - r.z;
@@ -1763,14 +1789,12 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                 if (i > 0 && i + 1 < n) {
                     const float maximum = lanes_limit(x);
                     if (maximum > 0.0f) {
-                        const float ratio = curvature_ratio_at([&](int k) { return P[k]; }, i, maximum);
+                        const float ratio = curvature_ratio_of(P[i - 1], x, y, previous_length, length, maximum);
                         cmax = max(cmax, __float_as_uint(fmaxf(ratio, 0.0f)));
                     }
                 }
                 if (i + 1 < n) {
-                    const float4 y = P[i + 1];
-                    const float ex = y.x - x.x, ey = y.y - x.y, ez = y.z - x.z;
-                    const float half = 0.5f * sqrtf(ex * ex + ey * ey + ez * ez);
+                    const float half = 0.5f * length;
                     w.geom[2 * (size_t)(s0 + i)] = make_float4(x.x, x.y, x.z, radius);
                     w.geom[2 * (size_t)(s0 + i) + 1] = make_float4(y.x, y.y, y.z, half);
                     if (contact_lists && half > w.contact_half_limit) contact_far = true;
