@@ -1491,6 +1491,110 @@ __device__ inline bool lanes_test(const float4 *P, int t, float stiffness, float
     return tr.pw > 0.0f || tr.cw > 0.0f || tr.nw > 0.0f;
 }
 
+// The two stages of lanes_test, for sweeps that evaluate the exact test
+// cooperatively. Stage one (every lane, its own triplet): the lengths, the
+// limit's cosine and the cheap rejection -- false when the triplet
+// certainly moves nothing. Stage two (lanes_exact_group): the exact test of
+// one candidate triplet of a lane group, its divisions and arc cosines
+// spread over the group's lanes; every lane ends with the candidate's
+// Triplet. Each value is the same expression on the same operands as in
+// lanes_test, so the results are bitwise lanes_test's.
+struct TripletCheap {
+    float ux, uy, uz, vx, vy, vz;
+    float first_length, second_length, minimum_cosine;
+    uint32_t pinned;  // bit 0: previous vertex, 1: centre, 2: next
+};
+
+__device__ inline bool lanes_pretest(const float4 *P, int t, float safety_margin, TripletCheap &c) {
+    const float4 pp = P[t], pc = P[t + 1], pn = P[t + 2];
+    const float maximum_curvature = lanes_limit(pc) * (1.0f - safety_margin);
+    if (!(maximum_curvature > 0.0f)) return false;
+    c.ux = pc.x - pp.x, c.uy = pc.y - pp.y, c.uz = pc.z - pp.z;
+    c.vx = pn.x - pc.x, c.vy = pn.y - pc.y, c.vz = pn.z - pc.z;
+    const float uu = c.ux * c.ux + c.uy * c.uy + c.uz * c.uz;
+    const float vv = c.vx * c.vx + c.vy * c.vy + c.vz * c.vz;
+    c.first_length = sqrtf(uu);
+    c.second_length = sqrtf(vv);
+    if (!(c.first_length > 1.0e-7f && c.second_length > 1.0e-7f)) return false;
+    const float sine_half = 0.25f * maximum_curvature * (c.first_length + c.second_length);
+    if (!(sine_half < 1.0f)) return false;
+    c.minimum_cosine = 1.0f - 2.0f * sine_half * sine_half;
+    if (uu > 1.0e-12f && vv > 1.0e-12f &&
+        (c.ux * c.vx + c.uy * c.vy + c.uz * c.vz) * rsqrtf(uu * vv) > c.minimum_cosine + 1.0e-5f)
+        return false;
+    c.pinned = (lanes_pinned(pp) ? 1u : 0u) | (lanes_pinned(pc) ? 2u : 0u) | (lanes_pinned(pn) ? 4u : 0u);
+    return true;
+}
+
+// Every lane of the warp calls this (it shuffles); `source` is the warp
+// lane holding the group's candidate, `gl` this lane's index in its group
+// of LPF lanes starting at warp lane `group_base`.
+template <int LPF>
+__device__ inline bool lanes_exact_group(const TripletCheap &mine, int source, int group_base, int gl, float stiffness,
+                                         Triplet &tr) {
+    const float ux = __shfl_sync(FULL, mine.ux, source), uy = __shfl_sync(FULL, mine.uy, source);
+    const float uz = __shfl_sync(FULL, mine.uz, source), vx = __shfl_sync(FULL, mine.vx, source);
+    const float vy = __shfl_sync(FULL, mine.vy, source), vz = __shfl_sync(FULL, mine.vz, source);
+    const float first_length = __shfl_sync(FULL, mine.first_length, source);
+    const float second_length = __shfl_sync(FULL, mine.second_length, source);
+    const float minimum_cosine = __shfl_sync(FULL, mine.minimum_cosine, source);
+    const uint32_t pinned = __shfl_sync(FULL, mine.pinned, source);
+    // Unit edge vectors: component m (unx, uny, unz, vnx, vny, vnz) is
+    // divided by lane m % LPF, in its (m / LPF)-th slot.
+    constexpr int SLOTS = (6 + LPF - 1) / LPF;
+    float q[SLOTS];
+#pragma unroll
+    for (int j = 0; j < SLOTS; ++j) {
+        const int m = gl + j * LPF;
+        const float numerator = m == 0 ? ux : m == 1 ? uy : m == 2 ? uz : m == 3 ? vx : m == 4 ? vy : vz;
+        q[j] = m < 6 ? numerator / (m < 3 ? first_length : second_length) : 0.0f;
+    }
+    float un[3], vn[3];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        const float value = __shfl_sync(FULL, q[m / LPF], group_base + m % LPF);
+        if (m < 3) un[m] = value; else vn[m - 3] = value;
+    }
+    const float cosine = clampf(un[0] * vn[0] + un[1] * vn[1] + un[2] * vn[2], -1.0f, 1.0f);
+    float violation = minimum_cosine - cosine;
+    const float sine = sqrtf(fmaxf(1.0f - cosine * cosine, 0.0f));
+    // The two arc cosines on lanes 0 and 1 of the group.
+    const float arc = acos_f32(gl == 0 ? cosine : minimum_cosine);
+    const float arc_cosine = __shfl_sync(FULL, arc, group_base);
+    const float arc_minimum = __shfl_sync(FULL, arc, group_base + 1);
+    if (violation > 0.0f && sine > 1.0e-3f) violation = (arc_cosine - arc_minimum) * sine;
+    // Gradients: component m (gux, guy, guz, gvx, gvy, gvz) on lane m % LPF.
+#pragma unroll
+    for (int j = 0; j < SLOTS; ++j) {
+        const int m = gl + j * LPF;
+        const int a = m < 3 ? m : m - 3;
+        const float una = a == 0 ? un[0] : a == 1 ? un[1] : un[2];
+        const float vna = a == 0 ? vn[0] : a == 1 ? vn[1] : vn[2];
+        q[j] = m < 3 ? (vna - cosine * una) / first_length : m < 6 ? (una - cosine * vna) / second_length : 0.0f;
+    }
+    float gu[3], gv[3];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        const float value = __shfl_sync(FULL, q[m / LPF], group_base + m % LPF);
+        if (m < 3) gu[m] = value; else gv[m - 3] = value;
+    }
+    if (!(violation > 0.0f)) return false;
+    tr.gux = gu[0], tr.guy = gu[1], tr.guz = gu[2];
+    tr.gvx = gv[0], tr.gvy = gv[1], tr.gvz = gv[2];
+    tr.cgx = tr.gux - tr.gvx;
+    tr.cgy = tr.guy - tr.gvy;
+    tr.cgz = tr.guz - tr.gvz;
+    tr.pw = pinned & 1u ? 0.0f : 1.0f;
+    tr.cw = pinned & 2u ? 0.0f : 1.0f;
+    tr.nw = pinned & 4u ? 0.0f : 1.0f;
+    const float denominator = tr.pw * (tr.gux * tr.gux + tr.guy * tr.guy + tr.guz * tr.guz) +
+                              tr.cw * (tr.cgx * tr.cgx + tr.cgy * tr.cgy + tr.cgz * tr.cgz) +
+                              tr.nw * (tr.gvx * tr.gvx + tr.gvy * tr.gvy + tr.gvz * tr.gvz);
+    if (!(denominator > 1.0e-12f)) return false;
+    tr.scale = stiffness * violation / denominator;
+    return tr.pw > 0.0f || tr.cw > 0.0f || tr.nw > 0.0f;
+}
+
 __device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float extent, const Grid &g, float4 *R) {
     const float4 pp = P[t], pc = P[t + 1], pn = P[t + 2];
     float4 a = pp, b = pc, c = pn;
@@ -1717,17 +1821,38 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             bool forward = true, moved = false;
             uint32_t sweep = 0;
             int t0 = 0;
+            // Each round: every lane runs the cheap stage on its triplet;
+            // then each group takes its candidates (triplets the cheap stage
+            // could not clear) in lane order, the group's lanes evaluating
+            // one candidate's exact test together, until one acts. Earlier
+            // candidates that do not act are no-ops in the serial order, so
+            // the first acting one is the serial sweep's next move.
+            const int group_base = LPF == 32 ? 0 : group * LPF;
             while (__any_sync(FULL, !done)) {
-                Triplet tr;
                 const int t = forward ? t0 + gl : t0 - gl;
-                const bool act = !done && (forward ? t <= last : t >= 0) &&
-                                 lanes_test(P, t, sp.curvature_limit_stiffness, sp.curvature_limit_safety_margin, tr);
-                const uint32_t ballot = __ballot_sync(FULL, act);
-                const uint32_t bits = LPF == 32 ? ballot : (ballot >> (group * LPF)) & ((1u << LPF) - 1u);
+                TripletCheap cheap{};  // defined values for groups without a candidate, whose lanes still shuffle
+                const bool candidate = !done && (forward ? t <= last : t >= 0) &&
+                                       lanes_pretest(P, t, sp.curvature_limit_safety_margin, cheap);
+                const uint32_t ballot = __ballot_sync(FULL, candidate);
+                uint32_t pending = LPF == 32 ? ballot : (ballot >> (group * LPF)) & ((1u << LPF) - 1u);
+                int first = -1;
+                while (__any_sync(FULL, pending != 0u)) {
+                    const int c = pending ? __ffs(pending) - 1 : 0;
+                    Triplet tr;
+                    const bool acts = lanes_exact_group<LPF>(cheap, group_base + c, group_base, gl,
+                                                             sp.curvature_limit_stiffness, tr);
+                    if (pending) {
+                        if (acts) {
+                            first = c;
+                            if (gl == 0) lanes_apply(P, forward ? t0 + c : t0 - c, tr, extent, g, R);
+                            pending = 0u;
+                        } else {
+                            pending &= pending - 1u;
+                        }
+                    }
+                }
                 if (!done) {
-                    if (bits) {
-                        const int first = __ffs(bits) - 1;
-                        if (gl == first) lanes_apply(P, t, tr, extent, g, R);
+                    if (first >= 0) {
                         moved = true;
                         t0 = forward ? t0 + first + 1 : t0 - first - 1;
                     } else {
