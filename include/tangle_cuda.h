@@ -517,6 +517,11 @@ typedef struct tgl_mp_graph_out {
  * overlap depth / d, s, t), each padded with zeros to 16. Both wait for
  * completion. */
 int tgl_warmstart_graph_count(tgl_world *world, float cutoff, int64_t *edge_count);
+/* Restricts the next contact graphs to pairs with a segment on a focus fiber
+ * (fiber_focus[f] nonzero; one flag per fiber), as for a ply deposited on a
+ * relaxed stack, whose proposal moves only its own fibers; NULL restores
+ * every pair. Nodes stay every vertex. */
+int tgl_warmstart_set_focus(tgl_world *world, const uint8_t *fiber_focus, size_t fibers);
 int tgl_warmstart_graph_fill(tgl_world *world, const tgl_mp_graph_out *out);
 
 /* Moves every unpinned vertex by scale * dx[v * ld .. v * ld + 2] (device

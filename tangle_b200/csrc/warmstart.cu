@@ -157,7 +157,7 @@ __global__ void graph_count_kernel(WorldDev w, GraphBuffers g, float cutoff) {
                     const uint32_t b = w.nbr_list[(size_t)a * w.block + i0 + lane];
                     float s, t, dist;
                     float3 off;
-                    if (b > a && keep_pair(w, a, b, cutoff, s, t, dist, off)) {
+                    if (b > a && in_focus(w, g, a, b) && keep_pair(w, a, b, cutoff, s, t, dist, off)) {
                         keep = true;
                         atomicAdd(&g.in_count[b], 1u);
                     }
@@ -255,7 +255,7 @@ __global__ void graph_fill_kernel(WorldDev w, GraphBuffers g, float cutoff) {
             float3 off = make_float3(0.0f, 0.0f, 0.0f);
             if (i0 + lane < count) {
                 b = w.nbr_list[(size_t)a * w.block + i0 + lane];
-                keep = b > a && keep_pair(w, a, b, cutoff, s, t, dist, off);
+                keep = b > a && in_focus(w, g, a, b) && keep_pair(w, a, b, cutoff, s, t, dist, off);
             }
             const uint32_t ballot = __ballot_sync(WFULL, keep);
             if (keep) {

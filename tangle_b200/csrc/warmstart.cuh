@@ -40,7 +40,16 @@ struct GraphBuffers {
     __nv_bfloat16 *node_features;            // [V * 16]
     int32_t *block_sums;                     // scan scratch
     int64_t edge_capacity;
+    // Focus fibers (nullptr: all): only pairs with a segment on one of them
+    // become edges (a new ply's contacts on a relaxed stack).
+    const uint32_t *fiber_focus;             // [F] nonzero = in focus
 };
+
+// Whether pair (a, b) may enter the graph under the focus set.
+__device__ inline bool in_focus(const WorldDev &w, const GraphBuffers &g, uint32_t a, uint32_t b) {
+    return g.fiber_focus == nullptr || g.fiber_focus[__float_as_uint(w.seg_static[a].w)] != 0u ||
+           g.fiber_focus[__float_as_uint(w.seg_static[b].w)] != 0u;
+}
 
 // Graph extraction from the world's Verlet lists (built from the current
 // positions): counts, offsets and edge records.

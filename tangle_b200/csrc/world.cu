@@ -104,11 +104,13 @@ struct WarmGraph {
     float *depth = nullptr;      // [depth_capacity]
     int64_t depth_capacity = 0;
     float *residual = nullptr;   // [2]
+    uint32_t *focus = nullptr;   // [F] focus flags (b.fiber_focus points here while a focus is set)
     int64_t edges = 0;
     float cutoff = 0.0f;
     bool ready = false, counted = false;
 
     ~WarmGraph() {
+        cudaFree(focus);
         cudaFree(b.fwd_count);
         cudaFree(b.in_count);
         cudaFree(b.fill);
@@ -1180,6 +1182,25 @@ int tgl_warmstart_graph_count(tgl_world *w, float cutoff, int64_t *edge_count) {
     w->warm.cutoff = cutoff;
     w->warm.counted = true;
     *edge_count = edges;
+    return 0;
+}
+
+int tgl_warmstart_set_focus(tgl_world *w, const uint8_t *fiber_focus, size_t fibers) {
+    if (!w) return set_error(TGL_ERR_INVALID, "null argument");
+    if (w->arena) return set_error(TGL_ERR_UNSUPPORTED, "the warm start takes one specimen");
+    w->warm.counted = false;
+    if (!fiber_focus) {
+        w->warm.b.fiber_focus = nullptr;
+        return 0;
+    }
+    if (fibers != w->dev.F) return set_error(TGL_ERR_INVALID, "one focus flag per fiber");
+    if (!w->warm.focus && cudaMalloc(&w->warm.focus, (size_t)w->dev.F * sizeof(uint32_t)) != cudaSuccess)
+        return set_error(TGL_ERR_MEMORY, "cudaMalloc of the focus flags failed");
+    std::vector<uint32_t> flags(fibers);
+    for (size_t f = 0; f < fibers; ++f) flags[f] = fiber_focus[f] ? 1u : 0u;
+    TGL_CUDA(cudaMemcpyAsync(w->warm.focus, flags.data(), fibers * sizeof(uint32_t), cudaMemcpyHostToDevice, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    w->warm.b.fiber_focus = w->warm.focus;
     return 0;
 }
 

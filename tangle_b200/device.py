@@ -46,7 +46,7 @@ EXPORTS = (
     "tgl_world_vertex_target_state", "tgl_world_target_errors", "tgl_world_compact_cell", "tgl_world_cell_bounds",
     "tgl_world_compaction_metrics", "tgl_world_wall_reactions", "tgl_world_set_wall_reactions",
     "tgl_world_set_fiber_max_curvatures", "tgl_world_get_launch_params", "tgl_world_set_launch_params",
-    "tgl_autotune",
+    "tgl_autotune", "tgl_warmstart_set_focus",
     "tgl_last_error",
 )
 

@@ -97,6 +97,7 @@ def _lib():
             "tgl_convert_bf16": [I64, P, P, P],
             "tgl_warmstart_graph_count": [P, F, ctypes.POINTER(I64)],
             "tgl_warmstart_graph_fill": [P, ctypes.POINTER(_MpGraphOut)],
+            "tgl_warmstart_set_focus": [P, P, ctypes.c_size_t],
             "tgl_world_displace": [P, P, I64, F, I32, F],
             "tgl_world_residual": [P, P, ctypes.POINTER(F), ctypes.POINTER(F), ctypes.POINTER(F)],
         }
@@ -172,17 +173,27 @@ class ContactGraph:
         self.edge_features = torch.empty(max(E, 1), EDGE_FEATURES, dtype=bf, device=device)
 
     @classmethod
-    def from_world(cls, world: DeviceWorld, cutoff: float) -> "ContactGraph":
-        """tgl_warmstart_graph_count / _fill on the world's current positions."""
+    def from_world(cls, world: DeviceWorld, cutoff: float, focus=None) -> "ContactGraph":
+        """tgl_warmstart_graph_count / _fill on the world's current positions.
+        With `focus` (fiber indices), only pairs with a segment on one of
+        those fibers become edges (tgl_warmstart_set_focus)."""
         import torch
 
         lib = _lib()
-        edges = ctypes.c_int64()
-        _check(lib.tgl_warmstart_graph_count(world._handle, ctypes.c_float(cutoff), ctypes.byref(edges)))
-        g = cls(world.vertex_count, world.segment_count, int(edges.value), torch.device("cuda"))
-        out = _MpGraphOut(_p(g.seg_v0), _p(g.links), _p(g.offsets), _p(g.dst), _p(g.src), _p(g.twin), _p(g.s),
-                          _p(g.t), _p(g.node_features), _p(g.edge_features))
-        _check(lib.tgl_warmstart_graph_fill(world._handle, ctypes.byref(out)))
+        if focus is not None:
+            flags = np.zeros(world.packed().fiber_count, dtype=np.uint8)
+            flags[np.asarray(focus, dtype=np.int64)] = 1
+            _check(lib.tgl_warmstart_set_focus(world._handle, flags.ctypes.data_as(ctypes.c_void_p), flags.size))
+        try:
+            edges = ctypes.c_int64()
+            _check(lib.tgl_warmstart_graph_count(world._handle, ctypes.c_float(cutoff), ctypes.byref(edges)))
+            g = cls(world.vertex_count, world.segment_count, int(edges.value), torch.device("cuda"))
+            out = _MpGraphOut(_p(g.seg_v0), _p(g.links), _p(g.offsets), _p(g.dst), _p(g.src), _p(g.twin), _p(g.s),
+                              _p(g.t), _p(g.node_features), _p(g.edge_features))
+            _check(lib.tgl_warmstart_graph_fill(world._handle, ctypes.byref(out)))
+        finally:
+            if focus is not None:
+                _check(lib.tgl_warmstart_set_focus(world._handle, None, 0))
         return g
 
     def struct(self) -> _MpGraph:
@@ -505,7 +516,9 @@ def warm_start(world: DeviceWorld, net: WarmStartNet, config: RelaxationConfig, 
     t0 = time.perf_counter()
     pen0, curv0, total0 = residual(world, config)
     saved = world.download_positions()
-    graph = ContactGraph.from_world(world, graph_cutoff(world))
+    # Only the moving fibers' contacts can carry their proposal: with
+    # `fibers`, the graph holds the pairs that touch one of them.
+    graph = ContactGraph.from_world(world, graph_cutoff(world), focus=fibers)
     y = net.forward(graph)
     if fibers is not None:
         spans = np.asarray(world.packed().fiber_vertex_spans, dtype=np.int64).reshape(-1, 2)

@@ -97,6 +97,38 @@ def test_contact_graph_is_symmetric_sorted_and_complete(cuda_lib):
     assert np.all(np.isclose(nf[:, 5], 0.7, atol=1e-2) | np.isclose(nf[:, 5], 1.9, atol=1e-2))
 
 
+def test_focused_graph_keeps_exactly_the_pairs_touching_the_focus(cuda_lib):
+    """A graph restricted to focus fibers (a new ply's warm start) holds
+    exactly the full graph's edges with an endpoint segment on a focus
+    fiber, with the same closest-point parameters and edge features; the
+    next unrestricted graph is the full one again."""
+    from tangle_b200.warmstart import ContactGraph, graph_cutoff
+
+    world, config, packed = small_world(seed=9)
+    world.run_batch(RelaxationConfig(**{**config.__dict__, "force_full_iterations": True}), 3)
+    cutoff = graph_cutoff(world)
+    full = ContactGraph.from_world(world, cutoff)
+    focus = np.arange(0, packed.fiber_count, 3)
+    part = ContactGraph.from_world(world, cutoff, focus=focus)
+    again = ContactGraph.from_world(world, cutoff)
+    fiber = packed.segment_fibers.astype(np.int64)
+    in_focus = np.zeros(packed.fiber_count, dtype=bool)
+    in_focus[focus] = True
+
+    def records(g):
+        E = g.E
+        dst, src = g.dst[:E].cpu().numpy(), g.src[:E].cpu().numpy()
+        s, t = g.s[:E].cpu().numpy(), g.t[:E].cpu().numpy()
+        feats = g.edge_features[:E].float().cpu().numpy()
+        return {(int(a), int(b)): (float(x), float(y), tuple(f)) for a, b, x, y, f in zip(dst, src, s, t, feats)}
+
+    r_full, r_part = records(full), records(part)
+    expected = {k: v for k, v in r_full.items() if in_focus[fiber[k[0]]] or in_focus[fiber[k[1]]]}
+    assert 0 < len(r_part) < len(r_full)
+    assert r_part == expected
+    assert records(again) == r_full
+
+
 def _params(net):
     return [(layer.w.cpu().numpy().astype(np.float64), layer.b.cpu().numpy().astype(np.float64))
             for layer in net.layers()]
