@@ -123,7 +123,7 @@ inline float acos_f32(float x) {
     return 2.0f * (pio2_hi - (r - pio2_lo));
 }
 
-/* cell_list.rs:88-135 (proxies == 1: the segment midpoint). */
+/* proxy_cell, cell_list.rs:34-79 (proxies == 1: the segment midpoint). */
 inline uint32_t proxy_cell(float px, float py, float pz, float qx, float qy, float qz,
                            const Grid &g) {
     float midpoint_x = 0.5f * (px + qx);
@@ -145,7 +145,7 @@ inline uint32_t proxy_cell(float px, float py, float pz, float qx, float qy, flo
     return (z * g.cy + y) * g.cx + x;
 }
 
-/* cell_list.rs:156-166. */
+/* along_fiber_gap, cell_list.rs:100-112. */
 inline float along_fiber_gap(const float *arc, uint32_t a0, uint32_t a1, uint32_t b0,
                              uint32_t b1) {
     float after = arc[b0] - arc[a1];
@@ -344,7 +344,7 @@ int size_world(orc_world &w, const orc_cell_list_config &cl, float max_step) {
     return 0;
 }
 
-/* Cell-list build: cell_list.rs:63-434, world/cell_list.rs:94-209. A stable
+/* Cell-list build: cell_list.rs:8-378, world/cell_list.rs:94-209. A stable
  * counting sort over ascending segment index gives the ranked order
  * rank_cell_segments produces (ascending segment within each cell). */
 void build_cell_list(orc_world &w) {
@@ -375,7 +375,7 @@ void build_cell_list(orc_world &w) {
     }
 }
 
-/* neighbor.rs:107-408 and world/neighbor_list.rs:19-114: one slot (one
+/* neighbor.rs:109-411 and world/neighbor_list.rs:19-114: one slot (one
  * segment here) at a time; each list sorted ascending by segment. */
 void build_neighbor_lists(orc_world &w) {
     build_cell_list(w);

@@ -17,7 +17,7 @@ namespace tgl {
 
 // Orthorhombic cell and its uniform grid. `length` is upper - lower and
 // `width` is length / cells, both rounded in f32 exactly as proxy_cell
-// computes them (cell_list.rs:116-118).
+// computes them (cell_list.rs:60-62).
 struct Grid {
     float lower[3];
     float upper[3];
@@ -73,7 +73,7 @@ __host__ __device__ inline float acos_f32(float x) {
     return 2.0f * (pio2_hi - (r - pio2_lo));
 }
 
-// cell_list.rs:88-135 for a one-piece segment: the cell of its midpoint.
+// proxy_cell (cell_list.rs:34-79) for a one-piece segment: the cell of its midpoint.
 __device__ inline uint32_t proxy_cell(float px, float py, float pz, float qx, float qy, float qz,
                                       const Grid &g) {
     float mx = 0.5f * (px + qx);

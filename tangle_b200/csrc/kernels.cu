@@ -172,7 +172,7 @@ __global__ void measure_start_kernel(WorldDev w) {
 }
 
 // ---------------------------------------------------------------- cell list
-// cell_list.rs:63-434 / world/cell_list.rs:94-209, gated on the rebuild flag.
+// cell_list.rs:8-378 / world/cell_list.rs:94-209, gated on the rebuild flag.
 
 // (In an arena, only the cells, segments and vertices of specimens whose
 // rebuild is pending are touched: each specimen owns a contiguous cell range
@@ -266,7 +266,7 @@ __global__ void rb_scatter_kernel(WorldDev w) {
             w.cell_segments[w.cell_offsets[w.cell_of[s]] + w.ticket[s]] = s;
 }
 
-// rank_cell_segments (cell_list.rs:392-434): ascending segment order inside
+// rank_cell_segments (cell_list.rs:346-378): ascending segment order inside
 // every cell. One warp per cell; a rank sort in shared memory, or over the
 // global range (into the free ticket array) for very crowded cells.
 template <bool A>
@@ -305,7 +305,7 @@ __global__ void rb_sort_cells_kernel(WorldDev w) {
     }
 }
 
-// gather_cell_slot_geometry (neighbor.rs:107-153): geometry in slot order,
+// gather_cell_slot_geometry (neighbor.rs:109-170): geometry in slot order,
 // plus each slot's bounding sphere (midpoint, half length + radius) for the
 // build's pre-test.
 template <bool A>
@@ -357,7 +357,7 @@ __device__ inline float key_float(int k) { return __int_as_float(k >= 0 ? k : k 
 // Distance along one axis from 0 to the interval [lo, hi].
 __device__ inline float interval_gap(float lo, float hi) { return fmaxf(0.0f, fmaxf(lo, -hi)); }
 
-// build_segment_neighbor_lists (neighbor.rs:155-364). One block per home cell.
+// build_segment_neighbor_lists (neighbor.rs:171-364). One block per home cell.
 // The 27 stencil cells' bounding spheres are staged in shared memory; each
 // warp takes one home segment and tests 32 candidates at a time with a
 // conservative sphere test. A pair the exact test accepts always passes it:
@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
     }
 }
 
-// sort_neighbor_lists (neighbor.rs:366-408): ascending segment order for
+// sort_neighbor_lists (neighbor.rs:373-411): ascending segment order for
 // every list that fits its block; overflowed lists are never read.
 template <bool A>
 __global__ void rb_sort_lists_kernel(WorldDev w) {
@@ -600,7 +600,7 @@ __global__ void rb_sort_lists_kernel(WorldDev w) {
     }
 }
 
-// snapshot_neighbor_reference_positions (neighbor.rs:410-422).
+// snapshot_neighbor_reference_positions (neighbor.rs:412-425).
 template <bool A>
 __global__ void rb_snapshot_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
@@ -608,7 +608,7 @@ __global__ void rb_snapshot_kernel(WorldDev w) {
         if (!A || rebuilding<A>(w, spec_of_vtx<A>(w, v))) w.ref_pos[v] = w.pos[v];
 }
 
-// finish_neighbor_list_rebuild (neighbor.rs:424-432).
+// finish_neighbor_list_rebuild (neighbor.rs:426-435).
 // New Verlet lists (and slots) also call for new contact lists.
 __device__ inline void finish_rebuild(Control *ctl) {
     if (ctl->neighbor_state[0] == 0) return;

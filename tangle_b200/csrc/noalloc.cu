@@ -84,7 +84,7 @@ __device__ inline void segment_records(const NoallocArgs &a, uint32_t s, float4 
     ob = make_float4(qx, qy, qz, 0.5f * sqrtf(dx * dx + dy * dy + dz * dz));
 }
 
-// count_cell_segments with the arrival ticket (cell_list.rs:170-219).
+// count_cell_segments with the arrival ticket (cell_list.rs:116-164).
 __global__ void noalloc_count(NoallocArgs a) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.S; s += gridDim.x * blockDim.x) {
         float4 oa, ob;
@@ -135,7 +135,7 @@ __global__ void noalloc_scatter(NoallocArgs a) {
         a.segments[a.offsets[a.cell_of[s]] + a.ticket[s]] = s;
 }
 
-// rank_cell_segments (cell_list.rs:392-434): ascending segments per cell,
+// rank_cell_segments (cell_list.rs:346-378): ascending segments per cell,
 // ranked over the global slot range into the free ticket array, then copied.
 __global__ void noalloc_rank(NoallocArgs a) {
     const int lane = threadIdx.x & 31;
