@@ -670,7 +670,27 @@ def _main(argv=None) -> int:
     ap.add_argument("--geometry", choices=["mid_size", "ply"], default="mid_size",
                     help="training specimens: mid-size-like cubes, or a ply deposited on a relaxed ply")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--learning-curve", default=None,
+                    help="comma-separated training-set sizes: one network per size, trained on the first that many "
+                         "specimens for --epochs epochs and evaluated on the same held-out specimens; no --out")
     args = ap.parse_args(argv)
+    if args.learning_curve:
+        sizes = sorted({int(x) for x in args.learning_curve.split(",") if x.strip()})
+        t0 = time.perf_counter()
+        samples = generate_samples(max(sizes) + args.held_out, args.iterations, geometry=args.geometry)
+        test_set = samples[max(sizes):]
+        curve = []
+        for size in sizes:
+            t1 = time.perf_counter()
+            net = WarmStartNet(seed=args.seed)
+            history = train(net, samples[:size], args.epochs, args.lr)
+            curve.append({"specimens": size, "adam_steps": size * args.epochs, "held_out": evaluate(net, test_set),
+                          "final_train_loss": history[-1], "train_seconds": time.perf_counter() - t1})
+            print(json.dumps(curve[-1]), flush=True)
+        print(json.dumps({"learning_curve": curve, "held_out_specimens": args.held_out, "epochs": args.epochs,
+                          "parameters": WarmStartNet(seed=args.seed).parameter_count,
+                          "seconds": time.perf_counter() - t0}), flush=True)
+        return 0
     if args.load:
         print(json.dumps(measure_gain(WarmStartNet.load(args.load), args.gain_specimens, args.iterations)),
               flush=True)
