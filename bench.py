@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--no-tta", action="store_true")
     ap.add_argument("--tta-iterations", type=int, default=20000, help="iteration cap of each time-to-admissible run")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--autotune", action="store_true", help="also time the steps with the autotuner's launch shapes")
+    ap.add_argument("--no-autotune", action="store_true", help="skip the autotuner comparison of the batched workload")
     ap.add_argument("--cpu-iterations", type=int, default=40)
     ap.add_argument("--cpu-specimens", type=int, default=16, help="arena specimens the CPU baseline relaxes")
     ap.add_argument("--reference-iterations", type=int, default=4,
@@ -774,6 +776,32 @@ def run_cuda(args):
                   "first_iteration": max(args.warmup, 1) * per_step,
                   "what": "the reference arm's iterations of the same trajectory from the initial specimen, "
                           "timed on the GPU with CUDA events"}
+    # The launch-shape autotuner on this workload: the same steps from the
+    # same state with the default shapes (the timed region above) and with
+    # the tuned ones, each on the production graph with CUDA events.
+    tuned = None
+    if args.autotune or (batched and not args.no_autotune):
+        from tangle_b200.autotune import autotune
+
+        default_params = world.launch_params()
+        world.upload_positions(start_state)
+        choice = autotune(world, fixed, trial_iterations=min(args.iterations, 32), force=True)
+        world.upload_positions(start_state)
+        world.run_batch(fixed, args.iterations)  # captures the tuned graph
+        world.upload_positions(start_state)
+        barrier()
+        done = 0
+        with torch.cuda.stream(stream):
+            start.record(stream)
+        for _ in range(args.steps):
+            done += world.run_batch(fixed, args.iterations).batch_iterations
+        with torch.cuda.stream(stream):
+            end.record(stream)
+        end.synchronize()
+        tuned_value, _, _ = replica_throughput(start.elapsed_time(end) / 1000.0, float(nodes * done), world_size)
+        tuned = {"default_value": value, "tuned_value": tuned_value, "unit": UNIT, "default_params": default_params,
+                 "tuned_params": choice["params"], "search": choice["report"],
+                 "what": "the timed steps again, from the same state, with the autotuner's launch shapes"}
     world.close()
 
     # Time to admissible from the initial specimen, plain PBD and with the
@@ -825,6 +853,7 @@ def run_cuda(args):
             "clocks": clock_summary,
             "e2e": e2e,
             "reference_window": window,
+            "autotune": tuned,
             "time_to_admissible": tta,
             "cpu_baseline": cpu,
         }
