@@ -24,6 +24,8 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 
 namespace tgl {
 
@@ -2148,6 +2150,22 @@ int grid_for(uint64_t n, int threads, int cap) {
 
 }  // namespace
 
+// A kernel's largest dynamic shared memory is a process-wide attribute of
+// the function, shared by every world: raise it when a plan needs more, and
+// never lower it below what another world (or an earlier plan of this one,
+// whose captured graphs may still launch) needs.
+template <typename Kernel>
+static void allow_dynamic_smem(Kernel kernel, size_t bytes) {
+    static std::mutex lock;
+    static std::map<const void *, size_t> granted;
+    const void *key = reinterpret_cast<const void *>(kernel);
+    std::lock_guard<std::mutex> guard(lock);
+    size_t &current = granted[key];
+    if (bytes <= current) return;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess)
+        current = bytes;
+}
+
 void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     int device = 0;
     cudaGetDevice(&device);
@@ -2201,12 +2219,10 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     while (sw > 1 && (size_t)sw * w.block * 4 > 96 * 1024) sw >>= 1;
     lp.sort_warps = sw;
     lp.sort_smem = (size_t)sw * w.block * 4;
-    cudaFuncSetAttribute(fiber_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(lp.fiber_smem, 1));
+    allow_dynamic_smem(fiber_kernel, std::max<size_t>(lp.fiber_smem, 1));
     if (lp.fiber_lanes) {
-        const int smem = (int)lp.lanes_smem;
-        const auto allow = [smem](auto kernel) {
-            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        };
+        const size_t smem = lp.lanes_smem;
+        const auto allow = [smem](auto kernel) { allow_dynamic_smem(kernel, smem); };
         allow(fiber_lanes_kernel<2, false, false>);
         allow(fiber_lanes_kernel<4, false, false>);
         allow(fiber_lanes_kernel<8, false, false>);
@@ -2220,12 +2236,10 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
         allow(fiber_lanes_kernel<8, false, true>);
         allow(fiber_lanes_kernel<32, false, true>);
     }
-    cudaFuncSetAttribute(rb_build_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.build_smem);
-    cudaFuncSetAttribute(rb_build_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp.build_smem);
-    cudaFuncSetAttribute(rb_sort_lists_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)std::max<size_t>(lp.sort_smem, 1));
-    cudaFuncSetAttribute(rb_sort_lists_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)std::max<size_t>(lp.sort_smem, 1));
+    allow_dynamic_smem(rb_build_kernel<false>, lp.build_smem);
+    allow_dynamic_smem(rb_build_kernel<true>, lp.build_smem);
+    allow_dynamic_smem(rb_sort_lists_kernel<false>, std::max<size_t>(lp.sort_smem, 1));
+    allow_dynamic_smem(rb_sort_lists_kernel<true>, std::max<size_t>(lp.sort_smem, 1));
 }
 
 int launch_begin_batch(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
