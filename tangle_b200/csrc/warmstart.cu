@@ -4,8 +4,15 @@
 
 #include <string>
 
+#include <cuda.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <mutex>
+
 #include "../../include/tangle_cuda.h"
 #include "umma_gemm.cuh"
+#include "umma_gemm_tma.cuh"
 
 namespace tgl {
 void set_last_error(const std::string &message);
@@ -16,6 +23,73 @@ namespace {
 int gemm_error(int code, const std::string &message) {
     tgl::set_last_error(message);
     return code;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry points (the
+// library does not link libcuda itself); null when the driver lacks it.
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_tiled() {
+    static std::once_flag once;
+    static EncodeTiled fn = nullptr;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    });
+    return fn;
+}
+
+// A K-major bf16 operand of `rows` rows and `k` columns (leading dimension
+// `ld` elements) as a 2-D tensor map with boxes of 8 contraction elements by
+// `box_rows` rows: each box is one k-group of the canonical no-swizzle
+// layout. Out-of-range elements read as zero.
+bool kmajor_map(CUtensorMap *map, const void *base, int64_t rows, int64_t k, int64_t ld, int box_rows) {
+    EncodeTiled encode = encode_tiled();
+    if (!encode) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2u};
+    const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+    const cuuint32_t element_strides[2] = {1u, 1u};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
+                  element_strides, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The persistent TMA kernel for products whose operands are both K-major and
+// whose contraction is not split; 0 when it ran, 1 when this product or the
+// driver calls for the staged kernel instead, or an error code.
+int gemm_tma(const tgl_gemm *p, const tgl::GemmArgs &g, cudaStream_t stream) {
+    if (p->a_mn || p->b_mn || p->k_split > 0 || p->k <= 0 || std::getenv("TGL_GEMM_STAGED")) return 1;
+    if (p->m > 0x7FFFFF80 || p->k > 0x7FFFFFF0) return 1;  // TMA coordinates are 32-bit
+    CUtensorMap map_a, map_b;
+    if (!kmajor_map(&map_a, p->a, p->m, p->k, p->lda, tgl::GEMM_BM) ||
+        !kmajor_map(&map_b, p->b, p->n, p->k, p->ldb, p->n))
+        return 1;
+    const size_t smem = (size_t)tgl::TMA_GEMM_STAGES * tgl::tma_stage_bytes(p->n);
+    static std::once_flag once;
+    static int sms = 0;
+    std::call_once(once, [] {
+        int device = 0;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        cudaFuncSetAttribute(tgl::umma_gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)((size_t)tgl::TMA_GEMM_STAGES * tgl::tma_stage_bytes(256)));
+    });
+    int cols = 32;
+    while (cols < p->n) cols <<= 1;
+    const int by_smem = (int)((220u * 1024u) / smem), by_tmem = 512 / (2 * cols);
+    const int per_sm = std::max(1, std::min(by_smem, by_tmem));
+    const int64_t tiles = ((int64_t)p->m + tgl::GEMM_BM - 1) / tgl::GEMM_BM;
+    const int blocks = (int)std::min<int64_t>(tiles, (int64_t)std::max(sms, 1) * per_sm);
+    tgl::umma_gemm_tma_kernel<<<blocks, tgl::TMA_GEMM_THREADS, smem, stream>>>(map_a, map_b, g);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return gemm_error(TGL_ERR_CUDA, std::string("tgl_gemm_bf16: ") + cudaGetErrorString(e));
+    return 0;
 }
 
 }  // namespace
@@ -68,6 +142,10 @@ extern "C" int tgl_gemm_bf16(const tgl_gemm *p, void *stream) {
     g.error = p->error;
     const int64_t splits = p->k > 0 ? (p->k + k_split - 1) / k_split : 1;
     if (splits > 65535) return gemm_error(TGL_ERR_UNSUPPORTED, "tgl_gemm_bf16: too many K splits");
+    if (splits == 1) {
+        const int rc = gemm_tma(p, g, static_cast<cudaStream_t>(stream));
+        if (rc != 1) return rc;
+    }
     const size_t smem = (size_t)tgl::GEMM_BM * tgl::GEMM_KC * 2 + (size_t)p->n * tgl::GEMM_KC * 2;
     static bool configured = false;
     if (!configured) {

@@ -134,3 +134,23 @@ def test_mask_and_residual_epilogue(cuda_lib):
     ref = (a.float() @ b.float().T) * (mask.float() > 0) + res
     scale = (a.float().abs() @ b.float().abs().T) + res.abs()
     assert bool(((out - ref).abs() <= 1.0e-5 * scale + 1e-30).all())
+
+
+@pytest.mark.parametrize("m,n,k", [(40000, 64, 1024), (20000, 256, 200), (70001, 16, 8)])
+def test_persistent_kernel_wraps_its_stages_and_accumulators(m, n, k, cuda_lib, monkeypatch):
+    """K-major products take the persistent TMA kernel: more 128-row tiles
+    than CTAs (each CTA alternates its two accumulators) and contractions of
+    many 64-wide chunks (the four pipeline stages wrap around). Against the
+    f32 reference, and equal to the staged kernel (the same tensor-core
+    products summed in the same chunk order)."""
+    import torch
+
+    g = torch.Generator(device="cuda").manual_seed(m + n + k)
+    a = torch.randn(m, k, device="cuda", generator=g).to(torch.bfloat16)
+    b = torch.randn(n, k, device="cuda", generator=g).to(torch.bfloat16)
+    bias = torch.randn(n, device="cuda", generator=g)
+    got, got_bf16 = run(cuda_lib, torch, a, b, m, n, k, 0, 0, bias=bias, relu=True, want_bf16=True)
+    check(torch, got, a, b, bias, relu=True)
+    monkeypatch.setenv("TGL_GEMM_STAGED", "1")
+    staged, staged_bf16 = run(cuda_lib, torch, a, b, m, n, k, 0, 0, bias=bias, relu=True, want_bf16=True)
+    assert torch.equal(got, staged) and torch.equal(got_bf16, staged_bf16)
