@@ -1493,110 +1493,6 @@ __device__ inline bool lanes_test(const float4 *P, int t, float stiffness, float
     return tr.pw > 0.0f || tr.cw > 0.0f || tr.nw > 0.0f;
 }
 
-// The two stages of lanes_test, for sweeps that evaluate the exact test
-// cooperatively. Stage one (every lane, its own triplet): the lengths, the
-// limit's cosine and the cheap rejection -- false when the triplet
-// certainly moves nothing. Stage two (lanes_exact_group): the exact test of
-// one candidate triplet of a lane group, its divisions and arc cosines
-// spread over the group's lanes; every lane ends with the candidate's
-// Triplet. Each value is the same expression on the same operands as in
-// lanes_test, so the results are bitwise lanes_test's.
-struct TripletCheap {
-    float ux, uy, uz, vx, vy, vz;
-    float first_length, second_length, minimum_cosine;
-    uint32_t pinned;  // bit 0: previous vertex, 1: centre, 2: next
-};
-
-__device__ inline bool lanes_pretest(const float4 *P, int t, float safety_margin, TripletCheap &c) {
-    const float4 pp = P[t], pc = P[t + 1], pn = P[t + 2];
-    const float maximum_curvature = lanes_limit(pc) * (1.0f - safety_margin);
-    if (!(maximum_curvature > 0.0f)) return false;
-    c.ux = pc.x - pp.x, c.uy = pc.y - pp.y, c.uz = pc.z - pp.z;
-    c.vx = pn.x - pc.x, c.vy = pn.y - pc.y, c.vz = pn.z - pc.z;
-    const float uu = c.ux * c.ux + c.uy * c.uy + c.uz * c.uz;
-    const float vv = c.vx * c.vx + c.vy * c.vy + c.vz * c.vz;
-    c.first_length = sqrtf(uu);
-    c.second_length = sqrtf(vv);
-    if (!(c.first_length > 1.0e-7f && c.second_length > 1.0e-7f)) return false;
-    const float sine_half = 0.25f * maximum_curvature * (c.first_length + c.second_length);
-    if (!(sine_half < 1.0f)) return false;
-    c.minimum_cosine = 1.0f - 2.0f * sine_half * sine_half;
-    if (uu > 1.0e-12f && vv > 1.0e-12f &&
-        (c.ux * c.vx + c.uy * c.vy + c.uz * c.vz) * rsqrtf(uu * vv) > c.minimum_cosine + 1.0e-5f)
-        return false;
-    c.pinned = (lanes_pinned(pp) ? 1u : 0u) | (lanes_pinned(pc) ? 2u : 0u) | (lanes_pinned(pn) ? 4u : 0u);
-    return true;
-}
-
-// Every lane of the warp calls this (it shuffles); `source` is the warp
-// lane holding the group's candidate, `gl` this lane's index in its group
-// of LPF lanes starting at warp lane `group_base`.
-template <int LPF>
-__device__ inline bool lanes_exact_group(const TripletCheap &mine, int source, int group_base, int gl, float stiffness,
-                                         Triplet &tr) {
-    const float ux = __shfl_sync(FULL, mine.ux, source), uy = __shfl_sync(FULL, mine.uy, source);
-    const float uz = __shfl_sync(FULL, mine.uz, source), vx = __shfl_sync(FULL, mine.vx, source);
-    const float vy = __shfl_sync(FULL, mine.vy, source), vz = __shfl_sync(FULL, mine.vz, source);
-    const float first_length = __shfl_sync(FULL, mine.first_length, source);
-    const float second_length = __shfl_sync(FULL, mine.second_length, source);
-    const float minimum_cosine = __shfl_sync(FULL, mine.minimum_cosine, source);
-    const uint32_t pinned = __shfl_sync(FULL, mine.pinned, source);
-    // Unit edge vectors: component m (unx, uny, unz, vnx, vny, vnz) is
-    // divided by lane m % LPF, in its (m / LPF)-th slot.
-    constexpr int SLOTS = (6 + LPF - 1) / LPF;
-    float q[SLOTS];
-#pragma unroll
-    for (int j = 0; j < SLOTS; ++j) {
-        const int m = gl + j * LPF;
-        const float numerator = m == 0 ? ux : m == 1 ? uy : m == 2 ? uz : m == 3 ? vx : m == 4 ? vy : vz;
-        q[j] = m < 6 ? numerator / (m < 3 ? first_length : second_length) : 0.0f;
-    }
-    float un[3], vn[3];
-#pragma unroll
-    for (int m = 0; m < 6; ++m) {
-        const float value = __shfl_sync(FULL, q[m / LPF], group_base + m % LPF);
-        if (m < 3) un[m] = value; else vn[m - 3] = value;
-    }
-    const float cosine = clampf(un[0] * vn[0] + un[1] * vn[1] + un[2] * vn[2], -1.0f, 1.0f);
-    float violation = minimum_cosine - cosine;
-    const float sine = sqrtf(fmaxf(1.0f - cosine * cosine, 0.0f));
-    // The two arc cosines on lanes 0 and 1 of the group.
-    const float arc = acos_f32(gl == 0 ? cosine : minimum_cosine);
-    const float arc_cosine = __shfl_sync(FULL, arc, group_base);
-    const float arc_minimum = __shfl_sync(FULL, arc, group_base + 1);
-    if (violation > 0.0f && sine > 1.0e-3f) violation = (arc_cosine - arc_minimum) * sine;
-    // Gradients: component m (gux, guy, guz, gvx, gvy, gvz) on lane m % LPF.
-#pragma unroll
-    for (int j = 0; j < SLOTS; ++j) {
-        const int m = gl + j * LPF;
-        const int a = m < 3 ? m : m - 3;
-        const float una = a == 0 ? un[0] : a == 1 ? un[1] : un[2];
-        const float vna = a == 0 ? vn[0] : a == 1 ? vn[1] : vn[2];
-        q[j] = m < 3 ? (vna - cosine * una) / first_length : m < 6 ? (una - cosine * vna) / second_length : 0.0f;
-    }
-    float gu[3], gv[3];
-#pragma unroll
-    for (int m = 0; m < 6; ++m) {
-        const float value = __shfl_sync(FULL, q[m / LPF], group_base + m % LPF);
-        if (m < 3) gu[m] = value; else gv[m - 3] = value;
-    }
-    if (!(violation > 0.0f)) return false;
-    tr.gux = gu[0], tr.guy = gu[1], tr.guz = gu[2];
-    tr.gvx = gv[0], tr.gvy = gv[1], tr.gvz = gv[2];
-    tr.cgx = tr.gux - tr.gvx;
-    tr.cgy = tr.guy - tr.gvy;
-    tr.cgz = tr.guz - tr.gvz;
-    tr.pw = pinned & 1u ? 0.0f : 1.0f;
-    tr.cw = pinned & 2u ? 0.0f : 1.0f;
-    tr.nw = pinned & 4u ? 0.0f : 1.0f;
-    const float denominator = tr.pw * (tr.gux * tr.gux + tr.guy * tr.guy + tr.guz * tr.guz) +
-                              tr.cw * (tr.cgx * tr.cgx + tr.cgy * tr.cgy + tr.cgz * tr.cgz) +
-                              tr.nw * (tr.gvx * tr.gvx + tr.gvy * tr.gvy + tr.gvz * tr.gvz);
-    if (!(denominator > 1.0e-12f)) return false;
-    tr.scale = stiffness * violation / denominator;
-    return tr.pw > 0.0f || tr.cw > 0.0f || tr.nw > 0.0f;
-}
-
 __device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float extent, const Grid &g, float4 *R) {
     const float4 pp = P[t], pc = P[t + 1], pn = P[t + 2];
     float4 a = pp, b = pc, c = pn;
@@ -1675,72 +1571,59 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             }
             __syncwarp();
             // find/apply_internal_corrections x constraint_iterations (Jacobi).
-            // Every edge's magnitude -- 0.5 k (length - rest) / length, the
-            // same for both endpoints, whose differences are exact negatives
-            // with equal squares -- is computed once, by the edge's lower
-            // vertex, and handed to the upper one by a shuffle (across a
-            // 32-vertex chunk boundary through the carries). A NaN stands for
-            // an edge shorter than 1e-7, whose term both endpoints skip. Each
-            // vertex still forms its own differences and adds its terms in
-            // the reference's order (i-1, i+1, i-2, i+2).
             for (uint32_t pass = 0; pass < sp.constraint_iterations; ++pass) {
                 float cxs[LANES_KMAX], cys[LANES_KMAX], czs[LANES_KMAX];
-                const float skip = __int_as_float(0x7fffffff);
-                float carry_s = skip, carry_b0 = skip, carry_b1 = skip;
 #pragma unroll
                 for (int k = 0; k < LANES_KMAX; ++k) {
-                    cxs[k] = 0.0f;
-                    cys[k] = 0.0f;
-                    czs[k] = 0.0f;
-                    if (32 * k >= n) continue;  // warp-uniform
                     const int i = lane + 32 * k;
-                    const float4 x = i < n ? P[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                    float ms = skip, mb = skip;  // edges (i, i+1) and (i, i+2)
-                    if (i + 1 < n) {
-                        const float4 o = P[i + 1];
-                        const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
-                        const float length = sqrtf(dx * dx + dy * dy + dz * dz);
-                        if (length > 1.0e-7f) ms = 0.5f * sp.stretch_stiffness * (length - w.rest[s0 + i]) / length;
-                    }
-                    if (i + 2 < n) {
-                        const float4 o = P[i + 2];
-                        const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
-                        const float length = sqrtf(dx * dx + dy * dy + dz * dz);
-                        if (length > 1.0e-7f) mb = 0.5f * sp.bend_stiffness * (length - w.vtx_static[v0 + i].z) / length;
-                    }
-                    float ms_back = __shfl_up_sync(FULL, ms, 1);
-                    float mb_back = __shfl_up_sync(FULL, mb, 2);
-                    if (lane == 0) ms_back = carry_s;
-                    if (lane == 0) mb_back = carry_b0;
-                    if (lane == 1) mb_back = carry_b1;
-                    carry_s = __shfl_sync(FULL, ms, 31);
-                    carry_b0 = __shfl_sync(FULL, mb, 30);
-                    carry_b1 = __shfl_sync(FULL, mb, 31);
                     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-                    if (i < n && !lanes_pinned(x)) {
-                        if (i > 0 && ms_back == ms_back) {
-                            const float4 o = P[i - 1];
-                            cx += (o.x - x.x) * ms_back;
-                            cy += (o.y - x.y) * ms_back;
-                            cz += (o.z - x.z) * ms_back;
-                        }
-                        if (i + 1 < n && ms == ms) {
-                            const float4 o = P[i + 1];
-                            cx += (o.x - x.x) * ms;
-                            cy += (o.y - x.y) * ms;
-                            cz += (o.z - x.z) * ms;
-                        }
-                        if (i > 1 && mb_back == mb_back) {
-                            const float4 o = P[i - 2];
-                            cx += (o.x - x.x) * mb_back;
-                            cy += (o.y - x.y) * mb_back;
-                            cz += (o.z - x.z) * mb_back;
-                        }
-                        if (i + 2 < n && mb == mb) {
-                            const float4 o = P[i + 2];
-                            cx += (o.x - x.x) * mb;
-                            cy += (o.y - x.y) * mb;
-                            cz += (o.z - x.z) * mb;
+                    if (i < n) {
+                        const float4 x = P[i];
+                        if (!lanes_pinned(x)) {
+                            if (i > 0) {
+                                float4 o = P[i - 1];
+                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                                if (length > 1.0e-7f) {
+                                    float magnitude = 0.5f * sp.stretch_stiffness * (length - w.rest[s0 + i - 1]) / length;
+                                    cx += dx * magnitude;
+                                    cy += dy * magnitude;
+                                    cz += dz * magnitude;
+                                }
+                            }
+                            if (i + 1 < n) {
+                                float4 o = P[i + 1];
+                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                                if (length > 1.0e-7f) {
+                                    float magnitude = 0.5f * sp.stretch_stiffness * (length - w.rest[s0 + i]) / length;
+                                    cx += dx * magnitude;
+                                    cy += dy * magnitude;
+                                    cz += dz * magnitude;
+                                }
+                            }
+                            if (i > 1) {
+                                float4 o = P[i - 2];
+                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                                if (length > 1.0e-7f) {
+                                    float magnitude = 0.5f * sp.bend_stiffness * (length - w.vtx_static[v0 + i].y) / length;
+                                    cx += dx * magnitude;
+                                    cy += dy * magnitude;
+                                    cz += dz * magnitude;
+                                }
+                            }
+                            if (i + 2 < n) {
+                                float4 o = P[i + 2];
+                                float dx = o.x - x.x, dy = o.y - x.y, dz = o.z - x.z;
+                                float length = sqrtf(dx * dx + dy * dy + dz * dz);
+                                if (length > 1.0e-7f) {
+                                    float magnitude = 0.5f * sp.bend_stiffness * (length - w.vtx_static[v0 + i].z) / length;
+                                    cx += dx * magnitude;
+                                    cy += dy * magnitude;
+                                    cz += dz * magnitude;
+                                }
+                            }
                         }
                     }
                     cxs[k] = cx;
@@ -1823,38 +1706,17 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             bool forward = true, moved = false;
             uint32_t sweep = 0;
             int t0 = 0;
-            // Each round: every lane runs the cheap stage on its triplet;
-            // then each group takes its candidates (triplets the cheap stage
-            // could not clear) in lane order, the group's lanes evaluating
-            // one candidate's exact test together, until one acts. Earlier
-            // candidates that do not act are no-ops in the serial order, so
-            // the first acting one is the serial sweep's next move.
-            const int group_base = LPF == 32 ? 0 : group * LPF;
             while (__any_sync(FULL, !done)) {
+                Triplet tr;
                 const int t = forward ? t0 + gl : t0 - gl;
-                TripletCheap cheap{};  // defined values for groups without a candidate, whose lanes still shuffle
-                const bool candidate = !done && (forward ? t <= last : t >= 0) &&
-                                       lanes_pretest(P, t, sp.curvature_limit_safety_margin, cheap);
-                const uint32_t ballot = __ballot_sync(FULL, candidate);
-                uint32_t pending = LPF == 32 ? ballot : (ballot >> (group * LPF)) & ((1u << LPF) - 1u);
-                int first = -1;
-                while (__any_sync(FULL, pending != 0u)) {
-                    const int c = pending ? __ffs(pending) - 1 : 0;
-                    Triplet tr;
-                    const bool acts = lanes_exact_group<LPF>(cheap, group_base + c, group_base, gl,
-                                                             sp.curvature_limit_stiffness, tr);
-                    if (pending) {
-                        if (acts) {
-                            first = c;
-                            if (gl == 0) lanes_apply(P, forward ? t0 + c : t0 - c, tr, extent, g, R);
-                            pending = 0u;
-                        } else {
-                            pending &= pending - 1u;
-                        }
-                    }
-                }
+                const bool act = !done && (forward ? t <= last : t >= 0) &&
+                                 lanes_test(P, t, sp.curvature_limit_stiffness, sp.curvature_limit_safety_margin, tr);
+                const uint32_t ballot = __ballot_sync(FULL, act);
+                const uint32_t bits = LPF == 32 ? ballot : (ballot >> (group * LPF)) & ((1u << LPF) - 1u);
                 if (!done) {
-                    if (first >= 0) {
+                    if (bits) {
+                        const int first = __ffs(bits) - 1;
+                        if (gl == first) lanes_apply(P, t, tr, extent, g, R);
                         moved = true;
                         t0 = forward ? t0 + first + 1 : t0 - first - 1;
                     } else {
@@ -1893,21 +1755,8 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
             const float radius = w.seg_static[s0].x;
             float4 *P = lanes_smem + (size_t)j * stride;
             if (FM) formation_targets_staged(w, f, P, n, v0, lane);
-            // Each edge's length, |P[i+1] - P[i]|, is taken once: it is the
-            // segment's geometry record (half of it), vertex i's second
-            // length and, through a shuffle, vertex i+1's first length of
-            // the curvature ratio -- the same expression in each place.
-            float carry_length = 0.0f;
-            for (int base = 0; base < n; base += 32) {  // warp-uniform
-                const int i = base + lane;
-                const float4 x = i < n ? P[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                const float4 y = i + 1 < n ? P[i + 1] : x;
-                const float ex = y.x - x.x, ey = y.y - x.y, ez = y.z - x.z;
-                const float length = i + 1 < n ? sqrtf(ex * ex + ey * ey + ez * ez) : 0.0f;
-                float previous_length = __shfl_up_sync(FULL, length, 1);
-                if (lane == 0) previous_length = carry_length;
-                carry_length = __shfl_sync(FULL, length, 31);
-                if (i >= n) continue;
+            for (int i = lane; i < n; i += 32) {
+                const float4 x = P[i];
                 w.pos[v0 + i] = make_float4(x.x, x.y, x.z, 0.0f);
                 const float4 r = w.ref_pos[v0 + i];
                 const float dx = x.x - r.x, dy = x.y - r.y, dz = x.z - r.z;
@@ -1916,12 +1765,14 @@ __global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepPar
                 if (i > 0 && i + 1 < n) {
                     const float maximum = lanes_limit(x);
                     if (maximum > 0.0f) {
-                        const float ratio = curvature_ratio_of(P[i - 1], x, y, previous_length, length, maximum);
+                        const float ratio = curvature_ratio_at([&](int k) { return P[k]; }, i, maximum);
                         cmax = max(cmax, __float_as_uint(fmaxf(ratio, 0.0f)));
                     }
                 }
                 if (i + 1 < n) {
-                    const float half = 0.5f * length;
+                    const float4 y = P[i + 1];
+                    const float ex = y.x - x.x, ey = y.y - x.y, ez = y.z - x.z;
+                    const float half = 0.5f * sqrtf(ex * ex + ey * ey + ez * ez);
                     w.geom[2 * (size_t)(s0 + i)] = make_float4(x.x, x.y, x.z, radius);
                     w.geom[2 * (size_t)(s0 + i) + 1] = make_float4(y.x, y.y, y.z, half);
                     if (contact_lists && half > w.contact_half_limit) contact_far = true;

@@ -144,24 +144,6 @@ __device__ inline float curvature_ratio_at(Fetch p, int i, float maximum) {
     return ratio;
 }
 
-// curvature_ratio_at from the three vertices and the two edge lengths
-// already taken (first = |c - a0|, second = |b1 - c|, each the sqrtf of the
-// same sum of squares curvature_ratio_at forms): the same bits.
-__device__ inline float curvature_ratio_of(float4 a0, float4 c, float4 b1, float first_length, float second_length,
-                                           float maximum) {
-    float ax = c.x - a0.x, ay = c.y - a0.y, az = c.z - a0.z;
-    float bx = b1.x - c.x, by = b1.y - c.y, bz = b1.z - c.z;
-    float ratio = 0.0f;
-    if (first_length > 1.0e-7f && second_length > 1.0e-7f) {
-        float cosine = (ax * bx + ay * by + az * bz) / (first_length * second_length);
-        cosine = clampf(cosine, -1.0f, 1.0f);
-        float dual_length = 0.5f * (first_length + second_length);
-        float curvature = 2.0f * sqrtf(0.5f * (1.0f - cosine)) / dual_length;
-        ratio = curvature / maximum;
-    }
-    return ratio;
-}
-
 // Formation launchers (formation.cu).
 // apply_formation_layer_targets once, outside a batch (world.rs:1758-1800).
 void launch_layer_targets_now(const WorldDev &w, cudaStream_t st);
