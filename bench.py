@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--iterations", type=int, default=128, help="relaxation iterations per step")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the mid-size cell (tests only)")
     ap.add_argument("--capacity", type=int, default=256, help="neighbor slots per segment")
+    ap.add_argument("--gemm-scale", type=float, default=1.0,
+                    help="scale the row counts of the gemm workload's network shapes (small profiling cases)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tta", action="store_true")
     ap.add_argument("--tta-iterations", type=int, default=20000, help="iteration cap of each time-to-admissible run")
@@ -906,11 +908,12 @@ def run_gemm(args):
     stream = torch.cuda.current_stream(dev)
     hbm, hbm_kind = measured_peak()
     tensor, tensor_kind = measured_tensor_peak()
+    rows = lambda m: max(128, int(m * args.gemm_scale))
     shapes = [
         # (label, m, n, k): forward products, K-major operands, bf16 output.
-        ("edge MLP layer 1 (E x 80 -> 64)", 16_000_000, 64, 80),
-        ("edge MLP layer 2 (E x 64 -> 64)", 16_000_000, 64, 64),
-        ("node MLP layer 1 (V x 192 -> 64)", 2_000_000, 64, 192),
+        ("edge MLP layer 1 (E x 80 -> 64)", rows(16_000_000), 64, 80),
+        ("edge MLP layer 2 (E x 64 -> 64)", rows(16_000_000), 64, 64),
+        ("node MLP layer 1 (V x 192 -> 64)", rows(2_000_000), 64, 192),
         ("large product (16384 x 8192 -> 256)", 16384, 256, 8192),
     ]
     results = []
