@@ -778,9 +778,11 @@ def run_cuda(args):
                   "first_iteration": max(args.warmup, 1) * per_step,
                   "what": "the reference arm's iterations of the same trajectory from the initial specimen, "
                           "timed on the GPU with CUDA events"}
-    # The launch-shape autotuner on this workload: the same steps from the
-    # same state with the default shapes (the timed region above) and with
-    # the tuned ones, each on the production graph with CUDA events.
+    # The launch-shape autotuner on this workload. After the search, the
+    # default and the tuned shapes each time the same steps from the same
+    # state on the production graph with CUDA events, alternately and twice
+    # each (default, tuned, default, tuned), so that neither gains from
+    # running later; each value is the better of its two.
     tuned = None
     if args.autotune or (batched and not args.no_autotune):
         from tangle_b200.autotune import autotune
@@ -788,22 +790,32 @@ def run_cuda(args):
         default_params = world.launch_params()
         world.upload_positions(start_state)
         choice = autotune(world, fixed, trial_iterations=min(args.iterations, 32), force=True)
-        world.upload_positions(start_state)
-        world.run_batch(fixed, args.iterations)  # captures the tuned graph
-        world.upload_positions(start_state)
-        barrier()
-        done = 0
-        with torch.cuda.stream(stream):
-            start.record(stream)
-        for _ in range(args.steps):
-            done += world.run_batch(fixed, args.iterations).batch_iterations
-        with torch.cuda.stream(stream):
-            end.record(stream)
-        end.synchronize()
-        tuned_value, _, _ = replica_throughput(start.elapsed_time(end) / 1000.0, float(nodes * done), world_size)
-        tuned = {"default_value": value, "tuned_value": tuned_value, "unit": UNIT, "default_params": default_params,
+
+        def time_shapes(params):
+            world.set_launch_params(params)
+            world.upload_positions(start_state)
+            world.run_batch(fixed, args.iterations)  # captures this shape's graph
+            world.upload_positions(start_state)
+            barrier()
+            done = 0
+            with torch.cuda.stream(stream):
+                start.record(stream)
+            for _ in range(args.steps):
+                done += world.run_batch(fixed, args.iterations).batch_iterations
+            with torch.cuda.stream(stream):
+                end.record(stream)
+            end.synchronize()
+            return replica_throughput(start.elapsed_time(end) / 1000.0, float(nodes * done), world_size)[0]
+
+        runs = {"default": [], "tuned": []}
+        for _ in range(2):
+            runs["default"].append(time_shapes(default_params))
+            runs["tuned"].append(time_shapes(choice["params"]))
+        tuned = {"default_value": max(runs["default"]), "tuned_value": max(runs["tuned"]), "unit": UNIT,
+                 "runs": runs, "timed_region_value": value, "default_params": default_params,
                  "tuned_params": choice["params"], "search": choice["report"],
-                 "what": "the timed steps again, from the same state, with the autotuner's launch shapes"}
+                 "what": "the timed steps again after the search, from the same state, default and tuned "
+                         "launch shapes alternately (two runs each, the better kept)"}
     world.close()
 
     # Time to admissible from the initial specimen, plain PBD and with the

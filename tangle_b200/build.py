@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libtangle_cuda.so")
 SOURCES = [os.path.join(HERE, "csrc", name) for name in ("kernels.cu", "world.cu", "noalloc.cu", "warmstart.cu", "capture.cu", "formation.cu")]
-HEADERS = [os.path.join(HERE, "csrc", name) for name in ("common.cuh", "kernels.cuh", "contact.cuh", "umma_gemm.cuh", "warmstart.cuh", "formation.cuh")] + [
+HEADERS = [os.path.join(HERE, "csrc", name) for name in ("common.cuh", "kernels.cuh", "contact.cuh", "umma_gemm.cuh", "umma_gemm_tma.cuh", "warmstart.cuh", "formation.cuh")] + [
     os.path.join(ROOT, "include", "tangle_cuda.h")
 ]
 
