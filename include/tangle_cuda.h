@@ -367,7 +367,9 @@ typedef struct {
     uint32_t build_chunk;           /* candidate slots a Verlet-build block stages at once: 512 to 4096 */
     float contact_skin_fraction;    /* contact-list skin over the neighbor skin: 0 (lists off) or (0, 1];
                                        above 0 only where the world allocated contact lists */
-    uint32_t reserved[4];
+    uint32_t update_warps_per_block; /* warps per fiber-update block: 1, 2 or 4 (fewer where one warp's
+                                        staged fibers times this exceed 200 KB of shared memory) */
+    uint32_t reserved[3];
 } tgl_launch_params;
 
 int tgl_world_get_launch_params(tgl_world *world, tgl_launch_params *params);

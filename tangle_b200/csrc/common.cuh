@@ -221,8 +221,12 @@ struct Control {
     // Running maxima (as u32 bits of non-negative floats) for the next gate:
     // penetration, vertex step, curvature ratio.
     uint32_t acc[3];
-    // Blocks of the contact kernel finished this pass (last-block gate).
+    // Blocks of the contact kernel finished this pass (last-block gate and
+    // the reset of next_batch).
     uint32_t done_blocks;
+    // Next 32-slot batch a warp of the running contact pass takes; the last
+    // block to finish puts it back to 0.
+    uint32_t next_batch;
     uint32_t cell_overflow;
     // Contact lists: refresh pending, refreshes done.
     uint32_t contact_state[2];

@@ -75,6 +75,7 @@ __device__ inline void begin_batch(Control *ctl) {
     ctl->acc[1] = 0;
     ctl->acc[2] = 0;
     ctl->done_blocks = 0;
+    ctl->next_batch = 0;
 }
 
 template <bool A>
@@ -87,6 +88,7 @@ __global__ void begin_batch_kernel(WorldDev w) {
         if (threadIdx.x == 0) {
             w.ctl->control[0] = 1;  // some specimen may run; the first gate refines it
             w.ctl->done_blocks = 0;
+            w.ctl->next_batch = 0;
         }
     }
 }
@@ -813,14 +815,22 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     uint32_t *hm = hit_mask[warp];
     hm[lane] = 0u;
     uint32_t thread_max = 0;
-    const uint32_t warps_total = gridDim.x * CONTACT_WARPS;
     const uint64_t geom_policy = make_keep_policy();
     if (MODE == CONTACT_REFRESH) {
         // The snapshot the next passes measure displacement against.
         for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x)
             w.contact_ref[v] = w.pos[v];
     }
-    for (uint32_t base = (blockIdx.x * CONTACT_WARPS + warp) * 32u; base < w.NS; base += warps_total * 32u) {
+    // Warps take the batches in slot order from one counter, so the batches
+    // in flight at any moment are a narrow band of neighboring cells whose
+    // candidates' records stay in L2 (a fixed stride lets the warps drift
+    // apart over the pass and widen that band).
+    const auto take_batch = [&]() {
+        uint32_t b = 0;
+        if (lane == 0) b = atomicAdd(&w.ctl->next_batch, 1u);
+        return __shfl_sync(FULL, b, 0) * 32u;
+    };
+    for (uint32_t base = take_batch(); base < w.NS; base = take_batch()) {
         // Batches follow the cell list's slot order, so the 32 segments of a
         // batch are spatial neighbors and share most of their candidates.
         const bool in_range = base + lane < w.NS;
@@ -1051,19 +1061,23 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         }
         __syncwarp();
     }
-    if (!gate) return;
     thread_max = warp_max_u32(thread_max);
     if (lane == 0) warp_max[warp] = thread_max;
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t m = 0;
         for (int k = 0; k < CONTACT_WARPS; ++k) m = max(m, warp_max[k]);
-        if (!A && m) atomicMax(&w.ctl->acc[0], m);
+        if (gate && !A && m) atomicMax(&w.ctl->acc[0], m);
         __threadfence();
         is_last = atomicAdd(&w.ctl->done_blocks, 1u) == gridDim.x - 1;
     }
     __syncthreads();
     if (!is_last) return;
+    if (threadIdx.x == 0) {  // every warp of every block is past its last batch
+        w.ctl->next_batch = 0;
+        if (!gate) w.ctl->done_blocks = 0;
+    }
+    if (!gate) return;
     if (!A) {
         if (threadIdx.x == 0) {
             __threadfence();
@@ -1534,18 +1548,22 @@ __device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float ex
 // FM compiles in the formation work (wall reactions, layer and vertex
 // targets); without it the kernel carries none of it.
 template <int LPF, bool A = false, bool FM = false>
-__global__ void __launch_bounds__(32, 24) fiber_lanes_kernel(WorldDev w, StepParams sp, int stride) {
+__global__ void __launch_bounds__(128, 8) fiber_lanes_kernel(WorldDev w, StepParams sp, int stride) {
     constexpr int FPW = 32 / LPF;  // fibers per warp
     if (w.ctl->control[0] == 0) return;
-    extern __shared__ float4 lanes_smem[];
-    const int lane = threadIdx.x;
+    extern __shared__ float4 lanes_smem_all[];
+    // Each warp works alone on its own fibers; a block holds up to 4 warps
+    // only so that 32 warps fit on an SM (at most 32 blocks are resident).
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    float4 *const lanes_smem = lanes_smem_all + (size_t)wib * FPW * stride;
     const int group = lane / LPF, gl = lane % LPF;
     const uint32_t gmask = LPF == 32 ? FULL : (((1u << LPF) - 1u) << (group * LPF));
     uint32_t smax = 0, cmax = 0;
     bool far = false;
     bool contact_far = false;
     const bool contact_lists = !A && w.contact_skin > 0.0f;
-    for (uint32_t batch = blockIdx.x; batch * FPW < w.FA; batch += gridDim.x) {
+    for (uint32_t batch = blockIdx.x * wpb + wib; batch * FPW < w.FA; batch += gridDim.x * wpb) {
         const uint32_t slot = batch * FPW + group;
         uint32_t mine = slot < w.FA ? w.fiber_order[slot] : TGL_NONE;
         if (A && mine != TGL_NONE && ctl_of<A>(w, spec_of_fiber<A>(w, mine))->control[0] == 0) mine = TGL_NONE;
@@ -2053,7 +2071,16 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     lp.lanes_stride = (int)(w.max_fiber | 1u);
     lp.lanes_smem = (size_t)fpw * lp.lanes_stride * sizeof(float4);
     lp.fiber_lanes = w.max_fiber <= 32u * LANES_KMAX && lp.lanes_smem <= 200 * 1024;
-    lp.lanes_blocks = (int)((w.FA + fpw - 1) / fpw);
+    // Warps per block: 4 where their staged fibers fit, so that 32 warps
+    // (the register file at the kernel's 64 registers, and 8 blocks of 4
+    // warps) are resident per SM instead of the 28 that one-warp blocks get
+    // (their shared memory and 1 KB reserve per block run out first); the
+    // long tail of the grid then runs on a full SM.
+    const int wpb_max = lp.tune_wpb == 1 || lp.tune_wpb == 2 ? lp.tune_wpb : 4;
+    lp.lanes_wpb = 1;
+    while (lp.lanes_wpb < wpb_max && lp.lanes_smem * (size_t)(2 * lp.lanes_wpb) <= 200 * 1024) lp.lanes_wpb *= 2;
+    const uint32_t lane_warps = (w.FA + fpw - 1) / fpw;
+    lp.lanes_blocks = (int)((lane_warps + lp.lanes_wpb - 1) / lp.lanes_wpb);
     lp.contact_lists = w.contact_skin > 0.0f;
     lp.build_ch = lp.tune_build_ch >= 512 && lp.tune_build_ch <= 4096 ? lp.tune_build_ch : 3072;
     lp.build_smem = (size_t)lp.build_ch * (sizeof(float4) + sizeof(uint32_t));
@@ -2072,7 +2099,7 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     lp.sort_smem = (size_t)sw * w.block * 4;
     allow_dynamic_smem(fiber_kernel, std::max<size_t>(lp.fiber_smem, 1));
     if (lp.fiber_lanes) {
-        const size_t smem = lp.lanes_smem;
+        const size_t smem = lp.lanes_smem * lp.lanes_wpb;
         const auto allow = [smem](auto kernel) { allow_dynamic_smem(kernel, smem); };
         allow(fiber_lanes_kernel<2, false, false>);
         allow(fiber_lanes_kernel<4, false, false>);
@@ -2211,13 +2238,13 @@ int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp
 
 template <bool A, bool FM>
 static void enqueue_lanes(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st) {
+    const dim3 grid(lp.lanes_blocks), block(32 * lp.lanes_wpb);
+    const size_t smem = lp.lanes_smem * lp.lanes_wpb;
     switch (lp.lanes_per_fiber) {
-        case 2: fiber_lanes_kernel<2, A, FM><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
-        case 8: fiber_lanes_kernel<8, A, FM><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
-        case 32:
-            fiber_lanes_kernel<32, A, FM><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride);
-            break;
-        default: fiber_lanes_kernel<4, A, FM><<<lp.lanes_blocks, 32, lp.lanes_smem, st>>>(w, sp, lp.lanes_stride); break;
+        case 2: fiber_lanes_kernel<2, A, FM><<<grid, block, smem, st>>>(w, sp, lp.lanes_stride); break;
+        case 8: fiber_lanes_kernel<8, A, FM><<<grid, block, smem, st>>>(w, sp, lp.lanes_stride); break;
+        case 32: fiber_lanes_kernel<32, A, FM><<<grid, block, smem, st>>>(w, sp, lp.lanes_stride); break;
+        default: fiber_lanes_kernel<4, A, FM><<<grid, block, smem, st>>>(w, sp, lp.lanes_stride); break;
     }
 }
 

@@ -209,7 +209,9 @@ struct LaunchPlan {
     bool fiber_lanes;       // grouped-lane update (fibers of at most 256 vertices)
     int lanes_per_fiber;    // lanes per fiber in its curvature sweeps (2, 4, 8 or 32)
     int lanes_stride;
-    size_t lanes_smem;
+    size_t lanes_smem;      // staged fibers of one warp
+    int lanes_wpb;          // warps per block (1, 2 or 4)
+    int tune_wpb = 0;       // requested warps per block (0: the default, 4)
     int lanes_blocks;
     bool contact_lists;     // contact lists on (contact_skin > 0)
     int build_ch;           // candidate slots staged per build chunk

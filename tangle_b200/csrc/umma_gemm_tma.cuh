@@ -7,12 +7,15 @@
 // with three roles:
 //   warp 0 (one lane): the producer. For each 64-wide contraction chunk it
 //     waits for a free pipeline stage, announces the stage's bytes on its
-//     "full" mbarrier and issues one 2-D TMA load per 8-element k-group of A
-//     (box 8 x 128 rows) and of B (box 8 x N rows). A box of 8 bf16 (16
-//     bytes) by R rows lands as R rows of 16 bytes, which is exactly one
-//     k-group of the canonical no-swizzle core-matrix layout umma_gemm.cuh
-//     describes (row groups 128 bytes apart, k groups R / 8 * 128 apart), so
-//     the same shared-memory descriptors apply. Rows past M and k past K
+//     "full" mbarrier and issues two 2-D TMA loads: A (box 64 x 128 rows)
+//     and B (box 64 x N rows), both with the 128-byte swizzle. A box row is
+//     the chunk's 64 bf16 of one operand row (128 bytes, one request), and
+//     the box lands in the canonical K-major SWIZZLE_128B layout: row r at
+//     r * 128 bytes, its 16-byte piece j at piece j ^ (r % 8), 8-row atoms
+//     of 1024 bytes (the stride byte offset). The MMA for contraction step
+//     s (16 elements, 32 bytes) starts its descriptors 32 s bytes into the
+//     atom; the tensor core applies the same XOR to the address bits, so
+//     every stage starts on a 1024-byte boundary. Rows past M and k past K
 //     read as zero.
 //   warp 1 (one lane): the MMA issuer. It waits for a stage, issues its
 //     tcgen05.mma instructions (K = 16 each) into the tile's accumulator and
@@ -22,9 +25,12 @@
 //     between two accumulators, so the next tile accumulates while the
 //     previous one is being drained.
 //   warps 2-5: the epilogue. Each reads its 32 tensor-memory lanes of the
-//     finished accumulator (warp w may access lanes 32 (w % 4) .. + 31),
-//     applies bias / ReLU / mask / residual and stores, then arrives on the
-//     accumulator's "empty" mbarrier.
+//     finished accumulator (warp w may access lanes 32 (w % 4) .. + 31) 16
+//     columns at a time, one row per lane, and turns the slice around in
+//     shared memory so that four lanes share a row: bias / ReLU / mask /
+//     residual are applied and the results stored as 64-byte row pieces
+//     (f32) or 32-byte ones (bf16) instead of one 16-byte piece per row and
+//     lane. Then it arrives on the accumulator's "empty" mbarrier.
 // Every mbarrier wait is bounded: one that gives up records an error and
 // the CTA stops issuing work; before it exits, the producer waits (bounded)
 // for its loads still in flight and the MMA issuer for its last commit, and
@@ -46,6 +52,33 @@ constexpr int TMA_GEMM_THREADS = 192;  // producer, MMA, four epilogue warps
 // (N x 64 bf16), each 1 KiB aligned.
 __host__ __device__ inline uint32_t tma_stage_bytes(int n) {
     return (uint32_t)(GEMM_BM * GEMM_KC * 2) + (((uint32_t)n * GEMM_KC * 2 + 1023u) & ~1023u);
+}
+
+// Epilogue slices: 32 rows x 16 columns per warp, rows 20 floats apart (the
+// 4-float pad keeps both the row-per-lane writes and the row-piece reads
+// free of bank conflicts).
+constexpr int TMA_EPI_STRIDE = 20;
+constexpr uint32_t TMA_EPI_BYTES = 4u * 32u * TMA_EPI_STRIDE * 4u;
+
+// Dynamic shared memory of the kernel: the stages, the epilogue slices and
+// the slack that lets the first stage start on a 1024-byte boundary.
+__host__ __device__ inline uint32_t tma_smem_bytes(int n) {
+    return (uint32_t)TMA_GEMM_STAGES * tma_stage_bytes(n) + TMA_EPI_BYTES + 1024u;
+}
+
+// tcgen05 shared-memory descriptor of a K-major operand in the 128-byte
+// swizzle layout: start address, leading byte offset 16 (unused by this
+// layout, the value the canonical form carries), stride byte offset 1024
+// (one 8-row atom), version 1 at bit 46, base offset 0, layout type 2
+// (SWIZZLE_128B) at bits 61-63.
+__device__ inline uint64_t smem_desc_sw128(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)(16u >> 4) << 16;
+    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)2u << 61;
+    return d;
 }
 
 __device__ inline void mbar_init(uint32_t bar, uint32_t count) {
@@ -81,7 +114,7 @@ __global__ void __launch_bounds__(TMA_GEMM_THREADS, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n = g.n;
     const uint32_t stage_bytes = tma_stage_bytes(n);
-    const uint32_t smem0 = smem_u32(tma_smem);
+    const uint32_t smem0 = (smem_u32(tma_smem) + 1023u) & ~1023u;
     const int64_t tiles = ((int64_t)g.m + GEMM_BM - 1) / GEMM_BM;
     const int64_t chunks = (g.k + GEMM_KC - 1) / GEMM_KC;
     int cols = 32;
@@ -119,20 +152,15 @@ __global__ void __launch_bounds__(TMA_GEMM_THREADS, 1)
                         failed = 1;
                         break;
                     }
-                    const int64_t k0 = c * GEMM_KC;
-                    // Whole MMA steps of 16: an odd last k-group gets its
-                    // partner loaded past K, which reads as zeros.
-                    const int kk = (int)(g.k - k0 < GEMM_KC ? g.k - k0 : GEMM_KC);
-                    const int kgroups = 2 * ((kk + 15) / 16);
+                    // Whole boxes: the part past K (and past M) is filled
+                    // with zeros and counts toward the stage's bytes.
+                    const int32_t x = (int32_t)(c * GEMM_KC);
                     const uint32_t full = smem_u32(&full_bar[stage]);
-                    mbar_expect_tx(full, (uint32_t)kgroups * 16u * (uint32_t)(GEMM_BM + n));
+                    mbar_expect_tx(full, (uint32_t)(GEMM_KC * 2) * (uint32_t)(GEMM_BM + n));
                     const uint32_t sa = smem0 + stage * stage_bytes;
                     const uint32_t sb = sa + GEMM_BM * GEMM_KC * 2;
-                    for (int kg = 0; kg < kgroups; ++kg) {
-                        const int32_t x = (int32_t)(k0 + 8 * kg);
-                        tma_load_2d(sa + kg * (GEMM_BM / 8) * 128, &map_a, x, (int32_t)(t * GEMM_BM), full);
-                        tma_load_2d(sb + kg * (n / 8) * 128, &map_b, x, 0, full);
-                    }
+                    tma_load_2d(sa, &map_a, x, (int32_t)(t * GEMM_BM), full);
+                    tma_load_2d(sb, &map_b, x, 0, full);
                     ++issued[stage];
                     if (++stage == TMA_GEMM_STAGES) {
                         stage = 0;
@@ -153,7 +181,6 @@ __global__ void __launch_bounds__(TMA_GEMM_THREADS, 1)
             uint32_t stage = 0, phase = 0;
             uint32_t acc = 0, acc_phase[2] = {1u, 1u};  // fresh accumulators count as drained
             const uint32_t idesc = instr_desc_bf16(GEMM_BM, n, 0, 0);
-            const uint32_t lbo_a = (GEMM_BM / 8) * 128, lbo_b = (uint32_t)(n / 8) * 128;
             uint32_t last_commit_bar = 0, last_commit_phase = 0;
             bool committed = false;
             for (int64_t t = blockIdx.x; t < tiles && !failed; t += gridDim.x) {
@@ -176,8 +203,8 @@ __global__ void __launch_bounds__(TMA_GEMM_THREADS, 1)
                     const uint32_t sa = smem0 + stage * stage_bytes;
                     const uint32_t sb = sa + GEMM_BM * GEMM_KC * 2;
                     for (int s = 0; s < steps; ++s) {
-                        const uint64_t da = smem_desc(sa + 2 * s * lbo_a, lbo_a, 128);
-                        const uint64_t db = smem_desc(sb + 2 * s * lbo_b, lbo_b, 128);
+                        const uint64_t da = smem_desc_sw128(sa + 32u * (uint32_t)s);
+                        const uint64_t db = smem_desc_sw128(sb + 32u * (uint32_t)s);
                         const uint32_t accumulate = (c > 0 || s > 0) ? 1u : 0u;
                         asm volatile(
                             "{\n\t.reg .pred p;\n\t"
@@ -210,6 +237,10 @@ __global__ void __launch_bounds__(TMA_GEMM_THREADS, 1)
     } else {
         // Epilogue: warps 2-5; this warp's tensor-memory lanes and tile rows.
         const int quarter = warp & 3;
+        float *slice = reinterpret_cast<float *>(tma_smem + (smem0 - smem_u32(tma_smem)) +
+                                                 TMA_GEMM_STAGES * stage_bytes) +
+                       quarter * 32 * TMA_EPI_STRIDE;
+        const int cq = 4 * (lane & 3);  // this lane's 4 columns of a slice
         uint32_t acc = 0, acc_phase[2] = {0u, 0u};
         for (int64_t t = blockIdx.x; t < tiles && !failed; t += gridDim.x) {
             // The whole warp agrees on the wait before its collective loads.
@@ -220,7 +251,7 @@ __global__ void __launch_bounds__(TMA_GEMM_THREADS, 1)
             }
             acc_phase[acc] ^= 1u;
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const int64_t row = t * GEMM_BM + 32 * quarter + lane;
+            const int64_t row0 = t * GEMM_BM + 32 * quarter;
             const uint32_t d_tmem = tmem + acc * (uint32_t)cols;
             for (int c0 = 0; c0 < n; c0 += 16) {
                 uint32_t r[16];
@@ -233,32 +264,40 @@ __global__ void __launch_bounds__(TMA_GEMM_THREADS, 1)
                       "=r"(r[15])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (row < g.m) {
-                    float v[16];
+                // Row per lane in.
+                float4 *mine = reinterpret_cast<float4 *>(slice + lane * TMA_EPI_STRIDE);
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        float x = __uint_as_float(r[j]);
-                        if (g.bias) x += g.bias[c0 + j];
-                        if (g.relu) x = fmaxf(x, 0.0f);
-                        if (g.mask && !(__bfloat162float(g.mask[row * g.ld_mask + c0 + j]) > 0.0f)) x = 0.0f;
-                        if (g.residual) x += g.residual[row * g.ld_res + c0 + j];
-                        v[j] = x;
-                    }
-                    if (g.out_f32) {
-                        float4 *o = reinterpret_cast<float4 *>(g.out_f32 + row * g.ldo + c0);
+                for (int j = 0; j < 4; ++j)
+                    mine[j] = make_float4(__uint_as_float(r[4 * j]), __uint_as_float(r[4 * j + 1]),
+                                          __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
+                __syncwarp();
+                // Four lanes per row out: rows lane / 4 + 8 i, columns c0 + cq .. + 3.
+                const int col = c0 + cq;
 #pragma unroll
-                        for (int j = 0; j < 4; ++j)
-                            o[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-                    }
-                    if (g.out_bf16) {
-                        __nv_bfloat162 h[8];
+                for (int i = 0; i < 4; ++i) {
+                    const int rr = (lane >> 2) + 8 * i;
+                    const int64_t row = row0 + rr;
+                    const float4 a4 = *reinterpret_cast<const float4 *>(slice + rr * TMA_EPI_STRIDE + cq);
+                    if (row < g.m) {
+                        float v[4] = {a4.x, a4.y, a4.z, a4.w};
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
-                        uint4 *o = reinterpret_cast<uint4 *>(g.out_bf16 + row * g.ldo_bf16 + c0);
-                        o[0] = *reinterpret_cast<uint4 *>(&h[0]);
-                        o[1] = *reinterpret_cast<uint4 *>(&h[4]);
+                        for (int j = 0; j < 4; ++j) {
+                            float x = v[j];
+                            if (g.bias) x += g.bias[col + j];
+                            if (g.relu) x = fmaxf(x, 0.0f);
+                            if (g.mask && !(__bfloat162float(g.mask[row * g.ld_mask + col + j]) > 0.0f)) x = 0.0f;
+                            if (g.residual) x += g.residual[row * g.ld_res + col + j];
+                            v[j] = x;
+                        }
+                        if (g.out_f32)
+                            *reinterpret_cast<float4 *>(g.out_f32 + row * g.ldo + col) = make_float4(v[0], v[1], v[2], v[3]);
+                        if (g.out_bf16) {
+                            __nv_bfloat162 h[2] = {__floats2bfloat162_rn(v[0], v[1]), __floats2bfloat162_rn(v[2], v[3])};
+                            *reinterpret_cast<uint2 *>(g.out_bf16 + row * g.ldo_bf16 + col) = *reinterpret_cast<uint2 *>(h);
+                        }
                     }
                 }
+                __syncwarp();
             }
             // This warp's lanes are read: the accumulator may be reused.
             asm volatile("tcgen05.fence::before_thread_sync;");

@@ -45,18 +45,19 @@ EncodeTiled encode_tiled() {
 }
 
 // A K-major bf16 operand of `rows` rows and `k` columns (leading dimension
-// `ld` elements) as a 2-D tensor map with boxes of 8 contraction elements by
-// `box_rows` rows: each box is one k-group of the canonical no-swizzle
-// layout. Out-of-range elements read as zero.
+// `ld` elements) as a 2-D tensor map with boxes of 64 contraction elements
+// (128 bytes) by `box_rows` rows in the 128-byte swizzle: each box is one
+// contraction chunk in the canonical K-major SWIZZLE_128B layout.
+// Out-of-range elements read as zero.
 bool kmajor_map(CUtensorMap *map, const void *base, int64_t rows, int64_t k, int64_t ld, int box_rows) {
     EncodeTiled encode = encode_tiled();
     if (!encode) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)ld * 2u};
-    const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+    const cuuint32_t box[2] = {(cuuint32_t)tgl::GEMM_KC, (cuuint32_t)box_rows};
     const cuuint32_t element_strides[2] = {1u, 1u};
     return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
-                  element_strides, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  element_strides, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -70,7 +71,7 @@ int gemm_tma(const tgl_gemm *p, const tgl::GemmArgs &g, cudaStream_t stream) {
     if (!kmajor_map(&map_a, p->a, p->m, p->k, p->lda, tgl::GEMM_BM) ||
         !kmajor_map(&map_b, p->b, p->n, p->k, p->ldb, p->n))
         return 1;
-    const size_t smem = (size_t)tgl::TMA_GEMM_STAGES * tgl::tma_stage_bytes(p->n);
+    const size_t smem = tgl::tma_smem_bytes(p->n);
     static std::once_flag once;
     static int sms = 0;
     std::call_once(once, [] {
@@ -78,7 +79,7 @@ int gemm_tma(const tgl_gemm *p, const tgl::GemmArgs &g, cudaStream_t stream) {
         cudaGetDevice(&device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         cudaFuncSetAttribute(tgl::umma_gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)((size_t)tgl::TMA_GEMM_STAGES * tgl::tma_stage_bytes(256)));
+                             (int)tgl::tma_smem_bytes(256));
     });
     int cols = 32;
     while (cols < p->n) cols <<= 1;

@@ -1803,6 +1803,8 @@ int check_launch_params(const tgl_world *w, const tgl_launch_params &p) {
         return set_error(TGL_ERR_INVALID, "contact_skin_fraction must be in [0, 1]");
     if (p.contact_skin_fraction > 0.0f && w->dev.contact_block == 0)
         return set_error(TGL_ERR_UNSUPPORTED, "this world has no contact lists to size");
+    if (p.update_warps_per_block != 1 && p.update_warps_per_block != 2 && p.update_warps_per_block != 4)
+        return set_error(TGL_ERR_INVALID, "update_warps_per_block must be 1, 2 or 4");
     return 0;
 }
 
@@ -1813,6 +1815,7 @@ void current_launch_params(const tgl_world *w, tgl_launch_params *p) {
     p->contact_blocks_per_sm = (uint32_t)(w->lp.tune_contact_per_sm ? w->lp.tune_contact_per_sm : std::min(3, std::max(per_sm, 1)));
     p->build_chunk = (uint32_t)w->lp.build_ch;
     p->contact_skin_fraction = w->contact_fraction;
+    p->update_warps_per_block = (uint32_t)(w->lp.tune_wpb ? w->lp.tune_wpb : 4);
 }
 
 int apply_launch_params(tgl_world *w, const tgl_launch_params &p) {
@@ -1820,6 +1823,7 @@ int apply_launch_params(tgl_world *w, const tgl_launch_params &p) {
     w->lp.tune_lanes = (int)p.lanes_per_fiber;
     w->lp.tune_contact_per_sm = (int)p.contact_blocks_per_sm;
     w->lp.tune_build_ch = (int)p.build_chunk;
+    w->lp.tune_wpb = (int)p.update_warps_per_block;
     if (w->dev.contact_block) set_contact_skin(w, p.contact_skin_fraction);
     plan_launches(w->dev, w->lp);
     drop_graphs(w);
@@ -1963,9 +1967,10 @@ int tgl_autotune(tgl_world *w, const tgl_relax_config *config, uint32_t trial_it
     const uint32_t block_choices[] = {1, 2, 3};
     const uint32_t chunk_choices[] = {1024, 2048, 3072, 4096};
     const float skin_choices[] = {0.05f, 0.1f, 0.15f, 0.25f};
+    const uint32_t wpb_choices[] = {1, 2, 4};
     // Coordinate descent: each parameter in turn over its candidates, the
     // others held at the best so far.
-    for (int parameter = 0; parameter < 4; ++parameter) {
+    for (int parameter = 0; parameter < 5; ++parameter) {
         std::vector<tgl_launch_params> candidates;
         tgl_launch_params c = current;
         if (parameter == 0 && lanes)
@@ -1976,6 +1981,8 @@ int tgl_autotune(tgl_world *w, const tgl_relax_config *config, uint32_t trial_it
             for (uint32_t v : chunk_choices) c.build_chunk = v, candidates.push_back(c);
         if (parameter == 3 && w->dev.contact_block)
             for (float v : skin_choices) c.contact_skin_fraction = v, candidates.push_back(c);
+        if (parameter == 4 && lanes)
+            for (uint32_t v : wpb_choices) c.update_warps_per_block = v, candidates.push_back(c);
         for (const tgl_launch_params &candidate : candidates) {
             if (std::memcmp(&candidate, &current, sizeof(candidate)) == 0) continue;
             if (int rc = apply_launch_params(w, candidate)) return fail(rc);

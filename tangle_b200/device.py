@@ -165,10 +165,13 @@ class LaunchParams(ctypes.Structure):
         ("contact_blocks_per_sm", ctypes.c_uint32),
         ("build_chunk", ctypes.c_uint32),
         ("contact_skin_fraction", ctypes.c_float),
-        ("reserved", ctypes.c_uint32 * 4),
+        ("update_warps_per_block", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 3),
     ]
 
-    FIELDS = ("lanes_per_fiber", "contact_blocks_per_sm", "build_chunk", "contact_skin_fraction")
+    FIELDS = ("lanes_per_fiber", "contact_blocks_per_sm", "build_chunk", "contact_skin_fraction",
+              "update_warps_per_block")
+    DEFAULTS = {"update_warps_per_block": 4}  # for choices saved before the field existed
 
     def as_dict(self) -> dict:
         return {name: (float(getattr(self, name)) if name == "contact_skin_fraction" else int(getattr(self, name)))
@@ -178,7 +181,7 @@ class LaunchParams(ctypes.Structure):
     def from_dict(cls, values: dict) -> "LaunchParams":
         out = cls()
         for name in cls.FIELDS:
-            setattr(out, name, values[name])
+            setattr(out, name, values[name] if name in values else cls.DEFAULTS[name])
         return out
 
 

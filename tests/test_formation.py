@@ -380,3 +380,33 @@ def test_checkpoint_carries_the_formation_state(cuda_lib, tmp_path):
                                   dev.download_positions().view(np.uint32))
     e1, e2 = restored.formation_target_error(), dev.formation_target_error()
     assert (e1.layer, e1.vertex) == (e2.layer, e2.vertex)
+
+
+@pytest.mark.gpu
+def test_frozen_fibers_stay_out_of_later_rebuilds(cuda_lib):
+    """Freezing deposited plies leaves their Verlet lists behind, unused;
+    several rebuilds later, and after the plies thaw again, the relaxation is
+    still the oracle's bit for bit and the lists of the segments in the cell
+    list are the oracle's."""
+    stack = small_stack()
+    packed = PackedAssembly.from_assembly(stack)
+    d = 7.0e-6
+    orc, dev = world_of("oracle", packed, 0.2 * d), world_of("cuda", packed, 0.2 * d)
+    flexible = deposit_stack(orc, dev, stack)
+    for w in (orc, dev):
+        w.activate_formation_step(0)
+    for k in range(3):
+        run_both(orc, dev, flexible, 3, f"frozen plies, rebuild {k}")
+        for w in (orc, dev):
+            w.debug_rebuild()
+    active = np.asarray(dev.fiber_active, dtype=bool)
+    on = active[np.asarray(packed.segment_fibers)]
+    oc, ol = orc.debug_neighbor_lists()
+    dc, dl = dev.debug_neighbor_lists()
+    for s in np.nonzero(on)[0]:
+        assert oc[s] == dc[s]
+        if ol[s] is not None:
+            np.testing.assert_array_equal(ol[s], dl[s])
+    for w in (orc, dev):
+        w.activate_formation_step(2)
+    run_both(orc, dev, flexible, 5, "plies thawed")

@@ -30,9 +30,12 @@ def small_world_inputs():
 
 
 @pytest.mark.parametrize("params", [
-    {"lanes_per_fiber": 4, "contact_blocks_per_sm": 1, "build_chunk": 1024, "contact_skin_fraction": 0.25},
-    {"lanes_per_fiber": 32, "contact_blocks_per_sm": 2, "build_chunk": 4096, "contact_skin_fraction": 0.05},
-    {"lanes_per_fiber": 2, "contact_blocks_per_sm": 3, "build_chunk": 512, "contact_skin_fraction": 0.0},
+    {"lanes_per_fiber": 4, "contact_blocks_per_sm": 1, "build_chunk": 1024, "contact_skin_fraction": 0.25,
+     "update_warps_per_block": 1},
+    {"lanes_per_fiber": 32, "contact_blocks_per_sm": 2, "build_chunk": 4096, "contact_skin_fraction": 0.05,
+     "update_warps_per_block": 2},
+    {"lanes_per_fiber": 2, "contact_blocks_per_sm": 3, "build_chunk": 512, "contact_skin_fraction": 0.0,
+     "update_warps_per_block": 4},
 ], ids=["lanes4", "lanes32", "lanes2_lists_off"])
 def test_every_launch_shape_gives_the_oracle_positions(params, cuda_lib):
     from oracle import OracleWorld
@@ -42,8 +45,8 @@ def test_every_launch_shape_gives_the_oracle_positions(params, cuda_lib):
     dev = DeviceWorld(packed, fixed.cell_list, fixed.max_step)
     dev.set_launch_params(params)
     got = dev.launch_params()
-    assert {k: got[k] for k in ("lanes_per_fiber", "contact_blocks_per_sm", "build_chunk")} == {
-        k: params[k] for k in ("lanes_per_fiber", "contact_blocks_per_sm", "build_chunk")}
+    keys = ("lanes_per_fiber", "contact_blocks_per_sm", "build_chunk", "update_warps_per_block")
+    assert {k: got[k] for k in keys} == {k: params[k] for k in keys}
     orc = OracleWorld(packed, fixed.cell_list, fixed.max_step)
     for batch in (9, 23):
         assert dev.run_batch(fixed, batch).total_iterations == orc.run_batch(fixed, batch).total_iterations
@@ -59,7 +62,7 @@ def test_launch_params_are_validated(cuda_lib):
     dev = DeviceWorld(packed, fixed.cell_list, fixed.max_step)
     good = dev.launch_params()
     for bad in ({"lanes_per_fiber": 16}, {"contact_blocks_per_sm": 4}, {"build_chunk": 8192},
-                {"contact_skin_fraction": 1.5}):
+                {"contact_skin_fraction": 1.5}, {"update_warps_per_block": 3}):
         with pytest.raises(ValueError):
             dev.set_launch_params({**good, **bad})
     assert dev.launch_params() == good
@@ -80,7 +83,7 @@ def test_search_leaves_the_world_state_unchanged(cuda_lib, tmp_path):
     assert not result["cached"] and result["report"]["trials"] >= 8
     p = result["params"]
     assert p["lanes_per_fiber"] in (2, 4, 8, 32) and p["contact_blocks_per_sm"] in (1, 2, 3)
-    assert p["build_chunk"] in (1024, 2048, 3072, 4096)
+    assert p["build_chunk"] in (1024, 2048, 3072, 4096) and p["update_warps_per_block"] in (1, 2, 4)
     assert any(abs(p["contact_skin_fraction"] - v) < 1.0e-6 for v in (0.05, 0.1, 0.15, 0.25))
     assert result["report"]["best_ms"] <= result["report"]["default_ms"]
     a, b = tuned.run_batch(fixed, 41), plain.run_batch(fixed, 41)
