@@ -1129,8 +1129,16 @@ __device__ inline bool curvature_triplet_test(const float4 *P, const float4 *St,
     float4 pp = P[prev], pc = P[center], pn = P[next];
     float ux = pc.x - pp.x, uy = pc.y - pp.y, uz = pc.z - pp.z;
     float vx = pn.x - pc.x, vy = pn.y - pc.y, vz = pn.z - pc.z;
-    float first_length = sqrtf(ux * ux + uy * uy + uz * uz);
-    float second_length = sqrtf(vx * vx + vy * vy + vz * vz);
+    const float uu = ux * ux + uy * uy + uz * uz;
+    const float vv = vx * vx + vy * vy + vz * vz;
+    if (uu > 1.0e-12f && vv > 1.0e-12f) {  // the rough rejection of lanes_test, below
+        const float ru = rsqrtf(uu), rv = rsqrtf(vv);
+        const float rough_half = 0.25f * maximum_curvature * (uu * ru + vv * rv);
+        const float rough_limit = 1.0f - 2.0f * rough_half * rough_half;
+        if ((ux * vx + uy * vy + uz * vz) * (ru * rv) > rough_limit + 1.0e-5f) return false;
+    }
+    float first_length = sqrtf(uu);
+    float second_length = sqrtf(vv);
     if (!(first_length > 1.0e-7f && second_length > 1.0e-7f)) return false;
     float unx = ux / first_length, uny = uy / first_length, unz = uz / first_length;
     float vnx = vx / second_length, vny = vy / second_length, vnz = vz / second_length;
@@ -1459,10 +1467,13 @@ __device__ inline float lanes_limit(float4 p) { return fabsf(p.w); }
 // (t, t+1, t+2) of a staged fiber, split into the test (does the projection
 // move anything?) and the move, so that a lane group can test several
 // triplets at once and apply only the first that acts. A cheap test first
-// rules out triplets that certainly satisfy their limit: the limit's cosine
-// uses the same IEEE square roots as the exact path (so it is identical),
-// and the rsqrt-based cosine is within 1e-6 of the exact f32 cosine, so a
-// 1e-5 margin never skips a triplet the exact computation would project.
+// rules out triplets that certainly satisfy their limit, before any IEEE
+// square root or division: edge lengths and the cosine from rsqrtf (2 ulp).
+// The rough limit cosine is within 2e-6 of the exact path's (whose lengths
+// are correctly rounded square roots) wherever the exact path can act, and
+// the rough cosine within 1e-6 of its cosine, so a 1e-5 margin never skips a
+// triplet the exact computation would project; the exact path that follows
+// is the reference's, operation for operation.
 __device__ inline bool lanes_test(const float4 *P, int t, float stiffness, float safety_margin, Triplet &tr) {
     const float4 pp = P[t], pc = P[t + 1], pn = P[t + 2];
     const float maximum_curvature = lanes_limit(pc) * (1.0f - safety_margin);
@@ -1471,15 +1482,18 @@ __device__ inline bool lanes_test(const float4 *P, int t, float stiffness, float
     const float vx = pn.x - pc.x, vy = pn.y - pc.y, vz = pn.z - pc.z;
     const float uu = ux * ux + uy * uy + uz * uz;
     const float vv = vx * vx + vy * vy + vz * vz;
+    if (uu > 1.0e-12f && vv > 1.0e-12f) {
+        const float ru = rsqrtf(uu), rv = rsqrtf(vv);
+        const float rough_half = 0.25f * maximum_curvature * (uu * ru + vv * rv);
+        const float rough_limit = 1.0f - 2.0f * rough_half * rough_half;
+        if ((ux * vx + uy * vy + uz * vz) * (ru * rv) > rough_limit + 1.0e-5f) return false;
+    }
     const float first_length = sqrtf(uu);
     const float second_length = sqrtf(vv);
     if (!(first_length > 1.0e-7f && second_length > 1.0e-7f)) return false;
     const float sine_half = 0.25f * maximum_curvature * (first_length + second_length);
     if (!(sine_half < 1.0f)) return false;
     const float minimum_cosine = 1.0f - 2.0f * sine_half * sine_half;
-    if (uu > 1.0e-12f && vv > 1.0e-12f &&
-        (ux * vx + uy * vy + uz * vz) * rsqrtf(uu * vv) > minimum_cosine + 1.0e-5f)
-        return false;
     const float unx = ux / first_length, uny = uy / first_length, unz = uz / first_length;
     const float vnx = vx / second_length, vny = vy / second_length, vnz = vz / second_length;
     const float cosine = clampf(unx * vnx + uny * vny + unz * vnz, -1.0f, 1.0f);
