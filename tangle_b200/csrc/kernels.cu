@@ -361,6 +361,58 @@ __device__ inline float key_float(int k) { return __int_as_float(k >= 0 ? k : k 
 // Distance along one axis from 0 to the interval [lo, hi].
 __device__ inline float interval_gap(float lo, float hi) { return fmaxf(0.0f, fmaxf(lo, -hi)); }
 
+// Each cell's CellBox, once per rebuild: one warp per cell reduces the
+// bounding spheres in its slot range. The build's culling reads the 27
+// boxes around a home cell from here instead of every home block
+// recomputing the boxes of its stencil cells.
+template <bool A>
+__global__ void rb_boxes_kernel(WorldDev w) {
+    if (w.ctl->neighbor_state[0] == 0) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < w.C; c += warps) {
+        const uint32_t spec = spec_of_cell<A>(w, c);
+        if (A && !rebuilding<A>(w, spec)) continue;
+        const Grid &g = grid_of<A>(w, spec);
+        const uint32_t local = c - cell_base_of<A>(w, spec);
+        const float face[3] = {g.lower[0] + (float)(local % g.cells[0]) * g.width[0],
+                               g.lower[1] + (float)((local / g.cells[0]) % g.cells[1]) * g.width[1],
+                               g.lower[2] + (float)(local / (g.cells[0] * g.cells[1])) * g.width[2]};
+        int lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = float_key(INFINITY);
+            hi[a] = float_key(-INFINITY);
+        }
+        uint32_t mag = 0u;
+        const uint32_t n = w.cell_counts[c], off = w.cell_offsets[c];
+        for (uint32_t i = lane; i < n; i += 32) {
+            const float4 sp = w.slot_sphere[off + i];
+            const float r = sp.w * 1.0003f;
+            const float centre[3] = {sp.x, sp.y, sp.z};
+            for (int a = 0; a < 3; ++a) {
+                float p = centre[a] - face[a];
+                if (g.periodic[a]) p -= rintf(p * g.inv_length[a]) * g.length[a];
+                float l = p - r, h = p + r;
+                if (!(isfinite(l) && isfinite(h))) {
+                    l = -INFINITY;
+                    h = INFINITY;
+                }
+                lo[a] = min(lo[a], float_key(l));
+                hi[a] = max(hi[a], float_key(h));
+            }
+            mag = max(mag, __float_as_uint(fabsf(sp.x) + fabsf(sp.y) + fabsf(sp.z)));
+        }
+        CellBox box;
+        for (int a = 0; a < 3; ++a) {
+            box.lo[a] = __reduce_min_sync(FULL, lo[a]);
+            box.hi[a] = __reduce_max_sync(FULL, hi[a]);
+        }
+        box.mag = __reduce_max_sync(FULL, mag);
+        box.pad = 0u;
+        if (lane == 0) w.cell_box[c] = box;
+    }
+}
+
 // build_segment_neighbor_lists (neighbor.rs:171-364). One block per home cell.
 // The 27 stencil cells' bounding spheres are staged in shared memory; each
 // warp takes one home segment and tests 32 candidates at a time with a
@@ -374,11 +426,13 @@ __device__ inline float interval_gap(float lo, float hi) { return fmaxf(0.0f, fm
 // queue up and get the exact test 32 at a time; hits append in scan order
 // and are sorted later.
 //
-// Stencil-cell culling (with the sphere test on). While staging, the block
-// bounds each stencil cell's staged spheres, radii scaled by 1.0003, by a box
-// in that cell's own frame: centre minus the cell's lower corner, wrapped
-// into the nearest image on periodic axes, so the frame is right whichever
-// image the unwrapped coordinates sit in. A home warp then skips every cell
+// Stencil-cell culling (with the sphere test on). rb_boxes_kernel bounds each
+// cell's spheres, radii scaled by 1.0003, by a box in that cell's own frame
+// (centre minus the cell's lower corner, wrapped into the nearest image on
+// periodic axes, so the frame is right whichever image the unwrapped
+// coordinates sit in), once per rebuild; the block reads the boxes of its 27
+// stencil cells (a stencil staged in several chunks tests each chunk against
+// its cells' whole boxes, a superset). A home warp then skips every cell
 // whose box is farther from its own sphere centre (in the home cell's frame,
 // shifted by the stencil offset, nearest of the three images on periodic
 // axes) than (home radius + skin) * 1.0002 + the sphere test's margin + a
@@ -421,6 +475,14 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
             }
             st_count[threadIdx.x] = cell == TGL_NONE ? 0u : w.cell_counts[cell];
             st_off[threadIdx.x] = cell == TGL_NONE ? 0u : w.cell_offsets[cell];
+            if (prefilter && cell != TGL_NONE) {
+                const CellBox box = w.cell_box[cell];
+                for (int a = 0; a < 3; ++a) {
+                    box_lo[threadIdx.x][a] = box.lo[a];
+                    box_hi[threadIdx.x][a] = box.hi[a];
+                }
+                box_mag[threadIdx.x] = box.mag;
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -442,38 +504,13 @@ __global__ void __launch_bounds__(256) rb_build_kernel(WorldDev w, int ch, int p
         }
         for (uint32_t base = 0; base < total; base += (uint32_t)ch) {
             uint32_t len = min((uint32_t)ch, total - base);
-            if (prefilter && threadIdx.x < 27) {
-                for (int a = 0; a < 3; ++a) {
-                    box_lo[threadIdx.x][a] = float_key(INFINITY);
-                    box_hi[threadIdx.x][a] = float_key(-INFINITY);
-                }
-                box_mag[threadIdx.x] = 0u;
-            }
-            __syncthreads();
             for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
                 uint32_t flat = base + i;
                 int k = 0;
                 while (k < 26 && st_prefix[k + 1] <= flat) ++k;
                 uint32_t slot = st_off[k] + (flat - st_prefix[k]);
                 slot_of[i] = slot;
-                const float4 sp = w.slot_sphere[slot];
-                build_smem[i] = sp;
-                if (prefilter) {
-                    const float r = sp.w * 1.0003f;
-                    const float c[3] = {sp.x, sp.y, sp.z};
-                    for (int a = 0; a < 3; ++a) {
-                        float p = c[a] - st_face[k][a];
-                        if (g.periodic[a]) p -= rintf(p * g.inv_length[a]) * g.length[a];
-                        float lo = p - r, hi = p + r;
-                        if (!(isfinite(lo) && isfinite(hi))) {
-                            lo = -INFINITY;
-                            hi = INFINITY;
-                        }
-                        atomicMin(&box_lo[k][a], float_key(lo));
-                        atomicMax(&box_hi[k][a], float_key(hi));
-                    }
-                    atomicMax(&box_mag[k], __float_as_uint(fabsf(sp.x) + fabsf(sp.y) + fabsf(sp.z)));
-                }
+                build_smem[i] = w.slot_sphere[slot];
             }
             __syncthreads();
             for (uint32_t hi = warp; hi < nh; hi += warps) {
@@ -2175,6 +2212,7 @@ static void enqueue_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_
     rb_scatter_kernel<A><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
     rb_sort_cells_kernel<A><<<grid_for(w.C, 8, cap), 256, 8 * CELL_SORT_CAP * sizeof(uint32_t), st>>>(w);
     rb_gather_kernel<A><<<grid_for(w.S, 256, cap), 256, 0, st>>>(w);
+    rb_boxes_kernel<A><<<grid_for(w.C, 8, cap), 256, 0, st>>>(w);
     rb_build_kernel<A><<<(int)std::min<uint64_t>(w.C, (uint64_t)lp.num_sms * 64), 256, lp.build_smem, st>>>(
         w, lp.build_ch, lp.build_prefilter, lp.build_sphere_eps);
     rb_sort_lists_kernel<A><<<grid_for(w.S, lp.sort_warps, cap), lp.sort_warps * 32, lp.sort_smem, st>>>(w);
@@ -2197,7 +2235,7 @@ int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st) {
         enqueue_rebuild<true>(w, lp, st);
     else
         enqueue_rebuild<false>(w, lp, st);
-    return 10;
+    return REBUILD_KERNELS;
 }
 
 // The condition reads exactly the flag the gated rebuild kernels test on

@@ -20,6 +20,16 @@ struct SpecimenDev {
 };
 
 // Every device pointer and size a kernel needs, passed by value.
+// Bounding box of a cell's segment spheres (radii x 1.0003) in the cell's
+// own frame: centre minus the cell's lower corner, wrapped to the nearest
+// image on periodic axes; as order-preserving int keys (float_key), and the
+// largest |x| + |y| + |z| of a centre (f32 bits). Empty cells keep
+// [+inf, -inf].
+struct CellBox {
+    int lo[3], hi[3];
+    uint32_t mag, pad;
+};
+
 struct WorldDev {
     uint32_t V, S, F, C;
     uint32_t block;      // neighbor slots per segment list
@@ -59,6 +69,7 @@ struct WorldDev {
     uint32_t *ticket;        // [S] scatter position inside its cell; sort scratch
     float4 *slot_geom;       // [2S] geometry records in slot order
     float4 *slot_sphere;     // [S] midpoint and half length + radius, slot order
+    CellBox *cell_box;       // [C] box of each cell's bounding spheres, cell frame (build culling)
     // Verlet lists.
     uint32_t *nbr_count; // [S] true neighbor count
     uint32_t *nbr_list;  // [S * block]
@@ -226,6 +237,8 @@ struct LaunchPlan {
 int launch_begin_batch(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 int launch_flag_displacement(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 int launch_measure_start(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
+// Kernels in one rebuild pipeline (launch_rebuild's launches).
+constexpr int REBUILD_KERNELS = 11;
 int launch_rebuild(const WorldDev &w, const LaunchPlan &lp, cudaStream_t st);
 // The cell list alone (clear, count, scan, scatter, rank) on w's grid and
 // cell buffers, gated on the rebuild flag like the full rebuild.

@@ -300,7 +300,7 @@ static cudaError_t capture_body(tgl_world *w, cudaGraph_t body, F enqueue) {
 
 // One step's rebuild as a conditional node: a kernel sets the condition
 // from the pending-rebuild flag and an IF node runs the rebuild pipeline
-// only then, so the ten gated-off launches are not made at all (every
+// only then, so the eleven gated-off launches are not made at all (every
 // kernel keeps its own test). The contact pass stays two gated launches:
 // an IF/ELSE node between them measured slower than the launch it saves.
 static cudaError_t enqueue_conditional_rebuild(tgl_world *w, int *kernels) {
@@ -839,6 +839,7 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
         (rc = w->upload(&d.geom, geom)) || (rc = w->alloc(&d.corr, 2 * (size_t)S)) ||
         (rc = w->alloc(&d.vertex_step, V)) || (rc = w->alloc(&d.cell_counts, C)) ||
         (rc = w->alloc(&d.cell_offsets, C)) || (rc = w->alloc(&d.cell_segments, S)) ||
+        (rc = w->alloc(&d.cell_box, C)) ||
         (rc = w->alloc(&d.cell_of, S)) || (rc = w->alloc(&d.ticket, S)) ||
         (rc = w->alloc(&d.slot_geom, 2 * (size_t)S)) || (rc = w->alloc(&d.slot_sphere, S)) || (rc = w->alloc(&d.nbr_count, S)) ||
         (rc = w->alloc(&d.nbr_list, std::max<uint64_t>((uint64_t)S * block, 1))) ||
@@ -1029,9 +1030,9 @@ int tgl_run_batch(tgl_world *w, const tgl_relax_config *config, uint32_t iterati
     if (int rc = read_status(w, *config, status)) return rc;
     if (it->second.looped)  // the step condition, two contact passes and the update per step that ran
         w->launches += 4ull * w->host_ctl[0].loop_step;
-    if (w->conditional) {  // rebuild pipelines the graph ran (10 kernels each)
+    if (w->conditional) {  // rebuild pipelines the graph ran (REBUILD_KERNELS each)
         const uint32_t bodies = w->host_ctl[0].rebuild_bodies;
-        w->launches += 10ull * (bodies >= w->rebuild_bodies_seen ? bodies - w->rebuild_bodies_seen : bodies);
+        w->launches += (uint64_t)REBUILD_KERNELS * (bodies >= w->rebuild_bodies_seen ? bodies - w->rebuild_bodies_seen : bodies);
         w->rebuild_bodies_seen = bodies;
     }
     TGL_CUDA(cudaGetLastError());

@@ -2,11 +2,11 @@
 the device.
 
 A one-thread kernel sets an IF node's condition from the pending-rebuild
-flag, so the ten gated rebuild kernels launch only when a rebuild runs. The
+flag, so the eleven gated rebuild kernels launch only when a rebuild runs. The
 alternative capture (`TGL_NO_CONDITIONAL_GRAPHS=1`, read when a world is
 created) launches them every step and lets each return at once. Both must
 give the same bits, and the launch count of the conditional graph must add
-the ten kernels only for the pipelines that ran.
+the eleven kernels only for the pipelines that ran.
 
 By default the batch graph is one WHILE node over a single step: a kernel
 sets the rebuild condition and the loop's own (another step while the gate
@@ -27,7 +27,7 @@ from tangle_b200.settings import CellListConfig, RelaxationConfig, RelaxationSet
 
 pytestmark = pytest.mark.gpu
 
-REBUILD_KERNELS = 10
+REBUILD_KERNELS = 11
 
 
 def make_world(packed, cell_list, max_step, conditional: bool, looped: bool = True):
@@ -74,7 +74,7 @@ def test_conditional_rebuild_matches_gated_launches(case, cuda_lib):
         assert (sc.total_iterations, sc.batch_iterations) == (sg.total_iterations, sg.batch_iterations)
         new_rebuilds = cond.neighbor_list_rebuilds() - rebuilds[0]
         assert new_rebuilds == gated.neighbor_list_rebuilds() - rebuilds[1]
-        # Per step the gated graph launches the ten rebuild kernels, the
+        # Per step the gated graph launches the eleven rebuild kernels, the
         # conditional one a condition kernel, plus the pipelines that ran.
         steps = batch + 1
         cond_launches = cond.kernel_launches - launches[0]
