@@ -240,11 +240,14 @@ def contact_bytes(world):
     info = world.contact_list_info()
     if info["block"] == 0:
         return full, full
-    ccounts, clists = world.debug_contact_lists()
+    from tangle_b200.device import CONTACT_USE_VERLET
+
+    states = world.debug_contact_states()
     _, _, slot_segment = world.debug_cell_list()
     verlet_by_slot = listed_verlet[slot_segment]
-    on_verlet = np.array([entries is None for entries in clists], dtype=bool)
-    chunked = np.where(on_verlet, 0, ccounts).astype(np.float64)
+    on_verlet = states == CONTACT_USE_VERLET
+    scanned = states == 0xFFFFFFFF
+    chunked = np.where(on_verlet | scanned, 0, states).astype(np.float64)
     walked = np.where(on_verlet, verlet_by_slot, chunked)
     listed = 60.0 * S + 4.0 * float(walked.sum())
     kept = chunked

@@ -330,7 +330,8 @@ int tgl_debug_neighbor_lists(tgl_world *world, uint32_t *counts, uint32_t *lists
  * Verlet list overflowed (the pass scans the cells) -- and the chunks
  * [ceil(S / 32) * 32 * block]: the 32 slots of batch b (slots 32b to
  * 32b + 31) keep their lists back to back, in slot order, from entry
- * 32b * block on. TGL_ERR_UNSUPPORTED when contact lists are off. */
+ * 32b * block on; `chunks` may be null (the states alone).
+ * TGL_ERR_UNSUPPORTED when contact lists are off. */
 int tgl_debug_contact_lists(tgl_world *world, uint32_t *states, uint32_t *chunks);
 /* One contact pass (find_segment_corrections, contact.rs:232-902) on the
  * current positions and lists, moving nothing: corrections [6S] and

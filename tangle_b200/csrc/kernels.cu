@@ -115,11 +115,10 @@ __global__ void flag_displacement_kernel(WorldDev w) {
         float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
         far = dx * dx + dy * dy + dz * dz > md * md;
         if (A && far) flag_rebuild<A>(w, spec);
-        if (!A && w.contact_skin > 0.0f) contact_far = contact_moved(w, v, p.x, p.y, p.z);
+        if (w.contact_skin > 0.0f) contact_far = contact_moved(w, v, p.x, p.y, p.z);
     }
-    if (A) return;
     if (w.contact_skin > 0.0f && v < w.S && w.geom[2 * (size_t)v + 1].w > w.contact_half_limit) contact_far = true;
-    if (__any_sync(FULL, far) && (threadIdx.x & 31) == 0) w.ctl->neighbor_state[0] = 1;
+    if (!A && __any_sync(FULL, far) && (threadIdx.x & 31) == 0) w.ctl->neighbor_state[0] = 1;
     if (__any_sync(FULL, contact_far) && (threadIdx.x & 31) == 0) w.ctl->contact_state[0] = 1;
 }
 
@@ -667,7 +666,10 @@ __global__ void rb_finish_kernel(WorldDev w) {
     if (w.ctl->neighbor_state[0] == 0) return;
     for (uint32_t p = threadIdx.x; p < w.P; p += blockDim.x) finish_rebuild(w.ctl + 1 + p);
     __syncthreads();
-    if (threadIdx.x == 0) w.ctl->neighbor_state[0] = 0;
+    if (threadIdx.x == 0) {
+        w.ctl->neighbor_state[0] = 0;
+        w.ctl->contact_state[0] = 1;  // the arena's one refresh flag: new lists somewhere
+    }
 }
 
 // ---------------------------------------------------------------- contact pass
@@ -819,7 +821,7 @@ enum { CONTACT_FULL = 0, CONTACT_REFRESH = 1, CONTACT_LISTED = 2 };
 // bit those of the full list. (The minimum image cannot change within the
 // window while every half length stays below contact_half_limit, which the
 // update kernel checks with the displacements.)
-// In an arena (A, full lists only) every lane looks up its segment's
+// In an arena (A) every lane looks up its segment's
 // specimen: grid and line margin for its candidates, whether the specimen is
 // still active, and the specimen whose gate its penetration feeds.
 template <int MODE, bool A = false>
@@ -1006,7 +1008,8 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
                         hit = contact_solve(home, __float_as_uint(eb.w), ea.w, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z,
                                             sp.correction_fraction, sp.contact_aggregation, pt);
                     if (MODE == CONTACT_REFRESH)
-                        keep = within_contact_skin(home, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z, ea.w, cskin, line_eps_world);
+                        keep = within_contact_skin(home, ea.x, ea.y, ea.z, eb.x, eb.y, eb.z, ea.w, cskin,
+                                                   A ? w.specs[lane_spec[A ? warp : 0][h]].line_eps : line_eps_world);
                 }
                 if (MODE == CONTACT_REFRESH) {
                     // Append the kept entries to the batch's chunk in queue
@@ -1081,6 +1084,9 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
                 w.contact_count[base + lane] = !listed ? CONTACT_USE_SCAN
                                                : (spilled_owners >> lane) & 1u ? CONTACT_USE_VERLET
                                                                                : kept[lane];
+            else if (A && in_range)  // a stopped specimen's slot: no list in this chunk; its Verlet list
+                                     // (or the cell scan) serves it until a refresh after it resumes
+                w.contact_count[base + lane] = w.nbr_count[segment] <= block ? CONTACT_USE_VERLET : CONTACT_USE_SCAN;
         }
         uint32_t spill = __ballot_sync(FULL, valid && !listed);
         while (spill) {
@@ -1145,6 +1151,10 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     if (threadIdx.x == 0) {
         w.ctl->control[0] = any_active ? 1u : 0u;
         w.ctl->done_blocks = 0;
+        if (MODE == CONTACT_REFRESH) {
+            w.ctl->contact_state[0] = 0;
+            w.ctl->contact_state[1] += 1;
+        }
         __threadfence();
     }
 }
@@ -1613,7 +1623,7 @@ __global__ void __launch_bounds__(128, 8) fiber_lanes_kernel(WorldDev w, StepPar
     uint32_t smax = 0, cmax = 0;
     bool far = false;
     bool contact_far = false;
-    const bool contact_lists = !A && w.contact_skin > 0.0f;
+    const bool contact_lists = w.contact_skin > 0.0f;
     for (uint32_t batch = blockIdx.x * wpb + wib; batch * FPW < w.FA; batch += gridDim.x * wpb) {
         const uint32_t slot = batch * FPW + group;
         uint32_t mine = slot < w.FA ? w.fiber_order[slot] : TGL_NONE;
@@ -1860,7 +1870,10 @@ __global__ void __launch_bounds__(128, 8) fiber_lanes_kernel(WorldDev w, StepPar
         }
         __syncwarp();
     }
-    if (A) return;
+    if (A) {  // one contact-list refresh flag for the whole arena
+        if (__any_sync(FULL, contact_far) && lane == 0) w.ctl->contact_state[0] = 1;
+        return;
+    }
     smax = warp_max_u32(smax);
     cmax = warp_max_u32(cmax);
     const bool any_far = __any_sync(FULL, far);
@@ -1887,7 +1900,7 @@ __global__ void __launch_bounds__(256) rigid_kernel(WorldDev w, StepParams sp) {
     if (w.ctl->control[0] == 0) return;
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    const bool contact_lists = !A && w.contact_skin > 0.0f;
+    const bool contact_lists = w.contact_skin > 0.0f;
     uint32_t smax = 0, cmax = 0;
     bool far = false, contact_far = false;
     for (uint32_t k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); k < w.FA; k += warps) {
@@ -2008,7 +2021,10 @@ __global__ void __launch_bounds__(256) rigid_kernel(WorldDev w, StepParams sp) {
             far = false;
         }
     }
-    if (A) return;
+    if (A) {  // one contact-list refresh flag for the whole arena
+        if (__any_sync(FULL, contact_far) && lane == 0) w.ctl->contact_state[0] = 1;
+        return;
+    }
     smax = warp_max_u32(smax);
     cmax = warp_max_u32(cmax);
     const bool any_far = __any_sync(FULL, far);
@@ -2274,6 +2290,11 @@ int launch_step_condition(const WorldDev &w, cudaGraphConditionalHandle rebuild,
 
 int launch_contact(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, bool gate, cudaStream_t st) {
     if (lp.arena) {
+        if (gate && lp.contact_lists) {
+            contact_kernel<CONTACT_LISTED, true><<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, 1, lp.line_eps);
+            contact_kernel<CONTACT_REFRESH, true><<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, 1, lp.line_eps);
+            return 2;
+        }
         contact_kernel<CONTACT_FULL, true><<<lp.contact_blocks, CONTACT_WARPS * 32, 0, st>>>(w, sp, gate ? 1 : 0,
                                                                                             lp.line_eps);
         return 1;

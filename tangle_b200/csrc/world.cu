@@ -168,8 +168,12 @@ struct tgl_world {
     double *metric_partials_d = nullptr;
     float *metric_out_d = nullptr;
     uint64_t allocated_cells = 0;
-    float maximum_radius = 0.0f, maximum_length = 0.0f;
+    float maximum_radius = 0.0f, maximum_length = 0.0f;  // over every specimen
     float contact_fraction = 0.0f;  // contact-list skin over the neighbor skin (0: lists off)
+    // What sizes the contact skin: the smallest neighbor skin and every
+    // specimen's grid (one of each for a single world).
+    float contact_skin_base = 0.0f;
+    std::vector<Grid> contact_grids;
 
     ~tgl_world() {
         for (auto &kv : graphs) destroy_entry(kv.second);
@@ -664,6 +668,8 @@ int prepare_specimen(const tgl_packed *pk, const tgl_cell_list_config *cl, float
 
 namespace {
 
+void set_contact_skin(tgl_world *w, float fraction);
+
 // Device world from prepared specimens: one (a single world) or several (an
 // arena, relaxed together with a gate per specimen).
 int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl, bool arena, tgl_world **out) {
@@ -797,30 +803,28 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
     w->allocated_cells = C;
     w->maximum_radius = h0.maximum_radius;
     w->maximum_length = h0.maximum_length;
+    w->contact_skin_base = h0.skin;
+    w->contact_grids.clear();
+    for (const HostSpecimen &h : hosts) {
+        w->maximum_radius = std::max(w->maximum_radius, h.maximum_radius);
+        w->maximum_length = std::max(w->maximum_length, h.maximum_length);
+        w->contact_skin_base = std::min(w->contact_skin_base, h.skin);
+        w->contact_grids.push_back(h.grid);
+    }
     d.block = block;
     d.max_fiber = max_fiber;
     d.skin = skin;
     d.grid = grid;
     // Contact lists: on by default at a tenth of the skin (TGL_CONTACT_SKIN
-    // sets the fraction, 0 turns them off). A pair's minimum image must stay
-    // fixed while its vertices move less than the contact skin: with every
-    // half length below H, pairs within reach + contact skin are closer than
-    // half a box length on every periodic axis, so
-    // H = (L/2 - 2 r_max - contact_skin) / 2, less 0.1 %.
+    // sets the fraction, 0 turns them off); in an arena one contact skin
+    // serves every specimen (a tenth of the smallest neighbor skin) and one
+    // refresh flag covers them all.
     float contact_fraction = 0.1f;
     if (const char *env = std::getenv("TGL_CONTACT_SKIN")) contact_fraction = std::strtof(env, nullptr);
-    if (arena) contact_fraction = 0.0f;  // the arena's contact pass reads the Verlet lists
-    if (!(contact_fraction > 0.0f && contact_fraction <= 1.0f) || !(skin > 0.0f)) contact_fraction = 0.0f;
-    d.contact_skin = contact_fraction * skin;
-    d.contact_half_limit = INFINITY;
-    for (int a = 0; a < 3; ++a)
-        if (grid.periodic[a])
-            d.contact_half_limit = std::fmin(
-                d.contact_half_limit, 0.999f * 0.5f * (0.5f * grid.length[a] - 2.0f * maximum_radius - d.contact_skin));
-    float longest_half = 0.5f * maximum_length;
-    if (!(d.contact_half_limit > longest_half)) d.contact_skin = 0.0f;  // no room: full lists every pass
+    if (!(contact_fraction > 0.0f && contact_fraction <= 1.0f) || !(w->contact_skin_base > 0.0f))
+        contact_fraction = 0.0f;
+    set_contact_skin(w, contact_fraction);
     d.contact_block = d.contact_skin > 0.0f ? CONTACT_BLOCK : 0u;
-    w->contact_fraction = d.contact_skin > 0.0f ? contact_fraction : 0.0f;
     int rc = 0;
     float4 *seg_static_d, *vtx_static_d;
     uint32_t *seg_v0_d, *fiber_s0_d, *pinned_d, *fiber_order_d;
@@ -1135,12 +1139,13 @@ int tgl_contact_list_info(tgl_world *w, float *contact_skin, uint32_t *block, ui
 }
 
 int tgl_debug_contact_lists(tgl_world *w, uint32_t *counts, uint32_t *lists) {
-    if (!w || !counts || !lists) return set_error(TGL_ERR_INVALID, "null argument");
+    if (!w || !counts) return set_error(TGL_ERR_INVALID, "null argument");
     if (!w->dev.contact_block) return set_error(TGL_ERR_UNSUPPORTED, "contact lists are off for this world");
     const size_t S = w->dev.S, padded = (S + 31) / 32 * 32;
     TGL_CUDA(cudaMemcpyAsync(counts, w->dev.contact_count, S * 4ull, cudaMemcpyDeviceToHost, w->stream));
-    TGL_CUDA(cudaMemcpyAsync(lists, w->dev.contact_list, padded * w->dev.contact_block * 4ull, cudaMemcpyDeviceToHost,
-                             w->stream));
+    if (lists)
+        TGL_CUDA(cudaMemcpyAsync(lists, w->dev.contact_list, padded * w->dev.contact_block * 4ull,
+                                 cudaMemcpyDeviceToHost, w->stream));
     TGL_CUDA(cudaStreamSynchronize(w->stream));
     return 0;
 }
@@ -1667,6 +1672,7 @@ int tgl_world_compact_cell(tgl_world *w, const float new_lower[3], const float n
         d.grid.inv_length[a] = 1.0f / extent;
     }
     d.C = (uint32_t)C;
+    w->contact_grids.assign(1, d.grid);
     // The contact lists' single-image bound follows the new box edges.
     if (d.contact_skin > 0.0f) {
         d.contact_half_limit = INFINITY;
@@ -1777,13 +1783,19 @@ namespace {
 // room for turns the lists off.
 void set_contact_skin(tgl_world *w, float fraction) {
     WorldDev &d = w->dev;
-    d.contact_skin = fraction > 0.0f ? fraction * d.skin : 0.0f;
+    d.contact_skin = fraction > 0.0f ? fraction * w->contact_skin_base : 0.0f;
+    // A pair's minimum image must stay fixed while its vertices move less
+    // than the contact skin: with every half length below H, pairs within
+    // reach + contact skin are closer than half a box length on every
+    // periodic axis, so H = (L/2 - 2 r_max - contact_skin) / 2, less 0.1 %,
+    // over every specimen's box.
     d.contact_half_limit = INFINITY;
-    for (int a = 0; a < 3; ++a)
-        if (d.grid.periodic[a])
-            d.contact_half_limit = std::fmin(
-                d.contact_half_limit, 0.999f * 0.5f * (0.5f * d.grid.length[a] - 2.0f * w->maximum_radius - d.contact_skin));
-    if (!(d.contact_half_limit > 0.5f * w->maximum_length)) d.contact_skin = 0.0f;
+    for (const Grid &g : w->contact_grids)
+        for (int a = 0; a < 3; ++a)
+            if (g.periodic[a])
+                d.contact_half_limit = std::fmin(
+                    d.contact_half_limit, 0.999f * 0.5f * (0.5f * g.length[a] - 2.0f * w->maximum_radius - d.contact_skin));
+    if (!(d.contact_half_limit > 0.5f * w->maximum_length)) d.contact_skin = 0.0f;  // no room: full lists every pass
     w->contact_fraction = d.contact_skin > 0.0f ? fraction : 0.0f;
 }
 

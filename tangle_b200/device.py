@@ -683,6 +683,14 @@ class DeviceWorld(FormationHooks):
                                                     ctypes.byref(refreshes)))
         return {"skin": float(skin.value), "block": int(block.value), "refreshes": int(refreshes.value)}
 
+    def debug_contact_states(self) -> np.ndarray:
+        """The contact-list state of every cell-list slot [S]: its list length,
+        CONTACT_USE_VERLET or 0xFFFFFFFF (tgl_debug_contact_lists without the
+        chunks)."""
+        states = np.empty(self.segment_count, dtype=np.uint32)
+        self._check(self._lib.tgl_debug_contact_lists(self._handle, _ptr(states), None))
+        return states
+
     def debug_contact_lists(self):
         """Contact lists by cell-list slot: counts [S] and a list per slot.
         A list of None (count CONTACT_USE_VERLET) marks a slot whose list ran

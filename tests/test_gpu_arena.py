@@ -91,3 +91,42 @@ def test_batched_generator_arena_runs(cuda_lib):
     per_spec = arena.specimen_statuses(cfg)
     assert len(per_spec) == 6
     assert all(np.isfinite(s.max_penetration) for s in per_spec)
+
+
+def test_arena_contact_lists_keep_every_specimen_bit_for_bit(cuda_lib):
+    """The arena's contact lists (one contact skin for all specimens, one
+    refresh flag) leave each specimen's positions those of the same
+    specimen relaxed alone, across refreshes and rebuilds."""
+    from tangle_b200.device import DeviceWorld
+
+    assemblies = batched_specimens(count=6, seed=5, max_fibers=300)
+    packs = [PackedAssembly.from_assembly(a) for a in assemblies]
+    d = min(a.smallest_diameter() for a in assemblies)
+    cfg = RelaxationSettings(penetration_tolerance=1.0e-3 * d, neighbor_capacity=256,
+                             max_list_bytes=1 << 30).to_config(d)
+    fixed = RelaxationConfig(**{**cfg.__dict__, "force_full_iterations": True})
+    arena = DeviceWorld.arena(packs, fixed.cell_list, fixed.max_step)
+    assert arena.contact_list_info()["block"] > 0
+    singles = [DeviceWorld(p, fixed.cell_list, fixed.max_step) for p in packs]
+    for batch in (9, 23, 31):
+        arena.run_batch(fixed, batch)
+        for w in singles:
+            w.run_batch(fixed, batch)
+    assert arena.contact_list_info()["refreshes"] > 1
+    for i, (got, w) in enumerate(zip(arena.specimen_positions(), singles)):
+        np.testing.assert_array_equal(got.view(np.uint32), w.download_positions().view(np.uint32),
+                                      err_msg=f"specimen {i}")
+    # Gated batches: specimens stop at their own iteration (their slots then
+    # read the Verlet lists), and the next batch resumes them.
+    gated = RelaxationConfig(**{**cfg.__dict__, "penetration_tolerance": 0.05 * d})
+    for batch in (40, 40, 40):
+        arena.run_batch(gated, batch)
+        last = [w.run_batch(gated, batch) for w in singles]
+        statuses = arena.specimen_statuses(gated)
+        assert [s.total_iterations for s in statuses] == [s.total_iterations for s in last]
+        assert [s.converged for s in statuses] == [s.converged for s in last]
+    for i, (got, w) in enumerate(zip(arena.specimen_positions(), singles)):
+        np.testing.assert_array_equal(got.view(np.uint32), w.download_positions().view(np.uint32),
+                                      err_msg=f"specimen {i} after the gated batches")
+    for w in [arena] + singles:
+        w.close()

@@ -113,7 +113,8 @@ def test_search_on_an_arena_leaves_its_state_unchanged(cuda_lib):
     for world in (tuned, plain):
         world.run_batch(fixed, 19)
     params, report = tuned.autotune_trials(fixed, 8)
-    assert report["trials"] >= 6 and params["contact_skin_fraction"] == 0.0
+    assert report["trials"] >= 6  # the arena's contact lists are searched too
+    assert any(abs(params["contact_skin_fraction"] - v) < 1.0e-6 for v in (0.05, 0.1, 0.15, 0.25))
     tuned.run_batch(fixed, 31)
     plain.run_batch(fixed, 31)
     np.testing.assert_array_equal(tuned.download_positions().view(np.uint32),
