@@ -2039,6 +2039,15 @@ __global__ void __launch_bounds__(256) rigid_kernel(WorldDev w, StepParams sp) {
 
 // ---------------------------------------------------------------- host copies
 
+// Raises *flag when any of the n staged floats is not finite (all exponent
+// bits set: an infinity or a NaN).
+__global__ void stage_nonfinite_kernel(const float *xyz, size_t n, unsigned int *flag) {
+    bool bad = false;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        bad |= (__float_as_uint(xyz[i]) & 0x7F800000u) == 0x7F800000u;
+    if (__any_sync(FULL, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
 __global__ void positions_from_stage_kernel(WorldDev w) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x)
         w.pos[v] = make_float4(w.xyz_stage[3 * (size_t)v], w.xyz_stage[3 * (size_t)v + 1],
@@ -2340,6 +2349,11 @@ int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParam
     } else {
         fiber_kernel<<<lp.fiber_blocks, lp.fiber_warps * 32, lp.fiber_smem, st>>>(w, sp);
     }
+    return 1;
+}
+
+int launch_stage_nonfinite(const WorldDev &w, unsigned int *flag, cudaStream_t st) {
+    stage_nonfinite_kernel<<<grid_for(3ull * w.V, 256, 1 << 14), 256, 0, st>>>(w.xyz_stage, 3ull * w.V, flag);
     return 1;
 }
 

@@ -261,6 +261,8 @@ int launch_rebuild_condition(const WorldDev &w, cudaGraphConditionalHandle rebui
 int launch_step_condition(const WorldDev &w, cudaGraphConditionalHandle rebuild, cudaGraphConditionalHandle loop,
                           uint32_t steps, cudaStream_t st);
 int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParams &sp, cudaStream_t st);
+// Sets *flag (device) when a staged coordinate is not finite.
+int launch_stage_nonfinite(const WorldDev &w, unsigned int *flag, cudaStream_t st);
 int launch_positions_from_stage(const WorldDev &w, cudaStream_t st);
 int launch_positions_to_stage(const WorldDev &w, cudaStream_t st);
 int launch_corrections_to_stage(const WorldDev &w, float *corr6, float *pen, cudaStream_t st);

@@ -165,6 +165,7 @@ struct tgl_world {
     uint32_t target_capacity = 0, target_count = 0;
     std::vector<uint32_t> h_target_vertices;
     unsigned int *error_bits_d = nullptr;
+    unsigned int *nonfinite_d = nullptr;  // upload check flag
     double *metric_partials_d = nullptr;
     float *metric_out_d = nullptr;
     uint64_t allocated_cells = 0;
@@ -1094,9 +1095,16 @@ int tgl_upload_positions(tgl_world *w, const float *xyz, size_t len) {
     if (!w || !xyz) return set_error(TGL_ERR_INVALID, "null argument");
     w->warm.counted = false;
     if (len != 3 * (size_t)w->dev.V) return set_error(TGL_ERR_INVALID, "position buffer has the wrong length");
-    for (size_t i = 0; i < len; ++i)
-        if (!std::isfinite(xyz[i])) return set_error(TGL_ERR_INVALID, "positions must be finite");
+    if (!w->nonfinite_d && w->alloc(&w->nonfinite_d, 1)) return TGL_ERR_MEMORY;
+    // The coordinates are checked where they land, in the staging buffer,
+    // before anything the world holds changes (no host pass over them).
     TGL_CUDA(cudaMemcpyAsync(w->dev.xyz_stage, xyz, len * sizeof(float), cudaMemcpyHostToDevice, w->stream));
+    TGL_CUDA(cudaMemsetAsync(w->nonfinite_d, 0, sizeof(unsigned int), w->stream));
+    w->launches += launch_stage_nonfinite(w->dev, w->nonfinite_d, w->stream);
+    unsigned int nonfinite = 0;
+    TGL_CUDA(cudaMemcpyAsync(&nonfinite, w->nonfinite_d, sizeof(unsigned int), cudaMemcpyDeviceToHost, w->stream));
+    TGL_CUDA(cudaStreamSynchronize(w->stream));
+    if (nonfinite) return set_error(TGL_ERR_INVALID, "positions must be finite");
     w->launches += launch_positions_from_stage(w->dev, w->stream);
     TGL_CUDA(cudaStreamSynchronize(w->stream));
     return 0;

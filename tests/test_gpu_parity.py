@@ -124,3 +124,25 @@ def test_admissibility_verdict_is_identical(case, cuda_lib):
     for key in ("max_penetration", "max_curvature_ratio", "max_displacement"):
         a, b = getattr(so, key), getattr(sd, key)
         assert abs(a - b) <= 1.0e-5 * max(abs(a), abs(b), d), (key, a, b)
+
+
+@pytest.mark.parametrize("bad", [np.nan, np.inf, -np.inf])
+def test_upload_rejects_non_finite_coordinates_and_keeps_the_state(bad, cuda_lib):
+    """tgl_upload_positions checks the staged coordinates on the device
+    before the world changes: a NaN or an infinity anywhere is refused with
+    TGL_ERR_INVALID and the positions stay as they were."""
+    from tangle_b200.device import DeviceWorld
+
+    packed = PackedAssembly.from_assembly(cpu_runnable_specimen())
+    dev = DeviceWorld(packed, CellListConfig(), 1.0e-6)
+    before = dev.download_positions()
+    for index in (0, before.size // 2, before.size - 1):
+        xyz = before.copy()
+        xyz[index] = bad
+        with pytest.raises(ValueError, match="finite"):
+            dev.upload_positions(xyz)
+        np.testing.assert_array_equal(dev.download_positions().view(np.uint32), before.view(np.uint32))
+    moved = before + np.float32(1.0e-7)
+    dev.upload_positions(moved)
+    np.testing.assert_array_equal(dev.download_positions().view(np.uint32), moved.view(np.uint32))
+    dev.close()
