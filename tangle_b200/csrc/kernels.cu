@@ -860,16 +860,22 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x)
             w.contact_ref[v] = w.pos[v];
     }
-    // Warps take the batches in slot order from one counter, so the batches
-    // in flight at any moment are a narrow band of neighboring cells whose
-    // candidates' records stay in L2 (a fixed stride lets the warps drift
-    // apart over the pass and widen that band).
+    // One world: warps take the batches in slot order from one counter, so
+    // the batches in flight at any moment are a narrow band of neighboring
+    // cells whose candidates' records stay in L2 (a fixed stride lets the
+    // warps drift apart over the pass and widen that band). An arena keeps
+    // the fixed stride: its hundreds of thousands of batches per pass would
+    // queue on the counter's one address (measured on 512 specimens: 4.26 ms
+    // per pass with the counter against 2.47 ms with the stride, while one
+    // mid-size world's 62 k batches run 0.283 ms against 0.309 ms).
     const auto take_batch = [&]() {
         uint32_t b = 0;
         if (lane == 0) b = atomicAdd(&w.ctl->next_batch, 1u);
         return __shfl_sync(FULL, b, 0) * 32u;
     };
-    for (uint32_t base = take_batch(); base < w.NS; base = take_batch()) {
+    const uint32_t stride = gridDim.x * CONTACT_WARPS * 32u;
+    for (uint32_t base = A ? (blockIdx.x * CONTACT_WARPS + warp) * 32u : take_batch(); base < w.NS;
+         base = A ? base + stride : take_batch()) {
         // Batches follow the cell list's slot order, so the 32 segments of a
         // batch are spatial neighbors and share most of their candidates.
         const bool in_range = base + lane < w.NS;
