@@ -64,6 +64,12 @@ template <bool A> __device__ inline void flag_rebuild(const WorldDev &w, uint32_
     ctl_of<A>(w, p)->neighbor_state[0] = 1;
     if (A) w.ctl->neighbor_state[0] = 1;
 }
+// Raises specimen p's contact-list refresh flag (and, in an arena, the
+// any-specimen one, which lets the refresh pass run).
+template <bool A> __device__ inline void flag_refresh(const WorldDev &w, uint32_t p) {
+    ctl_of<A>(w, p)->contact_state[0] = 1;
+    if (A) w.ctl->contact_state[0] = 1;
+}
 
 // ---------------------------------------------------------------- batch control
 
@@ -84,7 +90,12 @@ __global__ void begin_batch_kernel(WorldDev w) {
     if constexpr (!A) {
         if (threadIdx.x == 0) begin_batch(w.ctl);
     } else {
-        for (uint32_t p = threadIdx.x; p < w.P; p += blockDim.x) begin_batch(w.ctl + 1 + p);
+        for (uint32_t p = threadIdx.x; p < w.P; p += blockDim.x) {
+            begin_batch(w.ctl + 1 + p);
+            // A specimen resumed with a refresh still pending (it stopped
+            // first) gets it in this batch.
+            if (w.ctl[1 + p].contact_state[0]) w.ctl->contact_state[0] = 1;
+        }
         if (threadIdx.x == 0) {
             w.ctl->control[0] = 1;  // some specimen may run; the first gate refines it
             w.ctl->done_blocks = 0;
@@ -115,10 +126,17 @@ __global__ void flag_displacement_kernel(WorldDev w) {
         float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
         far = dx * dx + dy * dy + dz * dz > md * md;
         if (A && far) flag_rebuild<A>(w, spec);
-        if (w.contact_skin > 0.0f) contact_far = contact_moved(w, v, p.x, p.y, p.z);
+        if (w.contact_skin > 0.0f && contact_moved(w, v, p.x, p.y, p.z)) {
+            contact_far = true;
+            if (A) flag_refresh<A>(w, spec);
+        }
     }
-    if (w.contact_skin > 0.0f && v < w.S && w.geom[2 * (size_t)v + 1].w > w.contact_half_limit) contact_far = true;
-    if (!A && __any_sync(FULL, far) && (threadIdx.x & 31) == 0) w.ctl->neighbor_state[0] = 1;
+    if (w.contact_skin > 0.0f && v < w.S && w.geom[2 * (size_t)v + 1].w > w.contact_half_limit) {
+        contact_far = true;
+        if (A) flag_refresh<A>(w, spec_of_seg<A>(w, v));
+    }
+    if (A) return;
+    if (__any_sync(FULL, far) && (threadIdx.x & 31) == 0) w.ctl->neighbor_state[0] = 1;
     if (__any_sync(FULL, contact_far) && (threadIdx.x & 31) == 0) w.ctl->contact_state[0] = 1;
 }
 
@@ -838,8 +856,12 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     __shared__ uint32_t warp_max[CONTACT_WARPS];
     __shared__ int is_last;
     if (gate && w.ctl->control[0] == 0) return;
+    // One world refreshes everything or nothing. In an arena a listed pass
+    // always runs (for the specimens whose lists hold) and a refresh pass
+    // when some specimen's flag is up (for those specimens).
     if (MODE == CONTACT_REFRESH && w.ctl->contact_state[0] == 0) return;
-    if (MODE == CONTACT_LISTED && w.ctl->contact_state[0] != 0) return;
+    if (!A && MODE == CONTACT_LISTED && w.ctl->contact_state[0] != 0) return;
+    const bool refresh_follows = A && MODE == CONTACT_LISTED && w.ctl->contact_state[0] != 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t block = w.block;
     const uint32_t cblock = w.contact_block;
@@ -856,9 +878,15 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     uint32_t thread_max = 0;
     const uint64_t geom_policy = make_keep_policy();
     if (MODE == CONTACT_REFRESH) {
-        // The snapshot the next passes measure displacement against.
-        for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x)
+        // The snapshot the next passes measure displacement against (in an
+        // arena, of the specimens this pass refreshes).
+        for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.V; v += gridDim.x * blockDim.x) {
+            if (A) {
+                const Control *c = ctl_of<A>(w, spec_of_vtx<A>(w, v));
+                if (c->control[0] == 0 || c->contact_state[0] == 0) continue;
+            }
             w.contact_ref[v] = w.pos[v];
+        }
     }
     // One world: warps take the batches in slot order from one counter, so
     // the batches in flight at any moment are a narrow band of neighboring
@@ -881,12 +909,18 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         const bool in_range = base + lane < w.NS;
         const uint32_t segment = in_range ? w.cell_segments[base + lane] : 0u;
         const uint32_t my_spec = A && in_range ? spec_of_seg<A>(w, segment) : 0u;
-        // Segments of an arena specimen whose gate has stopped it are skipped.
-        const bool valid = in_range && (!A || ctl_of<A>(w, my_spec)->control[0] != 0);
+        // Segments of an arena specimen whose gate has stopped it are
+        // skipped; of the others, a listed pass takes those whose specimen's
+        // lists hold and a refresh pass those whose specimen's flag is up.
+        const bool alive = in_range && (!A || ctl_of<A>(w, my_spec)->control[0] != 0);
+        const bool flagged = A && MODE != CONTACT_FULL && alive && ctl_of<A>(w, my_spec)->contact_state[0] != 0;
+        const bool valid = MODE == CONTACT_LISTED ? alive && !flagged : MODE == CONTACT_REFRESH && A ? flagged : alive;
         // A listed pass reads the slot's contact-list state (coalesced), and
         // the segment's Verlet count only where its contact list did not fit
-        // the batch's chunk; the other passes walk the Verlet lists.
-        const uint32_t cstate = MODE == CONTACT_LISTED && valid ? w.contact_count[base + lane] : 0u;
+        // the batch's chunk; the other passes walk the Verlet lists. Every
+        // slot with a list in the chunk counts toward the others' offsets,
+        // whoever takes it in this pass.
+        const uint32_t cstate = MODE == CONTACT_LISTED && in_range ? w.contact_count[base + lane] : 0u;
         uint32_t count = 0u;
         if (MODE != CONTACT_LISTED) count = valid ? w.nbr_count[segment] : 0u;
         else if (valid && cstate == CONTACT_USE_VERLET) count = w.nbr_count[segment];
@@ -899,7 +933,7 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
             // lane order: a lane's list starts after the lists of the lanes
             // before it that read the chunk.
             const bool chunked = listed && cstate != CONTACT_USE_VERLET;  // cstate <= 32 * cblock
-            uint32_t before = chunked ? cstate : 0u;
+            uint32_t before = in_range && cstate < CONTACT_USE_VERLET ? cstate : 0u;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t t = __shfl_up_sync(FULL, before, o);
@@ -1086,12 +1120,16 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
         }
         if (MODE == CONTACT_REFRESH) {
             spilled_owners = __reduce_or_sync(FULL, spilled_owners);
+            const bool batch_refreshed = __any_sync(FULL, valid);
             if (valid)
                 w.contact_count[base + lane] = !listed ? CONTACT_USE_SCAN
                                                : (spilled_owners >> lane) & 1u ? CONTACT_USE_VERLET
                                                                                : kept[lane];
-            else if (A && in_range)  // a stopped specimen's slot: no list in this chunk; its Verlet list
-                                     // (or the cell scan) serves it until a refresh after it resumes
+            else if (A && in_range && batch_refreshed)
+                // The chunk was rewritten for the refreshed slots: a slot of
+                // another specimen in the batch (stopped, or with lists that
+                // hold) has no list in it now; its Verlet list (or the cell
+                // scan) serves it until its own specimen's next refresh.
                 w.contact_count[base + lane] = w.nbr_count[segment] <= block ? CONTACT_USE_VERLET : CONTACT_USE_SCAN;
         }
         uint32_t spill = __ballot_sync(FULL, valid && !listed);
@@ -1124,9 +1162,11 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     if (!is_last) return;
     if (threadIdx.x == 0) {  // every warp of every block is past its last batch
         w.ctl->next_batch = 0;
-        if (!gate) w.ctl->done_blocks = 0;
+        if (!gate || refresh_follows) w.ctl->done_blocks = 0;
     }
-    if (!gate) return;
+    // In an arena whose refresh pass runs next, that pass's last block runs
+    // the gates, over both passes' maxima.
+    if (!gate || refresh_follows) return;
     if (!A) {
         if (threadIdx.x == 0) {
             __threadfence();
@@ -1150,6 +1190,10 @@ __global__ void __launch_bounds__(256, 3) contact_kernel(WorldDev w, StepParams 
     for (uint32_t p = threadIdx.x; p < w.P; p += blockDim.x) {
         Control *c = w.ctl + 1 + p;
         if (c->control[0] == 0) continue;
+        if (MODE == CONTACT_REFRESH && c->contact_state[0]) {  // refreshed in this pass
+            c->contact_state[0] = 0;
+            c->contact_state[1] += 1;
+        }
         assess_reduced_metrics(c, sp, w.ctl->cell_overflow);
         if (c->control[0]) any_active = 1;
     }
@@ -1866,20 +1910,20 @@ __global__ void __launch_bounds__(128, 8) fiber_lanes_kernel(WorldDev w, StepPar
             if (A) {
                 cmax = warp_max_u32(cmax);
                 const bool fiber_far = __any_sync(FULL, far);
+                const bool fiber_contact_far = __any_sync(FULL, contact_far);
                 if (lane == 0) {
                     if (cmax) atomicMax(&ctl_of<A>(w, fspec)->acc[2], cmax);
                     if (fiber_far) flag_rebuild<A>(w, fspec);
+                    if (fiber_contact_far) flag_refresh<A>(w, fspec);
                 }
                 cmax = 0;
                 far = false;
+                contact_far = false;
             }
         }
         __syncwarp();
     }
-    if (A) {  // one contact-list refresh flag for the whole arena
-        if (__any_sync(FULL, contact_far) && lane == 0) w.ctl->contact_state[0] = 1;
-        return;
-    }
+    if (A) return;
     smax = warp_max_u32(smax);
     cmax = warp_max_u32(cmax);
     const bool any_far = __any_sync(FULL, far);
@@ -2018,19 +2062,19 @@ __global__ void __launch_bounds__(256) rigid_kernel(WorldDev w, StepParams sp) {
         if (A) {
             cmax = warp_max_u32(cmax);
             const bool fiber_far = __any_sync(FULL, far);
+            const bool fiber_contact_far = __any_sync(FULL, contact_far);
             if (lane == 0) {
                 if (smax) atomicMax(&ctl_of<A>(w, spec)->acc[1], smax);
                 if (cmax) atomicMax(&ctl_of<A>(w, spec)->acc[2], cmax);
                 if (fiber_far) flag_rebuild<A>(w, spec);
+                if (fiber_contact_far) flag_refresh<A>(w, spec);
             }
             smax = cmax = 0;
             far = false;
+            contact_far = false;
         }
     }
-    if (A) {  // one contact-list refresh flag for the whole arena
-        if (__any_sync(FULL, contact_far) && lane == 0) w.ctl->contact_state[0] = 1;
-        return;
-    }
+    if (A) return;
     smax = warp_max_u32(smax);
     cmax = warp_max_u32(cmax);
     const bool any_far = __any_sync(FULL, far);

@@ -791,8 +791,6 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
         block = (uint32_t)std::min<uint64_t>(cl->neighbor_capacity, std::max<uint64_t>(w->neighbor_slots / S, 1));
     }
     const float skin = h0.skin;
-    const float maximum_radius = h0.maximum_radius;
-    const float maximum_length = h0.maximum_length;
     const Grid grid = h0.grid;
     WorldDev &d = w->dev;
     d.V = V;
