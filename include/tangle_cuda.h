@@ -130,8 +130,10 @@ void tgl_world_destroy(tgl_world *world);
  * (its convergence mask), as a batch of its own world would, and the batch
  * status covers all of them (largest counts and metrics; converged when all
  * are). One neighbor-list block serves every specimen: the capacity within
- * max_list_bytes (8 GiB when 0). Contact lists are off; fibers of at most
- * 256 vertices. Checkpoints, residuals and the warm start take single
+ * max_list_bytes (8 GiB when 0). Contact lists are on as in a single world
+ * (TGL_CONTACT_SKIN), one contact skin for all specimens (a tenth of the
+ * smallest neighbor skin) and a refresh flag per specimen; fibers of at
+ * most 256 vertices. Checkpoints, residuals and the warm start take single
  * worlds. */
 int tgl_arena_create(const tgl_packed *specimens, uint32_t count, const tgl_cell_list_config *cell_list,
                      float max_step, tgl_world **out);
