@@ -279,36 +279,34 @@ def update_bytes(nodes: int, segments: int, contact_lists: bool) -> float:
     return float(nodes) * (72.0 + (16.0 if contact_lists else 0.0)) + float(segments) * 68.0
 
 
-def issue_bound(profile: str, avg_launch_s: float, clocks: dict, scale: float = 1.0, refresh_share=None):
-    """A kernel against its instruction-issue bound: the warp instructions
-    of one launch (the committed full-size ncu capture, times `scale` --
-    the node count over the capture's; for the contact pass listed and
-    refresh passes weighted by their share) over the launch's mean CUDA-event
-    duration, against 4 warp instructions per clock on every SM at the
-    median SM clock of the timed region. None without the capture."""
-    import torch
-
+def issue_bound(profile: str, refresh_share=None):
+    """A kernel against its instruction-issue bound, from the committed
+    full-size ncu capture (one pass per launch): the warp instructions of a
+    launch over the same launch's duration, against 4 warp instructions per
+    clock on each of the 148 SMs at the 1,965 MHz the capture ran at; for the
+    contact pass, listed and refresh passes weighted by their share of this
+    run's passes. Both figures come from the same launches (the capture's
+    state, early in the trajectory), so the fraction does not mix states
+    with this run's timing. None without the capture."""
     path = os.path.join(ROOT, "profiles", profile)
     try:
         with open(path) as fh:
             data = json.load(fh)
         if refresh_share is None:
             inst = float(data["warp_instructions_per_launch"])
+            us = float(data["capture_us_per_launch"])
         else:
             inst = (refresh_share * float(data["warp_instructions_per_refresh_pass"]) +
                     (1.0 - refresh_share) * float(data["warp_instructions_per_listed_pass"]))
+            us = (refresh_share * float(data["capture_us_per_refresh_pass"]) +
+                  (1.0 - refresh_share) * float(data["capture_us_per_listed_pass"]))
+        peak = 4.0 * 148 * 1965.0e6
     except (OSError, KeyError, ValueError):
         return None
-    inst *= scale
-    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
-    if not mhz or avg_launch_s <= 0:
-        return None
-    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-    peak = 4.0 * sms * float(mhz) * 1.0e6
-    achieved = inst / avg_launch_s
+    achieved = inst / (us * 1.0e-6)
     return {"achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
-            "warp_instructions_per_launch": inst, "sm_mhz": float(mhz), "sms": sms,
-            "source": f"profiles/{profile} (ncu smsp__inst_executed.sum, full size)"}
+            "warp_instructions_per_launch": inst, "capture_us_per_launch": us,
+            "source": f"profiles/{profile} (ncu smsp__inst_executed.sum and gpu__time_duration.sum, full size)"}
 
 
 def update_traffic(nodes: int):
@@ -760,8 +758,7 @@ def run_cuda(args):
                         "contact_passes": contact_passes, "refresh_passes": refreshes,
                         "contact_skin_m": contact_info["skin"]}
     if not batched and contact_info["block"] > 0:
-        roofline_contact["issue_bound"] = issue_bound("contact_traffic.json", avg_contact_s, clock_summary,
-                                                      nodes / 1997480.0, refresh_share)
+        roofline_contact["issue_bound"] = issue_bound("contact_traffic.json", refresh_share)
     # Roofline of the fiber update, the largest kernel (about 55 % of the
     # step): its algorithmic bytes per launch over its mean duration.
     segments = world.segment_count
@@ -775,7 +772,7 @@ def run_cuda(args):
                 "algorithmic_bytes_per_launch": update_algorithmic, "avg_launch_ms": avg_update_s * 1000.0,
                 "launches": updates}
     if not batched:
-        roofline["issue_bound"] = issue_bound("update_traffic.json", avg_update_s, clock_summary, nodes / 1997480.0)
+        roofline["issue_bound"] = issue_bound("update_traffic.json")
 
     # End to end through the public API with pinned host buffers: the timed
     # steps again, from the same start state, each step uploading the

@@ -1984,7 +1984,7 @@ int tgl_autotune(tgl_world *w, const tgl_relax_config *config, uint32_t trial_it
     const bool lanes = w->lp.fiber_lanes && config->motion_model == 0;
     const uint32_t lane_choices[] = {2, 4, 8, 32};
     const uint32_t block_choices[] = {1, 2, 3};
-    const uint32_t chunk_choices[] = {1024, 2048, 3072, 4096};
+    const uint32_t chunk_choices[] = {1024, 1536, 2048, 3072, 4096};
     const float skin_choices[] = {0.05f, 0.1f, 0.15f, 0.25f};
     const uint32_t wpb_choices[] = {1, 2, 4};
     // Coordinate descent: each parameter in turn over its candidates, the

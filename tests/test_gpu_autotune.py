@@ -83,7 +83,7 @@ def test_search_leaves_the_world_state_unchanged(cuda_lib, tmp_path):
     assert not result["cached"] and result["report"]["trials"] >= 8
     p = result["params"]
     assert p["lanes_per_fiber"] in (2, 4, 8, 32) and p["contact_blocks_per_sm"] in (1, 2, 3)
-    assert p["build_chunk"] in (1024, 2048, 3072, 4096) and p["update_warps_per_block"] in (1, 2, 4)
+    assert p["build_chunk"] in (1024, 1536, 2048, 3072, 4096) and p["update_warps_per_block"] in (1, 2, 4)
     assert any(abs(p["contact_skin_fraction"] - v) < 1.0e-6 for v in (0.05, 0.1, 0.15, 0.25))
     assert result["report"]["best_ms"] <= result["report"]["default_ms"]
     a, b = tuned.run_batch(fixed, 41), plain.run_batch(fixed, 41)
