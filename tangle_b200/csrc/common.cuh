@@ -234,6 +234,9 @@ struct Control {
     uint32_t rebuild_bodies;
     // Steps a looped batch graph has begun (its WHILE node's counter).
     uint32_t loop_step;
+    // Launches of the update's fiber-ranking kernel (it ranks every
+    // period-th launch).
+    uint32_t order_tick;
 };
 
 }  // namespace tgl

@@ -1647,6 +1647,69 @@ __device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float ex
     P[t + 2] = c;
 }
 
+// Order of the grouped-lane update's fibers. A warp's lane groups step
+// through their curvature sweeps together, so a warp takes as many rounds as
+// its slowest fiber. Every `period` launches of this kernel, the first FA
+// entries of fiber_order are ranked by the rounds each fiber's sweeps took at
+// its last update, most first, into update_order: a warp's fibers then need
+// about as many rounds as each other, and the heaviest warps start first.
+// Any order gives the same positions: a fiber's update reads and writes only
+// its own vertices and segments, and its maxima are order-free integer
+// maxima. Within one rank the order is whatever the shared-memory counters
+// hand out. One block of 1024 threads: a counting sort over ORDER_RANKS
+// ranks (rounds at or above the last rank share it).
+constexpr int ORDER_RANKS = 4096;
+constexpr int ORDER_THREADS = 1024;
+__global__ void __launch_bounds__(ORDER_THREADS) order_by_rounds_kernel(WorldDev w, uint32_t period) {
+    if (w.ctl->control[0] == 0) return;
+    const uint32_t tick = w.ctl->order_tick;
+    __syncthreads();
+    if (threadIdx.x == 0) w.ctl->order_tick = tick + 1u;
+    if (tick % period != 0u) return;
+    __shared__ uint32_t start[ORDER_RANKS];
+    __shared__ uint32_t warp_total[ORDER_THREADS / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const auto rank_of = [&](uint32_t f) { return ORDER_RANKS - 1 - (int)min(w.fiber_rounds[f], ORDER_RANKS - 1u); };
+    for (int i = tid; i < ORDER_RANKS; i += ORDER_THREADS) start[i] = 0;
+    __syncthreads();
+    for (uint32_t k = tid; k < w.FA; k += ORDER_THREADS) atomicAdd(&start[rank_of(w.fiber_order[k])], 1u);
+    __syncthreads();
+    // Exclusive scan of the counts: ORDER_RANKS / ORDER_THREADS per thread.
+    constexpr int PER = ORDER_RANKS / ORDER_THREADS;
+    uint32_t count[PER], sum = 0;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) sum += (count[j] = start[tid * PER + j]);
+    uint32_t inclusive = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, inclusive, o);
+        if (lane >= o) inclusive += v;
+    }
+    if (lane == 31) warp_total[warp] = inclusive;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t t = warp_total[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(FULL, t, o);
+            if (lane >= o) t += v;
+        }
+        warp_total[lane] = t;
+    }
+    __syncthreads();
+    uint32_t base = inclusive - sum + (warp > 0 ? warp_total[warp - 1] : 0u);
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        start[tid * PER + j] = base;
+        base += count[j];
+    }
+    __syncthreads();
+    for (uint32_t k = tid; k < w.FA; k += ORDER_THREADS) {
+        const uint32_t f = w.fiber_order[k];
+        w.update_order[atomicAdd(&start[rank_of(f)], 1u)] = f;
+    }
+}
+
 // Everything after the gate for 32/LPF fibers per warp (fibers of at most
 // 256 vertices), LPF lanes per fiber in the curvature sweeps. The warp stages
 // the fibers in shared memory and runs the internal stretch/bend passes
@@ -1682,7 +1745,7 @@ __global__ void __launch_bounds__(128, 8) fiber_lanes_kernel(WorldDev w, StepPar
     const bool contact_lists = w.contact_skin > 0.0f;
     for (uint32_t batch = blockIdx.x * wpb + wib; batch * FPW < w.FA; batch += gridDim.x * wpb) {
         const uint32_t slot = batch * FPW + group;
-        uint32_t mine = slot < w.FA ? w.fiber_order[slot] : TGL_NONE;
+        uint32_t mine = slot < w.FA ? w.update_order[slot] : TGL_NONE;
         if (A && mine != TGL_NONE && ctl_of<A>(w, spec_of_fiber<A>(w, mine))->control[0] == 0) mine = TGL_NONE;
         for (int j = 0; j < FPW; ++j) {
             const uint32_t f = __shfl_sync(FULL, mine, j * LPF);
@@ -1839,9 +1902,10 @@ __global__ void __launch_bounds__(128, 8) fiber_lanes_kernel(WorldDev w, StepPar
             float4 *P = lanes_smem + (size_t)group * stride;
             bool done = mine == TGL_NONE || sp.curvature_cleanup_sweeps == 0;
             bool forward = true, moved = false;
-            uint32_t sweep = 0;
+            uint32_t sweep = 0, rounds = 0;
             int t0 = 0;
             while (__any_sync(FULL, !done)) {
+                rounds += done ? 0u : 1u;
                 Triplet tr;
                 const int t = forward ? t0 + gl : t0 - gl;
                 const bool act = !done && (forward ? t <= last : t >= 0) &&
@@ -1874,6 +1938,8 @@ __global__ void __launch_bounds__(128, 8) fiber_lanes_kernel(WorldDev w, StepPar
                 }
                 __syncwarp();
             }
+            // The rounds this fiber's sweeps took rank it for the next updates.
+            if (!A && w.fiber_rounds != nullptr && mine != TGL_NONE && gl == 0) w.fiber_rounds[mine] = rounds;
         }
         __syncwarp();
         // Write back; displacement check; next gate's curvature ratios;
@@ -2213,6 +2279,12 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     while (lp.lanes_wpb < wpb_max && lp.lanes_smem * (size_t)(2 * lp.lanes_wpb) <= 200 * 1024) lp.lanes_wpb *= 2;
     const uint32_t lane_warps = (w.FA + fpw - 1) / fpw;
     lp.lanes_blocks = (int)((lane_warps + lp.lanes_wpb - 1) / lp.lanes_wpb);
+    // Fibers ranked by their sweep rounds every 16 update launches, where a
+    // warp holds several fibers and there are enough of them for the ranking
+    // to pay for its launch (TGL_UPDATE_ORDER_PERIOD sets the period; 0 = off).
+    lp.order_period = w.FA >= 4096u ? 16 : 0;
+    if (const char *env = std::getenv("TGL_UPDATE_ORDER_PERIOD")) lp.order_period = std::max(std::atoi(env), 0);
+    if (lp.arena || !lp.fiber_lanes || lp.lanes_per_fiber == 32 || w.fiber_rounds == nullptr) lp.order_period = 0;
     lp.contact_lists = w.contact_skin > 0.0f;
     lp.build_ch = lp.tune_build_ch >= 512 && lp.tune_build_ch <= 4096 ? lp.tune_build_ch : lp.arena ? 1536 : 3072;
     lp.build_smem = (size_t)lp.build_ch * (sizeof(float4) + sizeof(uint32_t));
@@ -2396,12 +2468,18 @@ int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParam
         return 1;
     }
     if (lp.fiber_lanes) {
+        int kernels = 1;
+        if (lp.order_period > 0) {
+            order_by_rounds_kernel<<<1, ORDER_THREADS, 0, st>>>(w, (uint32_t)lp.order_period);
+            kernels += 1;
+        }
         if (lp.arena)
             enqueue_lanes<true, false>(w, lp, sp, st);
         else if (w.reaction != nullptr || w.layer_target != nullptr || w.vertex_target != nullptr)
             enqueue_lanes<false, true>(w, lp, sp, st);
         else
             enqueue_lanes<false, false>(w, lp, sp, st);
+        return kernels;
     } else {
         fiber_kernel<<<lp.fiber_blocks, lp.fiber_warps * 32, lp.fiber_smem, st>>>(w, sp);
     }

@@ -862,7 +862,14 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
     d.vtx_static = vtx_static_d;
     w->fiber_order_d = fiber_order_d;
     w->vtx_static_d = vtx_static_d;
+    d.update_order = fiber_order_d;
+    d.fiber_rounds = nullptr;
     if (!arena) {
+        // The update's own fiber order (ranked by sweep rounds on the device)
+        // starts as fiber_order, every fiber at zero rounds.
+        if ((rc = w->upload(&d.update_order, fiber_order)) || (rc = w->alloc(&d.fiber_rounds, F))) return fail(rc);
+        if (cudaMemset(d.fiber_rounds, 0, F * sizeof(uint32_t)) != cudaSuccess)
+            return fail(set_error(TGL_ERR_CUDA, "device initialisation failed"));
         w->h_vspan = fiber_vspan;
         w->h_s0 = fiber_s0;
         w->h_active.assign(F, 1u);
@@ -1031,8 +1038,8 @@ int tgl_run_batch(tgl_world *w, const tgl_relax_config *config, uint32_t iterati
     TGL_CUDA(cudaGraphLaunch(it->second.exec, w->stream));
     w->launches += (uint64_t)it->second.kernels;
     if (int rc = read_status(w, *config, status)) return rc;
-    if (it->second.looped)  // the step condition, two contact passes and the update per step that ran
-        w->launches += 4ull * w->host_ctl[0].loop_step;
+    if (it->second.looped)  // the step condition, two contact passes, the ranking and the update per step that ran
+        w->launches += (w->lp.order_period > 0 ? 5ull : 4ull) * w->host_ctl[0].loop_step;
     if (w->conditional) {  // rebuild pipelines the graph ran (REBUILD_KERNELS each)
         const uint32_t bodies = w->host_ctl[0].rebuild_bodies;
         w->launches += (uint64_t)REBUILD_KERNELS * (bodies >= w->rebuild_bodies_seen ? bodies - w->rebuild_bodies_seen : bodies);
@@ -1484,9 +1491,12 @@ int tgl_world_set_active_fibers(tgl_world *w, const uint8_t *active, uint64_t fi
     // Active fibers by descending vertex count, as at creation.
     std::stable_sort(order.begin(), order.end(),
                      [&](uint32_t a, uint32_t b) { return w->h_vspan[a].y > w->h_vspan[b].y; });
-    if (!order.empty())
+    if (!order.empty()) {
         TGL_CUDA(cudaMemcpyAsync(w->fiber_order_d, order.data(), order.size() * sizeof(uint32_t),
                                  cudaMemcpyHostToDevice, w->stream));
+        TGL_CUDA(cudaMemcpyAsync(d.update_order, order.data(), order.size() * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, w->stream));
+    }
     const bool all = order.size() == d.F;
     if (!all) {
         if (!w->fiber_on_d && w->alloc(&w->fiber_on_d, d.F)) return TGL_ERR_MEMORY;

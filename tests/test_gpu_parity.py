@@ -111,6 +111,25 @@ def test_positions_after_fixed_iterations_agree(case, cuda_lib):
     assert orc.neighbor_list_rebuilds() == dev.neighbor_list_rebuilds()
 
 
+@pytest.mark.parametrize("period", ["1", "0"])
+def test_positions_do_not_depend_on_the_update_order(period, cuda_lib, monkeypatch):
+    """The grouped-lane update ranks its fibers by the rounds of their last
+    curvature sweeps (every 16 launches on worlds of 4,096 fibers or more).
+    TGL_UPDATE_ORDER_PERIOD=1 ranks them again before every launch of a small
+    world, 0 keeps the creation order: the positions stay bit-identical to
+    the oracle's either way."""
+    monkeypatch.setenv("TGL_UPDATE_ORDER_PERIOD", period)
+    name, assembly, cfg, pin, d = CASES[IDS.index("mid_size_scaled")]
+    orc, dev, _ = worlds(assembly, cfg.max_step, cfg.cell_list, pin)
+    fixed = RelaxationConfig(**{**cfg.__dict__, "force_full_iterations": True})
+    for batch in (5, 11, 16):
+        so = orc.run_batch(fixed, batch)
+        sd = dev.run_batch(fixed, batch)
+        assert (so.total_iterations, so.batch_iterations) == (sd.total_iterations, sd.batch_iterations)
+    np.testing.assert_array_equal(orc.download_positions().view(np.uint32), dev.download_positions().view(np.uint32))
+    assert orc.neighbor_list_rebuilds() == dev.neighbor_list_rebuilds()
+
+
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_admissibility_verdict_is_identical(case, cuda_lib):
     name, assembly, cfg, pin, d = case
