@@ -234,9 +234,17 @@ struct Control {
     uint32_t rebuild_bodies;
     // Steps a looped batch graph has begun (its WHILE node's counter).
     uint32_t loop_step;
-    // Launches of the update's fiber-ranking kernel (it ranks every
-    // period-th launch).
+    // The update's fiber order: launches of the ranking kernel, the order
+    // the last update ran in (0 creation, 1 ranked), the one chosen for the
+    // cycle's last epochs, update time and launches per order this cycle, and
+    // the last update's start and end (%globaltimer ns).
     uint32_t order_tick;
+    uint32_t order_mode;
+    uint32_t order_best;
+    uint32_t order_runs[2];
+    unsigned long long order_ns[2];
+    unsigned long long order_begin;
+    unsigned long long order_end;
 };
 
 }  // namespace tgl

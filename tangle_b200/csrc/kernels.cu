@@ -1649,10 +1649,19 @@ __device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float ex
 
 // Order of the grouped-lane update's fibers. A warp's lane groups step
 // through their curvature sweeps together, so a warp takes as many rounds as
-// its slowest fiber. Every `period` launches of this kernel, the first FA
-// entries of fiber_order are ranked by the rounds each fiber's sweeps took at
-// its last update, most first, into update_order: a warp's fibers then need
-// about as many rounds as each other, and the heaviest warps start first.
+// its slowest fiber. Ranking the fibers by the rounds their sweeps take
+// (most first) gives each warp fibers of about equal work: on the mid-size
+// specimen's first few thousand iterations, when the update is bound by
+// instruction issue, that makes it about 9 % faster than the creation order
+// (descending vertex count). In a relaxed packing it makes it slower (warps
+// of four of the heaviest fibers run the exact projection in nearly every
+// round), so the kernel measures both: the update's blocks stamp their end
+// (%globaltimer) and this kernel its own end, so every launch reads the last
+// update's duration. Epochs of `period` launches go in cycles of
+// ORDER_CYCLE: creation order, ranked order, creation order, then the order
+// with the shorter mean update for the rest of the cycle (`ranked` forces
+// the ranked order). The key is each fiber's rounds, averaged over the epochs
+// (16 x rounds, the last epoch weighing 1/4).
 // Any order gives the same positions: a fiber's update reads and writes only
 // its own vertices and segments, and its maxima are order-free integer
 // maxima. Within one rank the order is whatever the shared-memory counters
@@ -1660,53 +1669,113 @@ __device__ inline void lanes_apply(float4 *P, int t, const Triplet &tr, float ex
 // ranks (rounds at or above the last rank share it).
 constexpr int ORDER_RANKS = 4096;
 constexpr int ORDER_THREADS = 1024;
-__global__ void __launch_bounds__(ORDER_THREADS) order_by_rounds_kernel(WorldDev w, uint32_t period) {
-    if (w.ctl->control[0] == 0) return;
-    const uint32_t tick = w.ctl->order_tick;
+constexpr uint32_t ORDER_CYCLE = 10;
+
+__device__ inline uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__global__ void __launch_bounds__(ORDER_THREADS) order_by_rounds_kernel(WorldDev w, uint32_t period, int ranked) {
+    Control *const c = w.ctl;
+    if (c->control[0] == 0) return;
+    __shared__ uint32_t epoch_mode;  // 0: no new order, 1: creation order, 2: ranked order
+    if (threadIdx.x == 0) {
+        // The last update's duration counts toward the order it ran in.
+        const uint64_t begin = c->order_begin, end = c->order_end;
+        if (begin != 0 && end > begin) {
+            c->order_ns[c->order_mode] += end - begin;
+            c->order_runs[c->order_mode] += 1;
+        }
+        const uint32_t tick = c->order_tick;
+        c->order_tick = tick + 1u;
+        uint32_t mode = 0;
+        if (tick % period == 0u) {
+            const uint32_t epoch = tick / period % ORDER_CYCLE;
+            uint32_t order = 0;  // 0 creation, 1 ranked
+            if (epoch == 0) {
+                for (int m = 0; m < 2; ++m) c->order_ns[m] = 0, c->order_runs[m] = 0;
+            } else if (epoch == 1) {
+                order = 1;
+            } else if (epoch == 3) {
+                // Ranked when its mean update was shorter: ns1 / runs1 < ns0 / runs0.
+                const uint64_t n0 = c->order_runs[0], n1 = c->order_runs[1];
+                c->order_best = n0 && n1 && c->order_ns[1] * n0 < c->order_ns[0] * n1 ? 1u : 0u;
+            }
+            if (epoch >= 3) order = c->order_best;
+            if (ranked) order = 1;
+            c->order_mode = order;
+            mode = 1 + order;
+        }
+        epoch_mode = mode;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) w.ctl->order_tick = tick + 1u;
-    if (tick % period != 0u) return;
+    const uint32_t mode = epoch_mode;
     __shared__ uint32_t start[ORDER_RANKS];
     __shared__ uint32_t warp_total[ORDER_THREADS / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const auto rank_of = [&](uint32_t f) { return ORDER_RANKS - 1 - (int)min(w.fiber_rounds[f], ORDER_RANKS - 1u); };
-    for (int i = tid; i < ORDER_RANKS; i += ORDER_THREADS) start[i] = 0;
-    __syncthreads();
-    for (uint32_t k = tid; k < w.FA; k += ORDER_THREADS) atomicAdd(&start[rank_of(w.fiber_order[k])], 1u);
-    __syncthreads();
-    // Exclusive scan of the counts: ORDER_RANKS / ORDER_THREADS per thread.
-    constexpr int PER = ORDER_RANKS / ORDER_THREADS;
-    uint32_t count[PER], sum = 0;
+    if (mode == 1) {
+        for (uint32_t k = tid; k < w.FA; k += ORDER_THREADS) {
+            const uint32_t f = w.fiber_order[k];
+            const int average = (int)w.rounds_avg[f];
+            w.rounds_avg[f] = (uint32_t)(average + (16 * (int)min(w.fiber_rounds[f], 1u << 20) - average) / 4);
+            w.update_order[k] = f;
+        }
+    } else if (mode == 2) {
+        // The thread that updates a fiber's average reads it back below.
+        const auto rank_of = [&](uint32_t f) {
+            return ORDER_RANKS - 1 - (int)min(w.rounds_avg[f] >> 4, ORDER_RANKS - 1u);
+        };
+        for (int i = tid; i < ORDER_RANKS; i += ORDER_THREADS) start[i] = 0;
+        __syncthreads();
+        for (uint32_t k = tid; k < w.FA; k += ORDER_THREADS) {
+            const uint32_t f = w.fiber_order[k];
+            const int average = (int)w.rounds_avg[f];
+            w.rounds_avg[f] = (uint32_t)(average + (16 * (int)min(w.fiber_rounds[f], 1u << 20) - average) / 4);
+            atomicAdd(&start[rank_of(f)], 1u);
+        }
+        __syncthreads();
+        // Exclusive scan of the counts: ORDER_RANKS / ORDER_THREADS per thread.
+        constexpr int PER = ORDER_RANKS / ORDER_THREADS;
+        uint32_t count[PER], sum = 0;
 #pragma unroll
-    for (int j = 0; j < PER; ++j) sum += (count[j] = start[tid * PER + j]);
-    uint32_t inclusive = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(FULL, inclusive, o);
-        if (lane >= o) inclusive += v;
-    }
-    if (lane == 31) warp_total[warp] = inclusive;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t t = warp_total[lane];
+        for (int j = 0; j < PER; ++j) sum += (count[j] = start[tid * PER + j]);
+        uint32_t inclusive = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(FULL, t, o);
-            if (lane >= o) t += v;
+            const uint32_t v = __shfl_up_sync(FULL, inclusive, o);
+            if (lane >= o) inclusive += v;
         }
-        warp_total[lane] = t;
-    }
-    __syncthreads();
-    uint32_t base = inclusive - sum + (warp > 0 ? warp_total[warp - 1] : 0u);
+        if (lane == 31) warp_total[warp] = inclusive;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t t = warp_total[lane];
 #pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        start[tid * PER + j] = base;
-        base += count[j];
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, t, o);
+                if (lane >= o) t += v;
+            }
+            warp_total[lane] = t;
+        }
+        __syncthreads();
+        uint32_t base = inclusive - sum + (warp > 0 ? warp_total[warp - 1] : 0u);
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            start[tid * PER + j] = base;
+            base += count[j];
+        }
+        __syncthreads();
+        for (uint32_t k = tid; k < w.FA; k += ORDER_THREADS) {
+            const uint32_t f = w.fiber_order[k];
+            w.update_order[atomicAdd(&start[rank_of(f)], 1u)] = f;
+        }
     }
     __syncthreads();
-    for (uint32_t k = tid; k < w.FA; k += ORDER_THREADS) {
-        const uint32_t f = w.fiber_order[k];
-        w.update_order[atomicAdd(&start[rank_of(f)], 1u)] = f;
+    // The update starts when this kernel ends.
+    if (threadIdx.x == 0) {
+        c->order_end = 0;
+        c->order_begin = global_ns();
     }
 }
 
@@ -1938,8 +2007,10 @@ __global__ void __launch_bounds__(128, 8) fiber_lanes_kernel(WorldDev w, StepPar
                 }
                 __syncwarp();
             }
-            // The rounds this fiber's sweeps took rank it for the next updates.
+            // The rounds this fiber's sweeps took rank it for the next updates
+            // (a fiber of a stopped specimen took none).
             if (!A && w.fiber_rounds != nullptr && mine != TGL_NONE && gl == 0) w.fiber_rounds[mine] = rounds;
+            if (A && w.fiber_rounds != nullptr && gl == 0 && slot < w.FA) w.fiber_rounds[w.update_order[slot]] = rounds;
         }
         __syncwarp();
         // Write back; displacement check; next gate's curvature ratios;
@@ -1995,6 +2066,8 @@ __global__ void __launch_bounds__(128, 8) fiber_lanes_kernel(WorldDev w, StepPar
         }
         __syncwarp();
     }
+    // The end of the update, for the fiber-order choice.
+    if (lane == 0) atomicMax(&w.ctl->order_end, (unsigned long long)global_ns());
     if (A) return;
     smax = warp_max_u32(smax);
     cmax = warp_max_u32(cmax);
@@ -2279,12 +2352,15 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     while (lp.lanes_wpb < wpb_max && lp.lanes_smem * (size_t)(2 * lp.lanes_wpb) <= 200 * 1024) lp.lanes_wpb *= 2;
     const uint32_t lane_warps = (w.FA + fpw - 1) / fpw;
     lp.lanes_blocks = (int)((lane_warps + lp.lanes_wpb - 1) / lp.lanes_wpb);
-    // Fibers ranked by their sweep rounds every 16 update launches, where a
-    // warp holds several fibers and there are enough of them for the ranking
-    // to pay for its launch (TGL_UPDATE_ORDER_PERIOD sets the period; 0 = off).
+    // Fibers ranked by their sweep rounds every 16 update launches where
+    // there are enough of them for the ranking to pay for its launch
+    // (TGL_UPDATE_ORDER_PERIOD sets the period; 0 = off).
     lp.order_period = w.FA >= 4096u ? 16 : 0;
     if (const char *env = std::getenv("TGL_UPDATE_ORDER_PERIOD")) lp.order_period = std::max(std::atoi(env), 0);
-    if (lp.arena || !lp.fiber_lanes || lp.lanes_per_fiber == 32 || w.fiber_rounds == nullptr) lp.order_period = 0;
+    if (!lp.fiber_lanes || w.fiber_rounds == nullptr) lp.order_period = 0;
+    // TGL_UPDATE_ORDER_RANKED=1 keeps the ranked order instead of timing both.
+    lp.order_ranked = 0;
+    if (const char *env = std::getenv("TGL_UPDATE_ORDER_RANKED")) lp.order_ranked = std::atoi(env) != 0;
     lp.contact_lists = w.contact_skin > 0.0f;
     lp.build_ch = lp.tune_build_ch >= 512 && lp.tune_build_ch <= 4096 ? lp.tune_build_ch : lp.arena ? 1536 : 3072;
     lp.build_smem = (size_t)lp.build_ch * (sizeof(float4) + sizeof(uint32_t));
@@ -2470,7 +2546,7 @@ int launch_fiber_update(const WorldDev &w, const LaunchPlan &lp, const StepParam
     if (lp.fiber_lanes) {
         int kernels = 1;
         if (lp.order_period > 0) {
-            order_by_rounds_kernel<<<1, ORDER_THREADS, 0, st>>>(w, (uint32_t)lp.order_period);
+            order_by_rounds_kernel<<<1, ORDER_THREADS, 0, st>>>(w, (uint32_t)lp.order_period, lp.order_ranked);
             kernels += 1;
         }
         if (lp.arena)

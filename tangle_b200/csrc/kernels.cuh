@@ -52,10 +52,10 @@ struct WorldDev {
     const uint32_t *fiber_order; // [F] fibers by descending vertex count
     // The grouped-lane update's order of the first FA fibers (fiber_order
     // ranked by the rounds of their last curvature sweeps), and those rounds
-    // per fiber; an arena's update_order is fiber_order and fiber_rounds is
-    // nullptr.
+    // per fiber.
     uint32_t *update_order;     // [F]
     uint32_t *fiber_rounds;     // [F]
+    uint32_t *rounds_avg;       // [F] 16 x rounds, averaged over the rankings
     const float4 *vtx_static;   // [V] max curvature, rest chord to v-2, rest chord to v+2, wall extent
     const uint32_t *pinned;     // [V]
     const float *rest;          // [S] rest lengths
@@ -231,6 +231,7 @@ struct LaunchPlan {
     int tune_wpb = 0;       // requested warps per block (0: the default, 4)
     int lanes_blocks;
     int order_period;       // rank the update's fibers every this many launches (0: never)
+    int order_ranked;       // always the ranked order (1) instead of timing it against the creation order (0)
     bool contact_lists;     // contact lists on (contact_skin > 0)
     int build_ch;           // candidate slots staged per build chunk
     size_t build_smem;

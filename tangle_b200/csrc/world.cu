@@ -862,14 +862,15 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
     d.vtx_static = vtx_static_d;
     w->fiber_order_d = fiber_order_d;
     w->vtx_static_d = vtx_static_d;
-    d.update_order = fiber_order_d;
-    d.fiber_rounds = nullptr;
+    // The update's own fiber order (ranked by sweep rounds on the device)
+    // starts as fiber_order, every fiber at zero rounds.
+    if ((rc = w->upload(&d.update_order, fiber_order)) || (rc = w->alloc(&d.fiber_rounds, F)) ||
+        (rc = w->alloc(&d.rounds_avg, F)))
+        return fail(rc);
+    if (cudaMemset(d.fiber_rounds, 0, F * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMemset(d.rounds_avg, 0, F * sizeof(uint32_t)) != cudaSuccess)
+        return fail(set_error(TGL_ERR_CUDA, "device initialisation failed"));
     if (!arena) {
-        // The update's own fiber order (ranked by sweep rounds on the device)
-        // starts as fiber_order, every fiber at zero rounds.
-        if ((rc = w->upload(&d.update_order, fiber_order)) || (rc = w->alloc(&d.fiber_rounds, F))) return fail(rc);
-        if (cudaMemset(d.fiber_rounds, 0, F * sizeof(uint32_t)) != cudaSuccess)
-            return fail(set_error(TGL_ERR_CUDA, "device initialisation failed"));
         w->h_vspan = fiber_vspan;
         w->h_s0 = fiber_s0;
         w->h_active.assign(F, 1u);

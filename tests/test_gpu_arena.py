@@ -55,8 +55,16 @@ def test_arena_positions_match_single_worlds_bit_for_bit(cuda_lib):
     assert arena.neighbor_list_rebuilds() == sum(w.neighbor_list_rebuilds() for w in singles)
 
 
-def test_arena_gates_stop_each_specimen_on_its_own(cuda_lib):
+@pytest.mark.parametrize("ranked", [None, "1"])
+def test_arena_gates_stop_each_specimen_on_its_own(ranked, cuda_lib, monkeypatch):
+    """With ranked "1" the update ranks its fibers by their sweep rounds
+    before every launch (stopped specimens' fibers rank last, at zero
+    rounds): the bits do not change."""
     from tangle_b200.device import DeviceWorld
+
+    if ranked is not None:
+        monkeypatch.setenv("TGL_UPDATE_ORDER_PERIOD", "1")
+        monkeypatch.setenv("TGL_UPDATE_ORDER_RANKED", ranked)
 
     specimens = [cpu_runnable_specimen(seed=s) for s in (5, 6, 7)] + [fx.crossed_assembly(), fx.hairpin()]
     packeds = [PackedAssembly.from_assembly(a) for a in specimens]

@@ -111,14 +111,17 @@ def test_positions_after_fixed_iterations_agree(case, cuda_lib):
     assert orc.neighbor_list_rebuilds() == dev.neighbor_list_rebuilds()
 
 
-@pytest.mark.parametrize("period", ["1", "0"])
-def test_positions_do_not_depend_on_the_update_order(period, cuda_lib, monkeypatch):
-    """The grouped-lane update ranks its fibers by the rounds of their last
-    curvature sweeps (every 16 launches on worlds of 4,096 fibers or more).
-    TGL_UPDATE_ORDER_PERIOD=1 ranks them again before every launch of a small
-    world, 0 keeps the creation order: the positions stay bit-identical to
-    the oracle's either way."""
+@pytest.mark.parametrize("period,ranked", [("1", "0"), ("1", "1"), ("0", "0")])
+def test_positions_do_not_depend_on_the_update_order(period, ranked, cuda_lib, monkeypatch):
+    """The grouped-lane update takes its fibers in creation order or ranked
+    by the rounds of their curvature sweeps, whichever its timed epochs find
+    faster (epochs of 16 launches on worlds of 4,096 fibers or more).
+    TGL_UPDATE_ORDER_PERIOD=1 makes every launch of a small world an epoch
+    (both orders in turn), TGL_UPDATE_ORDER_RANKED=1 ranks before every one,
+    0 keeps the creation order: the positions stay bit-identical to the
+    oracle's in every case."""
     monkeypatch.setenv("TGL_UPDATE_ORDER_PERIOD", period)
+    monkeypatch.setenv("TGL_UPDATE_ORDER_RANKED", ranked)
     name, assembly, cfg, pin, d = CASES[IDS.index("mid_size_scaled")]
     orc, dev, _ = worlds(assembly, cfg.max_step, cfg.cell_list, pin)
     fixed = RelaxationConfig(**{**cfg.__dict__, "force_full_iterations": True})
