@@ -2352,9 +2352,9 @@ void plan_launches(const WorldDev &w, LaunchPlan &lp) {
     while (lp.lanes_wpb < wpb_max && lp.lanes_smem * (size_t)(2 * lp.lanes_wpb) <= 200 * 1024) lp.lanes_wpb *= 2;
     const uint32_t lane_warps = (w.FA + fpw - 1) / fpw;
     lp.lanes_blocks = (int)((lane_warps + lp.lanes_wpb - 1) / lp.lanes_wpb);
-    // Fibers ranked by their sweep rounds every 16 update launches where
-    // there are enough of them for the ranking to pay for its launch
-    // (TGL_UPDATE_ORDER_PERIOD sets the period; 0 = off).
+    // The update's fiber order is chosen in epochs of 16 launches where
+    // there are enough fibers for the choice to pay for its kernel
+    // (TGL_UPDATE_ORDER_PERIOD sets the epoch; 0 keeps the creation order).
     lp.order_period = w.FA >= 4096u ? 16 : 0;
     if (const char *env = std::getenv("TGL_UPDATE_ORDER_PERIOD")) lp.order_period = std::max(std::atoi(env), 0);
     if (!lp.fiber_lanes || w.fiber_rounds == nullptr) lp.order_period = 0;

@@ -50,12 +50,13 @@ struct WorldDev {
     const uint2 *fiber_vspan;   // [F] first vertex, vertex count
     const uint32_t *fiber_s0;   // [F] first segment
     const uint32_t *fiber_order; // [F] fibers by descending vertex count
-    // The grouped-lane update's order of the first FA fibers (fiber_order
-    // ranked by the rounds of their last curvature sweeps), and those rounds
-    // per fiber.
+    // The grouped-lane update's order of the first FA fibers: fiber_order
+    // itself, or its fibers ranked by their curvature-sweep rounds, whichever
+    // order_by_rounds_kernel timed as faster. The rounds of each fiber's last
+    // sweeps, and their moving average over the order epochs.
     uint32_t *update_order;     // [F]
     uint32_t *fiber_rounds;     // [F]
-    uint32_t *rounds_avg;       // [F] 16 x rounds, averaged over the rankings
+    uint32_t *rounds_avg;       // [F] 16 x rounds
     const float4 *vtx_static;   // [V] max curvature, rest chord to v-2, rest chord to v+2, wall extent
     const uint32_t *pinned;     // [V]
     const float *rest;          // [S] rest lengths
@@ -230,7 +231,7 @@ struct LaunchPlan {
     int lanes_wpb;          // warps per block (1, 2 or 4)
     int tune_wpb = 0;       // requested warps per block (0: the default, 4)
     int lanes_blocks;
-    int order_period;       // rank the update's fibers every this many launches (0: never)
+    int order_period;       // update launches per fiber-order epoch (0: creation order, no order kernel)
     int order_ranked;       // always the ranked order (1) instead of timing it against the creation order (0)
     bool contact_lists;     // contact lists on (contact_skin > 0)
     int build_ch;           // candidate slots staged per build chunk

@@ -862,8 +862,8 @@ int build_world(std::vector<HostSpecimen> &hosts, const tgl_cell_list_config *cl
     d.vtx_static = vtx_static_d;
     w->fiber_order_d = fiber_order_d;
     w->vtx_static_d = vtx_static_d;
-    // The update's own fiber order (ranked by sweep rounds on the device)
-    // starts as fiber_order, every fiber at zero rounds.
+    // The update's own fiber order (chosen on the device) starts as
+    // fiber_order, every fiber at zero rounds.
     if ((rc = w->upload(&d.update_order, fiber_order)) || (rc = w->alloc(&d.fiber_rounds, F)) ||
         (rc = w->alloc(&d.rounds_avg, F)))
         return fail(rc);
@@ -1039,7 +1039,7 @@ int tgl_run_batch(tgl_world *w, const tgl_relax_config *config, uint32_t iterati
     TGL_CUDA(cudaGraphLaunch(it->second.exec, w->stream));
     w->launches += (uint64_t)it->second.kernels;
     if (int rc = read_status(w, *config, status)) return rc;
-    if (it->second.looped)  // the step condition, two contact passes, the ranking and the update per step that ran
+    if (it->second.looped)  // the step condition, two contact passes, the order kernel and the update per step that ran
         w->launches += (w->lp.order_period > 0 ? 5ull : 4ull) * w->host_ctl[0].loop_step;
     if (w->conditional) {  // rebuild pipelines the graph ran (REBUILD_KERNELS each)
         const uint32_t bodies = w->host_ctl[0].rebuild_bodies;
